@@ -1,0 +1,85 @@
+"""Golden cases: seeded inputs (regenerated from these definitions) plus the
+svm-train options each case runs with.  make_golden.py runs the reference's own
+CPU solver (oracle/_ref/ref_dump, built from the reference sources) on every case
+and commits its output next to this file; tests compare the oracle restatement
+and the GPU engine against those outputs."""
+import hashlib
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "libsvm-cuda_b200"))
+
+from svmb200 import datagen  # noqa: E402
+
+
+def _binary_dense(n, nt, d, seed):
+    return datagen.dense_gauss(n=n, n_test=nt, d=d, seed=seed)
+
+
+def _sparse(n, nt, d, seed, nnz=40.0):
+    return datagen.sparse_text(n=n, n_test=nt, d=d, seed=seed, nnz_mean=nnz)
+
+
+def _pixels(n, nt, d, seed):
+    return datagen.dense_pixels(n=n, n_test=nt, d=d, seed=seed)
+
+
+def _multi(k, largest, d, seed):
+    tr, te, _ = datagen.multiclass_geo(n_classes=k, largest=largest, d=d, seed=seed, n_test_frac=0.2)
+    return tr, te
+
+
+def _edge_rows(seed):
+    """Rows with no features, duplicated rows and a one-feature row: empty and
+    degenerate inputs the reference accepts."""
+    import numpy as np
+    tr, te = datagen.dense_gauss(n=60, n_test=20, d=8, seed=seed)
+    X = tr.to_dense()
+    X[3] = 0.0           # empty row
+    X[10] = X[11]        # duplicate pair (same label after the next line)
+    tr.y[10] = tr.y[11]
+    X[20] = 0.0
+    X[20, 5] = 1.5       # single feature
+    return datagen.from_dense(X, tr.y), te
+
+
+# name -> (builder, svm-train options, mode); mode "train" (with test file) or "cv:<k>"
+CASES = {
+    "rbf_dense_small":      (lambda: _binary_dense(300, 100, 16, 11), "-s 0 -t 2 -c 1 -g 0.0625 -e 0.001", "train"),
+    "rbf_dense_noshrink":   (lambda: _binary_dense(300, 100, 16, 11), "-s 0 -t 2 -c 1 -g 0.0625 -h 0", "train"),
+    "rbf_dense_tinycache":  (lambda: _binary_dense(400, 50, 16, 12), "-s 0 -t 2 -c 4 -g 0.1 -m 0.01", "train"),
+    "linear_dense":         (lambda: _binary_dense(300, 100, 16, 13), "-s 0 -t 0 -c 0.5", "train"),
+    "poly_dense":           (lambda: _binary_dense(300, 100, 16, 14), "-s 0 -t 1 -d 3 -g 0.05 -r 1 -c 2", "train"),
+    "sigmoid_dense":        (lambda: _binary_dense(300, 100, 16, 15), "-s 0 -t 3 -g 0.01 -r -0.5 -c 1", "train"),
+    "nu_rbf_dense":         (lambda: _binary_dense(300, 100, 16, 16), "-s 1 -t 2 -n 0.3 -g 0.0625", "train"),
+    "nu_poly_noshrink":     (lambda: _binary_dense(250, 50, 16, 17), "-s 1 -t 1 -d 3 -g 0.05 -r 1 -n 0.4 -h 0", "train"),
+    "weighted_rbf":         (lambda: _binary_dense(300, 100, 16, 18), "-s 0 -t 2 -c 1 -g 0.0625 -w1 3 -w-1 0.5", "train"),
+    "rbf_sparse":           (lambda: _sparse(600, 150, 2000, 21), "-s 0 -t 2 -c 4 -g 0.5", "train"),
+    "linear_sparse":        (lambda: _sparse(600, 150, 2000, 22), "-s 0 -t 0 -c 4", "train"),
+    "rbf_pixels":           (lambda: _pixels(500, 100, 196, 31), "-s 0 -t 2 -c 10 -g 0.0051020408163265302", "train"),
+    "multiclass_rbf":       (lambda: _multi(4, 120, 32, 41), "-s 0 -t 2 -c 1 -g 0.03125", "train"),
+    "multiclass_nu":        (lambda: _multi(3, 100, 32, 42), "-s 1 -t 2 -n 0.2 -g 0.03125", "train"),
+    "cv_multiclass":        (lambda: _multi(3, 90, 16, 43), "-s 0 -t 2 -c 2 -g 0.0625", "cv:5"),
+    "edge_rows":            (lambda: _edge_rows(51), "-s 0 -t 2 -c 1 -g 0.125", "train"),
+    "rbf_dense_c1":         (lambda: _binary_dense(4000, 1000, 64, 1), "-s 0 -t 2 -c 1 -g 0.015625 -m 100 -h 1", "train"),
+}
+
+# cases small enough to run in the default CPU suite in a second or two
+FAST = [k for k in CASES if k != "rbf_dense_c1"]
+
+
+def materialise(name, outdir):
+    """Write the case's train (and test) file; return (train, test|None, options, mode, sha256)."""
+    build, opts, mode = CASES[name]
+    tr, te = build()
+    trp = os.path.join(outdir, f"{name}.train")
+    datagen.write_libsvm(trp, tr)
+    h = hashlib.sha256(open(trp, "rb").read())
+    tep = None
+    if mode == "train" and te is not None and te.n > 0:
+        tep = os.path.join(outdir, f"{name}.test")
+        datagen.write_libsvm(tep, te)
+        h.update(open(tep, "rb").read())
+    return trp, tep, opts, mode, h.hexdigest()
