@@ -1,0 +1,113 @@
+/*
+ * svm_b200.h -- C-ABI of the B200 SVM engine beyond the svm.h drop-in API.
+ *
+ * Plain pointers and sizes only.  Every function returns 0 on success and a
+ * negative value on failure; svmb_last_error() then describes the failure
+ * (per calling thread).  Nothing here allocates memory the caller must free,
+ * except the resident-rows handle (svmb_rows_free).
+ *
+ * The reference has no such layer: its svm.cpp calls the CudaSolver methods
+ * (reference libsvm/cuda_solver.h:224-243: setup_solver, select_working_set,
+ * compute_alpha, update_gradient, update_alpha_status, fetch_vectors) from
+ * inside Solver::Solve (svm.cpp:556-776).  svmb_solve_binary_csr replaces that
+ * whole seam with one call that runs an entire Solver::Solve /
+ * Solver_NU::Solve on the device.
+ */
+#ifndef LIBSVM_B200_SVMB_H
+#define LIBSVM_B200_SVMB_H
+
+#include "svm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Statistics of one binary solve (what the reference prints through info():
+ * "#iter", "obj", "rho", "nSV", "nBSV", reference svm.cpp:821, 1739, 1763). */
+typedef struct svmb_solve_stats {
+    long long iters;
+    double obj;          /* dual objective, after the nu-SVC 1/r^2 scaling */
+    double rho;          /* after the nu-SVC 1/r scaling */
+    double r;            /* nu-SVC only */
+    int l;
+    int nr_sv;
+    int nr_bsv;
+    int status;          /* 0 converged, 1 max_iter reached */
+    int active_size;     /* active set size at exit (shrinking) */
+    int pad;
+    double seconds;      /* device time of the launch that solved it */
+} svmb_solve_stats;
+
+/* Parameters of a binary solve (the subset of svm_parameter the solver reads). */
+typedef struct svmb_params {
+    int svm_type;        /* C_SVC or NU_SVC */
+    int kernel_type;     /* LINEAR, POLY, RBF, SIGMOID */
+    int degree;
+    int shrinking;
+    double gamma;
+    double coef0;
+    double C_pos;        /* C-SVC: C for y>0 (reference solve_c_svc Cp) */
+    double C_neg;        /* C-SVC: C for y<=0 (Cn) */
+    double nu;           /* nu-SVC */
+    double eps;
+    double cache_mb;     /* Q-row cache budget per solve, MB (svm_parameter.cache_size) */
+    int form;            /* SVMB_FORM_* */
+    int blocks;          /* thread blocks per solve; 0 = automatic */
+} svmb_params;
+
+#define SVMB_FORM_EXACT 0   /* fp32 features, fp64 accumulation in feature order */
+#define SVMB_FORM_FP32  1   /* fp32 features, fp32 accumulation (plain CUDA-core form) */
+
+const char *svmb_last_error(void);
+int svmb_version(void);                         /* LIBSVM_VERSION * 100 + engine revision */
+int svmb_device_available(void);                /* 1 if a CUDA device can be used */
+
+/* Process-wide engine options used by svm_train / svm_cross_validation:
+ *   "form"   SVMB_FORM_EXACT (default) or SVMB_FORM_FP32
+ *   "blocks" thread blocks per solve (0 = automatic)
+ *   "layout" -1 automatic, 0 CSR, 1 dense device layout of the rows */
+int svmb_set_option(const char *name, long long value);
+
+/* Per-subproblem statistics of the last svm_train / svm_cross_validation
+ * call on this process; returns the number of records (copies at most cap). */
+int svmb_last_train_stats(svmb_solve_stats *out, int cap);
+
+/* Decision values of n rows in one device pass (the batched form of
+ * svm_predict_values, reference svm.cpp:2569-2643).  labels[n];
+ * dec_values may be NULL or [n][nr_class*(nr_class-1)/2]. */
+int svmb_predict_batch(const struct svm_model *model, const struct svm_node *const *rows, int n,
+                       double *labels, double *dec_values);
+
+/* One binary solve from host CSR rows (0-based columns, n rows, d columns).
+ * y[i] > 0 is the positive class.  alpha_out[n] receives the signed
+ * coefficients y_i*alpha_i (nu-SVC: divided by r), i.e. the reference's
+ * decision_function.alpha (svm.cpp:1532, :1578-1584); stats may be NULL.
+ * Host buffers; host<->device copies are part of the call. */
+int svmb_solve_binary_csr(int n, int d, const long long *rowptr, const int *col, const float *val,
+                          const double *y, const svmb_params *params, double *alpha_out,
+                          svmb_solve_stats *stats);
+
+/* Many independent binary solves over subsets of one row set, in ONE
+ * persistent device launch (one-vs-one pairs, CV folds, grid points).
+ * Instance k uses rows inst_rows[inst_ptr[k] .. inst_ptr[k+1]) with labels
+ * inst_y[same range] and params[k]; kernel parameters and form must agree
+ * across instances.  alpha_out is laid out like inst_rows. */
+int svmb_solve_many_csr(int n, int d, const long long *rowptr, const int *col, const float *val,
+                        int ninst, const int *inst_ptr, const int *inst_rows, const double *inst_y,
+                        const svmb_params *params, double *alpha_out, svmb_solve_stats *stats);
+
+/* Resident rows: upload once, solve many times (the data stays in HBM). */
+typedef struct svmb_rows svmb_rows;
+int svmb_rows_upload_csr(int n, int d, const long long *rowptr, const int *col, const float *val,
+                         int layout /* -1 auto, 0 CSR, 1 dense */, svmb_rows **out);
+int svmb_rows_info(const svmb_rows *rows, int *n, int *d, int *dense, long long *bytes);
+int svmb_rows_solve_many(const svmb_rows *rows, int ninst, const int *inst_ptr, const int *inst_rows,
+                         const double *inst_y, const svmb_params *params, double *alpha_out,
+                         svmb_solve_stats *stats);
+void svmb_rows_free(svmb_rows *rows);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIBSVM_B200_SVMB_H */

@@ -1,0 +1,231 @@
+// capi.cpp -- the svmb_* C-ABI (include/svm_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "engine.hpp"
+#include "predict.hpp"
+#include "svm_b200.h"
+
+namespace svmb {
+int api_set_option(const char *name, long long value);
+int api_last_stats(svmb_solve_stats *out, int cap);
+}
+
+struct svmb_rows {
+    svmb::DeviceRows dev;
+};
+
+namespace {
+
+int check_params(const svmb_params *p)
+{
+    if (!p) { svmb::set_error("params is NULL"); return -1; }
+    if (p->svm_type != C_SVC && p->svm_type != NU_SVC) { svmb::set_error("svm_type must be C_SVC or NU_SVC"); return -1; }
+    if (p->kernel_type < LINEAR || p->kernel_type > SIGMOID) { svmb::set_error("kernel_type must be LINEAR, POLY, RBF or SIGMOID"); return -1; }
+    if (p->gamma < 0) { svmb::set_error("gamma < 0"); return -1; }
+    if (p->degree < 0) { svmb::set_error("degree of polynomial kernel < 0"); return -1; }
+    if (p->eps <= 0) { svmb::set_error("eps <= 0"); return -1; }
+    if (p->cache_mb <= 0) { svmb::set_error("cache_size <= 0"); return -1; }
+    if (p->svm_type == C_SVC && (p->C_pos <= 0 || p->C_neg <= 0)) { svmb::set_error("C <= 0"); return -1; }
+    if (p->svm_type == NU_SVC && (p->nu <= 0 || p->nu > 1)) { svmb::set_error("nu <= 0 or nu > 1"); return -1; }
+    if (p->form != SVMB_FORM_EXACT && p->form != SVMB_FORM_FP32) { svmb::set_error("unknown form"); return -1; }
+    return 0;
+}
+
+int solve_many(const svmb::DeviceRows &rows, int ninst, const int *inst_ptr, const int *inst_rows, const double *inst_y,
+               const svmb_params *params, double *alpha_out, svmb_solve_stats *stats)
+{
+    if (ninst <= 0) return 0;
+    for (int k = 0; k < ninst; k++) {
+        if (check_params(&params[k])) return -1;
+        if (params[k].kernel_type != params[0].kernel_type || params[k].gamma != params[0].gamma ||
+            params[k].coef0 != params[0].coef0 || params[k].degree != params[0].degree || params[k].form != params[0].form) {
+            svmb::set_error("instances of one launch must share kernel parameters and form");
+            return -1;
+        }
+    }
+    std::vector<svmb::SubProblem> subs(ninst);
+    for (int k = 0; k < ninst; k++) {
+        const int a = inst_ptr[k], b = inst_ptr[k + 1];
+        const int l = b - a;
+        if (l < 0) { svmb::set_error("inst_ptr must be non-decreasing"); return -1; }
+        svmb::SubProblem &sp = subs[k];
+        sp.rows.assign(inst_rows + a, inst_rows + b);
+        for (int r : sp.rows)
+            if (r < 0 || r >= rows.n) { svmb::set_error("row id out of range"); return -1; }
+        sp.y.resize(l);
+        for (int i = 0; i < l; i++) sp.y[i] = inst_y[a + i] > 0 ? +1 : -1;
+        sp.alpha0.assign(l, 0.0);
+        sp.p.assign(l, 0.0);
+        const svmb_params &p = params[k];
+        if (p.svm_type == NU_SVC) {
+            // solve_nu_svc initial point (reference svm.cpp:1546-1564)
+            int npos = 0, nneg = 0;
+            for (int i = 0; i < l; i++) (sp.y[i] > 0 ? npos : nneg)++;
+            if (p.nu * l / 2 > std::min(npos, nneg)) { svmb::set_error("specified nu is infeasible"); return -1; }
+            double sum_pos = p.nu * l / 2, sum_neg = p.nu * l / 2;
+            for (int i = 0; i < l; i++) {
+                if (sp.y[i] == +1) { sp.alpha0[i] = std::min(1.0, sum_pos); sum_pos -= sp.alpha0[i]; }
+                else { sp.alpha0[i] = std::min(1.0, sum_neg); sum_neg -= sp.alpha0[i]; }
+            }
+            sp.nu = 1;
+            sp.Cp = sp.Cn = 1.0;
+        } else {
+            for (int i = 0; i < l; i++) sp.p[i] = -1;
+            sp.Cp = p.C_pos;
+            sp.Cn = p.C_neg;
+        }
+    }
+    svmb::SolveParams prm;
+    prm.kp.type = params[0].kernel_type;
+    prm.kp.degree = params[0].degree;
+    prm.kp.gamma = params[0].gamma;
+    prm.kp.coef0 = params[0].coef0;
+    prm.eps = params[0].eps;
+    prm.shrinking = params[0].shrinking;
+    prm.cache_mb = params[0].cache_mb;
+    prm.form = params[0].form;
+    prm.blocks_override = params[0].blocks;
+    for (int k = 1; k < ninst; k++)
+        if (params[k].eps != prm.eps || params[k].shrinking != prm.shrinking || params[k].cache_mb != prm.cache_mb) {
+            svmb::set_error("instances of one launch must share eps, shrinking and cache_mb");
+            return -1;
+        }
+    std::vector<svmb::SolveResult> res;
+    if (svmb::solve_batch(rows, subs, prm, res, 0) != 0) return -1;
+    for (int k = 0; k < ninst; k++) {
+        const svmb::SubProblem &sp = subs[k];
+        const svmb::SolveResult &R = res[k];
+        const int a = inst_ptr[k], l = (int)sp.rows.size();
+        double rho = R.out.rho, obj = R.out.obj, up = sp.Cp, un = sp.Cn;
+        for (int i = 0; i < l; i++) {
+            double v = R.alpha[i];
+            if (sp.nu) v *= sp.y[i] / R.out.r;
+            else v *= sp.y[i];
+            alpha_out[a + i] = v;
+        }
+        if (sp.nu) {
+            rho /= R.out.r;
+            obj /= (R.out.r * R.out.r);
+            up = un = 1 / R.out.r;
+        }
+        if (stats) {
+            svmb_solve_stats &st = stats[k];
+            memset(&st, 0, sizeof st);
+            st.iters = R.out.iters;
+            st.obj = obj;
+            st.rho = rho;
+            st.r = R.out.r;
+            st.l = l;
+            st.status = R.out.status;
+            st.active_size = R.out.active_size;
+            st.seconds = R.seconds;
+            for (int i = 0; i < l; i++) {
+                const double v = alpha_out[a + i];
+                if (v != 0) {
+                    st.nr_sv++;
+                    if (fabs(v) >= (sp.y[i] > 0 ? up : un)) st.nr_bsv++;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *svmb_last_error(void) { return svmb::last_error(); }
+int svmb_version(void) { return LIBSVM_VERSION * 100 + 1; }
+
+int svmb_device_available(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n > 0 ? 1 : 0;
+}
+
+int svmb_set_option(const char *name, long long value)
+{
+    if (!name || svmb::api_set_option(name, value) != 0) {
+        svmb::set_error("unknown option or value");
+        return -1;
+    }
+    return 0;
+}
+
+int svmb_last_train_stats(svmb_solve_stats *out, int cap) { return svmb::api_last_stats(out, cap); }
+
+int svmb_predict_batch(const struct svm_model *model, const struct svm_node *const *rows, int n, double *labels,
+                       double *dec_values)
+{
+    if (!model || (n > 0 && (!rows || !labels))) {
+        svmb::set_error("NULL argument");
+        return -1;
+    }
+    return svmb::predict_batch(model, rows, n, labels, dec_values);
+}
+
+int svmb_rows_upload_csr(int n, int d, const long long *rowptr, const int *col, const float *val, int layout,
+                         svmb_rows **out)
+{
+    if (!out || n < 0 || d < 0 || (n > 0 && !rowptr)) {
+        svmb::set_error("invalid rows");
+        return -1;
+    }
+    for (int r = 0; r < n; r++)
+        if (rowptr[r + 1] < rowptr[r]) { svmb::set_error("rowptr must be non-decreasing"); return -1; }
+    for (long long e = 0; e < (n ? rowptr[n] : 0); e++)
+        if (col[e] < 0 || col[e] >= d) { svmb::set_error("column index out of range"); return -1; }
+    std::unique_ptr<svmb_rows> h(new svmb_rows());
+    if (svmb::upload_csr(rowptr, col, val, n, d, h->dev, layout, 0) != 0) return -1;
+    *out = h.release();
+    return 0;
+}
+
+int svmb_rows_info(const svmb_rows *rows, int *n, int *d, int *dense, long long *bytes)
+{
+    if (!rows) { svmb::set_error("NULL rows"); return -1; }
+    if (n) *n = rows->dev.n;
+    if (d) *d = rows->dev.d;
+    if (dense) *dense = rows->dev.dense ? 1 : 0;
+    if (bytes) *bytes = (long long)rows->dev.bytes;
+    return 0;
+}
+
+int svmb_rows_solve_many(const svmb_rows *rows, int ninst, const int *inst_ptr, const int *inst_rows, const double *inst_y,
+                         const svmb_params *params, double *alpha_out, svmb_solve_stats *stats)
+{
+    if (!rows) { svmb::set_error("NULL rows"); return -1; }
+    return solve_many(rows->dev, ninst, inst_ptr, inst_rows, inst_y, params, alpha_out, stats);
+}
+
+void svmb_rows_free(svmb_rows *rows) { delete rows; }
+
+int svmb_solve_many_csr(int n, int d, const long long *rowptr, const int *col, const float *val, int ninst,
+                        const int *inst_ptr, const int *inst_rows, const double *inst_y, const svmb_params *params,
+                        double *alpha_out, svmb_solve_stats *stats)
+{
+    svmb_rows *rows = nullptr;
+    if (svmb_rows_upload_csr(n, d, rowptr, col, val, -1, &rows) != 0) return -1;
+    const int rc = solve_many(rows->dev, ninst, inst_ptr, inst_rows, inst_y, params, alpha_out, stats);
+    svmb_rows_free(rows);
+    return rc;
+}
+
+int svmb_solve_binary_csr(int n, int d, const long long *rowptr, const int *col, const float *val, const double *y,
+                          const svmb_params *params, double *alpha_out, svmb_solve_stats *stats)
+{
+    std::vector<int> ptr = {0, n};
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; i++) idx[i] = i;
+    return svmb_solve_many_csr(n, d, rowptr, col, val, 1, ptr.data(), idx.data(), y, params, alpha_out, stats);
+}
+
+}  // extern "C"

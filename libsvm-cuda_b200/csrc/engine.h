@@ -1,0 +1,118 @@
+// engine.h -- structures shared by the device solver (smo_kernel.cu) and the
+// host orchestration (engine.cpp).  Internal to libsvm_b200.so.
+//
+// One SMO "instance" is one binary subproblem of the reference's svm_train
+// (reference libsvm/svm.cpp:1707 svm_train_one -> Solver::Solve :515 or
+// Solver_NU::Solve :1060).  An instance is solved by a GROUP of thread blocks
+// of one persistent launch; several instances (one-vs-one pairs, CV folds,
+// grid points) can share a launch, each with its own group.
+#pragma once
+#include <cstdint>
+#include <cstddef>
+
+namespace svmb {
+
+constexpr int kThreads = 512;           // threads per block of the persistent solver
+constexpr int kWarps = kThreads / 32;
+constexpr int kSrcBatch = 8;            // source rows staged per pass in the row-block product
+constexpr int kMaxWays = 8;             // set associativity of the Q-row cache
+constexpr int kEpochFull = -2;          // cache slot holds the complete row
+constexpr int kNoTag = -1;
+
+enum : uint8_t { ST_LOWER = 0, ST_UPPER = 1, ST_FREE = 2 };   // reference svm.cpp:425
+
+// arithmetic form of the kernel-row evaluation
+enum RowForm : int {
+    FORM_EXACT = 0,   // fp32 X, fp64 accumulation in feature order (matches the reference's Kernel::dot)
+    FORM_FP32 = 1,    // fp32 X, fp32 accumulation (the plain CUDA-core form)
+};
+
+struct KernelParams {
+    int type;         // LINEAR, POLY, RBF, SIGMOID
+    int degree;
+    double gamma;
+    double coef0;
+};
+
+// Feature rows on the device, shared by every instance built from the same problem.
+struct DevX {
+    const float *X;             // dense row-major [n_rows][ld] (nullptr for CSR)
+    int ld;                     // floats per dense row, multiple of 4
+    const long long *rowptr;    // CSR [n_rows+1]
+    const int *col;             // CSR 0-based column
+    const float *val;           // CSR value
+    int d;                      // number of feature columns
+    const double *xsq;          // [n_rows] dot(x,x) in the reference's order
+};
+
+// Q-row cache of one instance: `nsets` x `nways` slots of `stride` floats;
+// columns are indexed by the instance's LOCAL variable index (not position),
+// so shrinking permutations never move cached data.
+struct CacheView {
+    float *data;
+    int *tag;                   // [nslots] local row held, or kNoTag
+    int *epoch;                 // [nslots] active-set epoch the row is valid for, or kEpochFull
+    unsigned long long *stamp;  // [nslots] LRU clock
+    int nsets, nways;
+    long long stride;
+};
+
+struct GroupSync {
+    unsigned int count;
+    unsigned int gen;
+    int error;                  // nonzero: a wait timed out somewhere in the group
+    int pad[29];
+};
+
+// Cross-block reduction record (one per block per phase).  Besides the
+// reduced value and position it carries the winner's per-variable data
+// (alpha, QD, label, local index, row id) so that no block has to read
+// another block's chunk of the state arrays.
+struct Partial {
+    double v[8];
+    int n[8];
+    float q[2];
+    int pad[6];
+};
+static_assert(sizeof(Partial) == 128, "Partial must stay 128 bytes");
+
+struct SolveOut {
+    long long iters;
+    double rho, obj, r;
+    int status;                 // 0 ok, 1 max_iter reached, <0 error
+    int active_size;
+    int unshrink;
+    int nr_free;
+    double gap;                 // m(alpha) - M(alpha) at exit
+};
+
+struct InstanceDesc {
+    int l;
+    int nu;                     // 0: Solver (C-SVC), 1: Solver_NU
+    int shrinking;
+    int form;                   // RowForm
+    double Cp, Cn, eps;
+    long long max_iter;
+    KernelParams kp;
+    DevX x;
+    // position-indexed state (permuted by shrinking exactly like the reference)
+    double *G, *G_bar, *alpha, *p, *QD;
+    signed char *y;
+    unsigned char *status;
+    int *pos_local;             // position -> local index (cache column)
+    int *pos_row;               // position -> row id in DevX
+    // outputs
+    double *alpha_local;        // [l] final alpha by local index (unsigned, unscaled)
+    SolveOut *out;
+    // group
+    int block0, nblocks;
+    GroupSync *sync;
+    Partial *partials;          // [2][nblocks]
+    int *scratch;               // [2*l] shrink pair lists
+    CacheView cache;
+    // source-row staging in dynamic shared memory
+    int stage_cap;              // rows staged at once (1..kSrcBatch); 0: read sources from global memory
+    int stage_lds;              // floats per staged row (dense: ld; sparse: d)
+};
+
+}  // namespace svmb

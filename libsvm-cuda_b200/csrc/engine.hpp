@@ -1,0 +1,78 @@
+// engine.hpp -- host-side interface of the device solver (C++, internal).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+struct svm_node;
+
+namespace svmb {
+
+void set_error(const std::string &msg);
+const char *last_error();
+
+// Feature rows resident in HBM.  Dense when the matrix is dense enough,
+// otherwise CSR.  Row ids are the caller's row order.
+struct DeviceRows {
+    int n = 0;
+    int d = 0;                  // feature columns (max index)
+    int ld = 0;                 // dense row stride in floats
+    bool dense = false;
+    float *X = nullptr;
+    long long *rowptr = nullptr;
+    int *col = nullptr;
+    float *val = nullptr;
+    double *xsq[2] = {nullptr, nullptr};   // per RowForm
+    size_t bytes = 0;
+    ~DeviceRows();
+    DevX view(int form) const;
+};
+
+// Upload rows given as libsvm svm_node lists (index >= 1, terminated by -1).
+// force: -1 auto, 0 CSR, 1 dense.
+int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cudaStream_t s);
+// Upload rows given as host CSR arrays (0-based columns).
+int upload_csr(const long long *rowptr, const int *col, const float *val, int n, int d, DeviceRows &out,
+               int force, cudaStream_t s);
+
+struct SubProblem {
+    std::vector<int> rows;          // row id in DeviceRows per local variable
+    std::vector<signed char> y;     // +1 / -1
+    std::vector<double> alpha0;     // initial alpha
+    std::vector<double> p;          // linear term
+    double Cp = 1, Cn = 1;
+    int nu = 0;                     // Solver_NU
+};
+
+struct SolveParams {
+    KernelParams kp{2, 3, 0.0, 0.0};
+    double eps = 1e-3;
+    int shrinking = 1;
+    double cache_mb = 100;
+    int form = FORM_EXACT;
+    int blocks_override = 0;        // 0: heuristic
+};
+
+struct SolveResult {
+    std::vector<double> alpha;      // by local index (unsigned)
+    SolveOut out{};
+    double seconds = 0;
+};
+
+// Solve every subproblem in one persistent launch (instances get disjoint
+// groups of blocks).  Returns 0 on success.
+int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm,
+                std::vector<SolveResult> &res, cudaStream_t s);
+
+int device_sm_count();
+
+// device-side launchers (smo_kernel.cu)
+cudaError_t launch_xsq(const DevX &x, int n, double *out, int form, cudaStream_t s);
+cudaError_t launch_smo(int form, const InstanceDesc *d_insts, const int *d_block_inst, int nblocks,
+                       size_t dyn_smem, bool cooperative, cudaStream_t s);
+cudaError_t smo_max_blocks(int form, size_t dyn_smem, int *blocks_per_sm);
+
+}  // namespace svmb

@@ -1,0 +1,400 @@
+// predict_kernel.cu -- decision values of the reference's svm_predict_values
+// (reference libsvm/svm.cpp:2569-2643) for a batch of rows on the device.
+//
+// kvalue[t][s] = K(x_t, SV_s) with the prediction-time kernel of the reference
+// (Kernel::k_function, svm.cpp:327-384: RBF walks the squared difference over
+// the union of nonzero features in index order, no norm trick).  Each pair's
+// sum runs sequentially over the two classes' SVs in model order, exactly as
+// the reference, so decision values match it bit for bit on float inputs.
+// The file is compiled with -fmad=false.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "engine.hpp"
+#include "predict.hpp"
+
+namespace svmb {
+
+namespace {
+
+struct Rows {
+    // dense [n][ld] or CSR
+    float *X = nullptr;
+    long long *rowptr = nullptr;
+    int *col = nullptr;
+    float *val = nullptr;
+    int n = 0, ld = 0;
+    bool dense = true;
+    void release()
+    {
+        cudaFree(X); cudaFree(rowptr); cudaFree(col); cudaFree(val);
+        X = nullptr; rowptr = nullptr; col = nullptr; val = nullptr;
+    }
+};
+
+__device__ __forceinline__ double powi_p(double base, int times)
+{
+    double tmp = base, ret = 1.0;
+    for (int t = times; t > 0; t /= 2) {
+        if (t % 2 == 1) ret = __dmul_rn(ret, tmp);
+        tmp = __dmul_rn(tmp, tmp);
+    }
+    return ret;
+}
+
+struct KP {
+    int type, degree;
+    double gamma, coef0;
+};
+
+// kvalue for rows given as CSR in global memory (merge walks, svm.cpp:305-384)
+__device__ double kval_csr(const KP &kp, const long long *rpa, const int *ca, const float *va, int a,
+                           const long long *rpb, const int *cb, const float *vb, int b)
+{
+    long long e = rpa[a], ee = rpa[a + 1], f = rpb[b], ff = rpb[b + 1];
+    double sum = 0.0;
+    if (kp.type == 2) {
+        while (e < ee && f < ff) {
+            const int x = ca[e], y = cb[f];
+            if (x == y) {
+                const double d = __dsub_rn((double)va[e], (double)vb[f]);
+                sum = __dadd_rn(sum, __dmul_rn(d, d));
+                ++e; ++f;
+            } else if (x > y) {
+                sum = __dadd_rn(sum, __dmul_rn((double)vb[f], (double)vb[f]));
+                ++f;
+            } else {
+                sum = __dadd_rn(sum, __dmul_rn((double)va[e], (double)va[e]));
+                ++e;
+            }
+        }
+        for (; e < ee; ++e) sum = __dadd_rn(sum, __dmul_rn((double)va[e], (double)va[e]));
+        for (; f < ff; ++f) sum = __dadd_rn(sum, __dmul_rn((double)vb[f], (double)vb[f]));
+        return exp(__dmul_rn(-kp.gamma, sum));
+    }
+    while (e < ee && f < ff) {
+        const int x = ca[e], y = cb[f];
+        if (x == y) { sum = __dadd_rn(sum, __dmul_rn((double)va[e], (double)vb[f])); ++e; ++f; }
+        else if (x > y) ++f;
+        else ++e;
+    }
+    if (kp.type == 0) return sum;
+    if (kp.type == 1) return powi_p(__dadd_rn(__dmul_rn(kp.gamma, sum), kp.coef0), kp.degree);
+    return tanh(__dadd_rn(__dmul_rn(kp.gamma, sum), kp.coef0));
+}
+
+constexpr int kTT = 8;   // test rows per block (dense path)
+
+// dense path: block = kTT test rows (staged in smem) x 256 SVs (one per thread)
+__global__ void kvalue_dense(KP kp, const float *__restrict__ T, int nt, const float *__restrict__ S, int ns, int ld,
+                             double *__restrict__ out)
+{
+    extern __shared__ __align__(16) float tst[];
+    const int t0 = blockIdx.y * kTT;
+    const int tcount = min(kTT, nt - t0);
+    for (int k = threadIdx.x; k < kTT * ld; k += blockDim.x) {
+        const int tr = k / ld, c = k % ld;
+        tst[k] = tr < tcount ? T[(long long)(t0 + tr) * ld + c] : 0.0f;
+    }
+    __syncthreads();
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ns) return;
+    const float *sv = S + (long long)s * ld;
+    double acc[kTT];
+#pragma unroll
+    for (int k = 0; k < kTT; k++) acc[k] = 0.0;
+    for (int c = 0; c < ld; c += 4) {
+        const float4 w = __ldg(reinterpret_cast<const float4 *>(sv + c));
+        const float wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+#pragma unroll
+            for (int k = 0; k < kTT; k++) {
+                const float xv = tst[k * ld + c + q];
+                if (kp.type == 2) {
+                    const double d = __dsub_rn((double)xv, (double)wv[q]);
+                    acc[k] = __dadd_rn(acc[k], __dmul_rn(d, d));
+                } else {
+                    acc[k] = __dadd_rn(acc[k], __dmul_rn((double)xv, (double)wv[q]));
+                }
+            }
+        }
+    }
+    for (int k = 0; k < tcount; k++) {
+        double v;
+        if (kp.type == 2) v = exp(__dmul_rn(-kp.gamma, acc[k]));
+        else if (kp.type == 0) v = acc[k];
+        else if (kp.type == 1) v = powi_p(__dadd_rn(__dmul_rn(kp.gamma, acc[k]), kp.coef0), kp.degree);
+        else v = tanh(__dadd_rn(__dmul_rn(kp.gamma, acc[k]), kp.coef0));
+        out[(long long)(t0 + k) * ns + s] = v;
+    }
+}
+
+__global__ void kvalue_csr(KP kp, Rows T, Rows S, double *__restrict__ out)
+{
+    const long long total = (long long)T.n * S.n;
+    for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total; id += (long long)gridDim.x * blockDim.x) {
+        const int t = (int)(id / S.n), s = (int)(id % S.n);
+        out[id] = kval_csr(kp, T.rowptr, T.col, T.val, t, S.rowptr, S.col, S.val, s);
+    }
+}
+
+// one thread per (test row, pair): sequential sums in model order (svm.cpp:2606-2631)
+__global__ void pair_sums(const double *__restrict__ kv, int nt, int ns, int nr_class, const int *__restrict__ start,
+                          const int *__restrict__ nsv, const double *__restrict__ coef, const double *__restrict__ rho,
+                          double *__restrict__ dec)
+{
+    const int npair = nr_class * (nr_class - 1) / 2;
+    const long long total = (long long)nt * npair;
+    for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total; id += (long long)gridDim.x * blockDim.x) {
+        const int t = (int)(id / npair);
+        const int p = (int)(id % npair);
+        // pair index -> (i,j)
+        int i = 0, rem = p;
+        while (rem >= nr_class - 1 - i) { rem -= nr_class - 1 - i; ++i; }
+        const int j = i + 1 + rem;
+        const double *k = kv + (long long)t * ns;
+        const double *coef1 = coef + (long long)(j - 1) * ns;
+        const double *coef2 = coef + (long long)i * ns;
+        double sum = 0;
+        for (int q = 0; q < nsv[i]; q++) sum = __dadd_rn(sum, __dmul_rn(coef1[start[i] + q], k[start[i] + q]));
+        for (int q = 0; q < nsv[j]; q++) sum = __dadd_rn(sum, __dmul_rn(coef2[start[j] + q], k[start[j] + q]));
+        dec[id] = __dsub_rn(sum, rho[p]);
+    }
+}
+
+struct Session {
+    // fingerprint
+    const svm_node *const *SV = nullptr;
+    const double *coef0 = nullptr;
+    int l = 0, nr_class = 0;
+    double rho0 = 0;
+    // device copy
+    Rows sv;
+    int d = 0, base = 1;
+    double *coef = nullptr, *rho = nullptr;
+    int *start = nullptr, *nsv = nullptr;
+    void release()
+    {
+        sv.release();
+        cudaFree(coef); cudaFree(rho); cudaFree(start); cudaFree(nsv);
+        coef = rho = nullptr;
+        start = nsv = nullptr;
+    }
+};
+
+std::mutex g_mu;
+std::map<const svm_model *, std::unique_ptr<Session>> g_sessions;
+
+#define PK(call)                                                                  \
+    do {                                                                          \
+        cudaError_t e_ = (call);                                                  \
+        if (e_ != cudaSuccess) {                                                  \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));        \
+            return -1;                                                            \
+        }                                                                         \
+    } while (0)
+
+int upload_nodes(const svm_node *const *x, int n, int d, int base, bool dense, Rows &out)
+{
+    out.n = n;
+    out.dense = dense;
+    out.ld = (d + 3) & ~3;
+    if (out.ld == 0) out.ld = 4;
+    if (dense) {
+        std::vector<float> h((size_t)std::max(n, 1) * out.ld, 0.0f);
+        for (int r = 0; r < n; r++)
+            for (const svm_node *p = x[r]; p->index != -1; ++p) {
+                const int c = p->index - base;
+                if (c >= 0 && c < out.ld) h[(size_t)r * out.ld + c] = (float)p->value;
+            }
+        PK(cudaMalloc(&out.X, h.size() * sizeof(float)));
+        PK(cudaMemcpy(out.X, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<long long> rp(n + 1, 0);
+        std::vector<int> col;
+        std::vector<float> val;
+        for (int r = 0; r < n; r++) {
+            rp[r] = (long long)col.size();
+            for (const svm_node *p = x[r]; p->index != -1; ++p) {
+                col.push_back(p->index - base);
+                val.push_back((float)p->value);
+            }
+        }
+        rp[n] = (long long)col.size();
+        if (col.empty()) { col.push_back(0); val.push_back(0); }
+        PK(cudaMalloc(&out.rowptr, rp.size() * sizeof(long long)));
+        PK(cudaMalloc(&out.col, col.size() * sizeof(int)));
+        PK(cudaMalloc(&out.val, val.size() * sizeof(float)));
+        PK(cudaMemcpy(out.rowptr, rp.data(), rp.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        PK(cudaMemcpy(out.col, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice));
+        PK(cudaMemcpy(out.val, val.data(), val.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return 0;
+}
+
+Session *get_session(const svm_model *m)
+{
+    auto it = g_sessions.find(m);
+    if (it != g_sessions.end()) {
+        Session *s = it->second.get();
+        if (s->SV == m->SV && s->l == m->l && s->nr_class == m->nr_class &&
+            s->coef0 == (m->nr_class > 1 ? m->sv_coef[0] : nullptr) && s->rho0 == (m->nr_class > 1 ? m->rho[0] : 0.0))
+            return s;
+        s->release();
+        g_sessions.erase(it);
+    }
+    std::unique_ptr<Session> s(new Session());
+    s->SV = m->SV;
+    s->l = m->l;
+    s->nr_class = m->nr_class;
+    s->coef0 = m->nr_class > 1 ? m->sv_coef[0] : nullptr;
+    s->rho0 = m->nr_class > 1 ? m->rho[0] : 0.0;
+    int maxi = 0;
+    long long nnz = 0;
+    for (int i = 0; i < m->l; i++)
+        for (const svm_node *p = m->SV[i]; p->index != -1; ++p) { maxi = std::max(maxi, p->index); nnz++; }
+    s->base = 0;
+    s->d = maxi + 1;
+    const bool dense = m->l == 0 || (double)nnz >= 0.25 * (double)m->l * s->d || (double)m->l * s->d * 4 < 32e6;
+    if (upload_nodes(m->SV, m->l, s->d, s->base, dense, s->sv) != 0) return nullptr;
+    const int k = m->nr_class, npair = k * (k - 1) / 2;
+    std::vector<double> coef((size_t)std::max(k - 1, 1) * std::max(m->l, 1), 0.0);
+    for (int j = 0; j < k - 1; j++)
+        for (int i = 0; i < m->l; i++) coef[(size_t)j * m->l + i] = m->sv_coef[j][i];
+    std::vector<int> start(std::max(k, 1), 0), nsv(std::max(k, 1), 0);
+    for (int i = 0; i < k; i++) nsv[i] = m->nSV ? m->nSV[i] : 0;
+    for (int i = 1; i < k; i++) start[i] = start[i - 1] + nsv[i - 1];
+    std::vector<double> rho(std::max(npair, 1), 0.0);
+    for (int p = 0; p < npair; p++) rho[p] = m->rho[p];
+    if (cudaMalloc(&s->coef, coef.size() * 8) != cudaSuccess || cudaMalloc(&s->rho, rho.size() * 8) != cudaSuccess ||
+        cudaMalloc(&s->start, start.size() * 4) != cudaSuccess || cudaMalloc(&s->nsv, nsv.size() * 4) != cudaSuccess) {
+        set_error("device allocation for prediction failed");
+        s->release();
+        return nullptr;
+    }
+    cudaMemcpy(s->coef, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->start, start.data(), start.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->nsv, nsv.data(), nsv.size() * 4, cudaMemcpyHostToDevice);
+    Session *raw = s.get();
+    g_sessions[m] = std::move(s);
+    return raw;
+}
+
+}  // namespace
+
+void predict_forget(const svm_model *model)
+{
+    std::lock_guard<std::mutex> g(g_mu);
+    auto it = g_sessions.find(model);
+    if (it != g_sessions.end()) {
+        it->second->release();
+        g_sessions.erase(it);
+    }
+}
+
+int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double *labels, double *dec_out)
+{
+    if (m->param.svm_type != C_SVC && m->param.svm_type != NU_SVC) {
+        set_error("prediction supports C_SVC and NU_SVC models");
+        return -1;
+    }
+    if (m->param.kernel_type == PRECOMPUTED) {
+        set_error("precomputed kernels are not supported on the GPU");
+        return -1;
+    }
+    std::lock_guard<std::mutex> g(g_mu);
+    Session *s = get_session(m);
+    if (!s) return -1;
+    const int k = m->nr_class, npair = k * (k - 1) / 2;
+    if (n == 0) return 0;
+    KP kp{m->param.kernel_type, m->param.degree, m->param.gamma, m->param.coef0};
+    std::vector<double> dec((size_t)n * std::max(npair, 1), 0.0);
+    if (npair > 0 && m->l > 0) {
+        // chunk test rows so that the kvalue block stays below ~1 GB
+        const long long per_row = (long long)m->l * 8;
+        const int chunk = (int)std::max<long long>(1, std::min<long long>(n, (1LL << 30) / per_row));
+        double *kv = nullptr, *d_dec = nullptr;
+        PK(cudaMalloc(&kv, (size_t)chunk * per_row));
+        PK(cudaMalloc(&d_dec, (size_t)chunk * npair * 8));
+        for (int t0 = 0; t0 < n; t0 += chunk) {
+            const int tn = std::min(chunk, n - t0);
+            Rows T;
+            // test rows: features beyond the SVs' width cannot meet an SV feature in a
+            // dot product but still count in the RBF distance, so widen to cover them
+            int maxi = s->d - 1;
+            for (int r = 0; r < tn; r++)
+                for (const svm_node *p = rows[t0 + r]; p->index != -1; ++p) maxi = std::max(maxi, p->index);
+            const bool wider = maxi + 1 > s->d;
+            if (s->sv.dense && !wider) {
+                if (upload_nodes(rows + t0, tn, s->d, s->base, true, T) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
+                dim3 grid((m->l + 255) / 256, (tn + kTT - 1) / kTT);
+                const size_t smem = (size_t)kTT * s->sv.ld * sizeof(float);
+                if (smem > 200 * 1024) {
+                    T.release();
+                    set_error("feature dimension too large for the dense prediction path");
+                    cudaFree(kv); cudaFree(d_dec);
+                    return -1;
+                }
+                cudaFuncSetAttribute(kvalue_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                kvalue_dense<<<grid, 256, smem>>>(kp, T.X, tn, s->sv.X, m->l, s->sv.ld, kv);
+            } else {
+                Rows Sc = s->sv;
+                Rows svcsr;
+                if (s->sv.dense) {
+                    // a CSR copy of the SVs for the merge path
+                    if (upload_nodes(m->SV, m->l, s->d, s->base, false, svcsr) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
+                    Sc = svcsr;
+                }
+                if (upload_nodes(rows + t0, tn, maxi + 1, s->base, false, T) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
+                kvalue_csr<<<std::min<long long>(((long long)tn * m->l + 255) / 256, 148 * 16), 256>>>(kp, T, Sc, kv);
+                if (s->sv.dense) {
+                    cudaDeviceSynchronize();
+                    svcsr.release();
+                }
+            }
+            pair_sums<<<std::min<long long>(((long long)tn * npair + 127) / 128, 148 * 8), 128>>>(kv, tn, m->l, k, s->start, s->nsv, s->coef, s->rho, d_dec);
+            cudaError_t e = cudaDeviceSynchronize();
+            T.release();
+            if (e != cudaSuccess) {
+                set_error(std::string("prediction kernels failed: ") + cudaGetErrorString(e));
+                cudaFree(kv); cudaFree(d_dec);
+                return -1;
+            }
+            PK(cudaMemcpy(dec.data() + (size_t)t0 * npair, d_dec, (size_t)tn * npair * 8, cudaMemcpyDeviceToHost));
+        }
+        cudaFree(kv);
+        cudaFree(d_dec);
+    } else if (npair > 0) {
+        for (int t = 0; t < n; t++)
+            for (int p = 0; p < npair; p++) dec[(size_t)t * npair + p] = -m->rho[p];
+    }
+    // votes, ties to the lowest class index (svm.cpp:2627-2637)
+    for (int t = 0; t < n; t++) {
+        std::vector<int> vote(std::max(k, 1), 0);
+        int p = 0;
+        for (int i = 0; i < k; i++)
+            for (int j = i + 1; j < k; j++) {
+                if (dec[(size_t)t * npair + p] > 0) ++vote[i];
+                else ++vote[j];
+                p++;
+            }
+        int best = 0;
+        for (int i = 1; i < k; i++)
+            if (vote[i] > vote[best]) best = i;
+        labels[t] = m->label ? m->label[best] : 0;
+        if (dec_out)
+            for (int q = 0; q < npair; q++) dec_out[(size_t)t * npair + q] = dec[(size_t)t * npair + q];
+    }
+    return 0;
+}
+
+}  // namespace svmb
