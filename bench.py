@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SVM engine: batched one-vs-one RBF training.
+
+Workload (one step): the 45 binary C-SVC subproblems of a 10-class problem
+(class sizes 12000*0.8^k, k=0..9, 53,646 rows, d=256, Gaussian classes at
+N(0,4) centres with unit std), RBF gamma=1/256, C=1, eps=1e-3, 100 MB Q-cache
+per subproblem, shrinking on.  All 45 solves run in ONE persistent launch.
+Synthetic, seeded data; no dataset is read.
+
+  value  solves/s with the rows resident in HBM (svmb_rows_solve_many)
+  e2e    solves/s through svm_train() -- the public svm.h API -- from host
+         svm_node buffers in pinned memory: upload, all pairs, model assembly
+  --impl reference   the reference's own CPU solver (oracle/_ref/libsvm_ref.so,
+         built from the reference sources) on the same 45 subproblems, one
+         process per host core.
+
+Multi-GPU: the workload does not shard; every rank solves its own replica of
+the batch (weak scaling, no collective on the data path).  Timing is CUDA
+events on the launching stream, max over ranks.  L2 is flushed (256 MiB
+write) between timed steps.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "libsvm-cuda_b200"))
+
+import numpy as np  # noqa: E402
+
+from svmb200 import cabi, datagen  # noqa: E402
+
+WORKLOAD = "ovo45_rbf_d256: 10 classes 12000*0.8^k (53646 rows), d=256, RBF g=1/256, C=1, eps=1e-3, 100MB cache/solve"
+D = 256
+GAMMA = 1.0 / 256
+CVAL = 1.0
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_problem(seed=4):
+    tr, _, sizes = datagen.multiclass_geo(n_classes=10, largest=12000, ratio=0.8, d=D, seed=seed)
+    return tr, sizes
+
+
+def pair_instances(p):
+    """The one-vs-one subproblems exactly as svm_train forms them (reference
+    svm.cpp:2081-2154 class grouping, :2260-2295 pairs): classes in order of
+    first occurrence, rows of class i (+1) then class j (-1)."""
+    labels = []
+    for v in p.y:
+        if v not in labels:
+            labels.append(v)
+    members = [np.nonzero(p.y == lab)[0].astype(np.int32) for lab in labels]
+    rows, ys = [], []
+    for i in range(len(labels)):
+        for j in range(i + 1, len(labels)):
+            rows.append(np.concatenate([members[i], members[j]]))
+            ys.append(np.concatenate([np.ones(len(members[i])), -np.ones(len(members[j]))]))
+    return rows, ys
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index, path):
+        self.path, self.proc = path, None
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# reference arm: the reference's own CPU solver, one process per core
+# ----------------------------------------------------------------------------
+_W = {}
+
+
+def _ref_worker_init():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    lib = oracle_py.reference_lib()
+    if lib is None:
+        raise RuntimeError("oracle/_ref/libsvm_ref.so is not built")
+    quiet = cabi.PRINT_FUNC(lambda s: None)
+    lib.svm_set_print_string_function(quiet)
+    lib.svm_free_and_destroy_model.argtypes = [C.POINTER(C.POINTER(cabi.svm_model))]
+    p, _ = make_problem()
+    rows, ys = pair_instances(p)
+    _W.update(lib=lib, quiet=quiet, p=p, rows=rows, ys=ys)
+
+
+def _ref_solve_pair(k):
+    """One binary subproblem through the reference's svm_train (C-SVC, RBF)."""
+    lib, p = _W["lib"], _W["p"]
+    sub = p.take(_W["rows"][k])
+    sub.y = _W["ys"][k]
+    nodes = cabi.NodeRows(sub)
+    prm = cabi.make_param(svm_type=0, kernel_type=2, gamma=GAMMA, C_=CVAL, cache_size=100.0, eps=1e-3, shrinking=1,
+                          cuda_flag=0)
+    t0 = time.perf_counter()
+    m = lib.svm_train(C.byref(nodes.prob), C.byref(prm))
+    dt = time.perf_counter() - t0
+    nsv = m.contents.l
+    lib.svm_free_and_destroy_model(C.byref(m))
+    return k, dt, nsv
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    npairs = 45
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(processes=min(cores, npairs), initializer=_ref_worker_init) as pool:
+        times = []
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_ref_solve_pair, range(npairs), chunksize=1)
+            dt = time.perf_counter() - t0
+            if step >= args.warmup:
+                times.append(dt)
+    mean = sum(times) / len(times)
+    value = npairs / mean
+    line = {
+        "impl": "reference", "metric": "batched_solves_per_s", "value": value, "unit": "solves/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "instances_per_step": npairs, "parallelism": f"{min(cores, npairs)} processes"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": min(cores, npairs), "kind": "reference",
+                         "sample": f"all {npairs} one-vs-one subproblems per step, reference svm_train (CPU, libsvm 3.18 "
+                                   f"from the reference sources), one process per subproblem on {min(cores, npairs)} cores"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+def cpu_baseline_sample(p, rows, ys, budget_s=20.0):
+    """The reference's CPU solver (single core) on a seeded random sample of the
+    45 subproblems, until ~budget_s of CPU work: solves/s of that sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    lib = oracle_py.reference_lib()
+    if lib is None:
+        return None
+    quiet = cabi.PRINT_FUNC(lambda s: None)
+    lib.svm_set_print_string_function(quiet)
+    order = np.random.default_rng(12345).permutation(len(rows))
+    done, spent = 0, 0.0
+    for k in order:
+        sub = p.take(rows[k])
+        sub.y = ys[k]
+        nodes = cabi.NodeRows(sub)
+        prm = cabi.make_param(svm_type=0, kernel_type=2, gamma=GAMMA, C_=CVAL, cache_size=100.0, eps=1e-3,
+                              shrinking=1, cuda_flag=0)
+        t0 = time.perf_counter()
+        m = lib.svm_train(C.byref(nodes.prob), C.byref(prm))
+        spent += time.perf_counter() - t0
+        lib.svm_free_and_destroy_model(C.byref(m))
+        done += 1
+        if spent >= budget_s:
+            break
+    return {"value": done / spent, "unit": "solves/s", "cores": 1, "kind": "reference",
+            "sample": f"{done} of the 45 subproblems (seeded random order), reference svm_train on 1 core, {spent:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import torch
+    import torch.distributed as dist
+    from svmb200 import Engine
+    from svmb200.lib import ResidentRows, make_params
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    eng = Engine()
+    if not eng.available():
+        raise SystemExit("no CUDA device")
+
+    p, sizes = make_problem(seed=4 + rank)
+    rows, ys = pair_instances(p)
+    params = [make_params(svm_type=0, kernel_type=2, gamma=GAMMA, C_pos=CVAL, eps=1e-3, cache_mb=100.0, shrinking=1)
+              for _ in rows]
+    res = ResidentRows(eng, p)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------- value: resident rows ----------------
+    for _ in range(args.warmup):
+        res.solve_many(rows, ys, params)
+    clocks = Clocks(local, os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")) if os.path.isdir(
+        os.path.join(ROOT, "gpurun_out")) else Clocks(local, f"/tmp/svmb_clocks_{rank}.csv")
+    step_ms, kern_s, alg_bytes, stats_all = [], [], [], []
+    launches0 = eng.launches()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        alphas, stats = res.solve_many(rows, ys, params)
+        e1.record()
+        barrier()
+        step_ms.append(e0.elapsed_time(e1))
+        kern_s.append(stats[0]["seconds"])
+        # algorithmic bytes of the launch: per iteration 46 B per active position
+        # (WSS 22 B + update 24 B), per kernel value evaluated one stored row + 4 B
+        row_bytes = res.bytes / max(res.n, 1)
+        alg_bytes.append(sum(46.0 * s["sum_active"] + s["q_evals"] * (row_bytes + 4.0) for s in stats))
+        stats_all.append(stats)
+    launches = eng.launches() - launches0
+    clk = clocks.stop()
+    t = torch.tensor([max(step_ms)], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    mean_ms = sum(step_ms) / len(step_ms)
+    if world > 1:
+        tm = torch.tensor([mean_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        mean_ms = float(tm.item())
+    solves_per_step = len(rows) * world
+    value = solves_per_step / (mean_ms * 1e-3)
+
+    # ---------------- e2e: svm_train from host buffers ----------------
+    prm = cabi.make_param(svm_type=0, kernel_type=2, gamma=GAMMA, C_=CVAL, cache_size=100.0, eps=1e-3, shrinking=1)
+    nodes = cabi.NodeRows(p)
+    # move the svm_node buffer into pinned memory
+    pinned = torch.empty(nodes.buf.nbytes, dtype=torch.uint8).pin_memory()
+    pinned.numpy()[:] = nodes.buf.view(np.uint8)
+    base = pinned.data_ptr()
+    starts = (nodes.addrs - nodes.buf.ctypes.data) + base
+    ptrs = np.ascontiguousarray(starts.astype(np.uint64))
+    yv = np.ascontiguousarray(p.y, dtype=np.float64)
+    prob = cabi.svm_problem()
+    prob.l = p.n
+    prob.y = yv.ctypes.data_as(C.POINTER(C.c_double))
+    prob.x = C.cast(ptrs.ctypes.data, C.POINTER(C.POINTER(cabi.svm_node)))
+    for _ in range(args.warmup):
+        m = eng.lib.svm_train(C.byref(prob), C.byref(prm))
+        eng.lib.svm_free_and_destroy_model(C.byref(m))
+    e2e_ms, h2d, d2h = [], [], []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        barrier()
+        hb0, db0 = C.c_longlong(), C.c_longlong()
+        eng.lib.svmb_transfer_bytes(C.byref(hb0), C.byref(db0))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        m = eng.lib.svm_train(C.byref(prob), C.byref(prm))
+        nsv_total = m.contents.l            # the model (results) is in host memory here
+        e1.record()
+        barrier()
+        hb1, db1 = C.c_longlong(), C.c_longlong()
+        eng.lib.svmb_transfer_bytes(C.byref(hb1), C.byref(db1))
+        e2e_ms.append(e0.elapsed_time(e1))
+        h2d.append(hb1.value - hb0.value)
+        d2h.append(db1.value - db0.value)
+        eng.lib.svm_free_and_destroy_model(C.byref(m))
+    e2e_mean = sum(e2e_ms) / len(e2e_ms)
+    if world > 1:
+        tm = torch.tensor([e2e_mean], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        e2e_mean = float(tm.item())
+
+    # ---------------- batched vs largest subproblem alone ----------------
+    big = int(np.argmax([len(r) for r in rows]))
+    alone = []
+    for _ in range(3):
+        _, st = res.solve_many([rows[big]], [ys[big]], [params[big]])
+        alone.append(st[0]["seconds"])
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        kavg = sum(kern_s) / len(kern_s)
+        abytes = sum(alg_bytes) / len(alg_bytes)
+        achieved = abytes / kavg / 1e9
+        iters = [s["iters"] for s in stats_all[-1]]
+        cpu = None if args.no_cpu_baseline else cpu_baseline_sample(p, rows, ys)
+        line = {
+            "metric": "batched_solves_per_s", "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "rows": p.n, "d": D, "instances_per_step": len(rows),
+                       "pair_sizes": [int(min(len(r) for r in rows)), int(max(len(r) for r in rows))],
+                       "l2": "flushed between timed steps (256 MiB write); rows 55 MB < L2",
+                       "parallelism": f"replicas x{world} (no data-path collective)"},
+            "e2e": {"value": solves_per_step / (e2e_mean * 1e-3), "unit": "solves/s",
+                    "h2d_bytes_per_step": int(sum(h2d) / len(h2d)), "d2h_bytes_per_step": int(sum(d2h) / len(d2h)),
+                    "api": "svm_train (svm.h) from pinned host svm_node rows"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "kernel": "smo_persistent<FORM_EXACT>",
+                         "algorithmic_bytes_per_launch": abytes, "kernel_ms": kavg * 1e3,
+                         "peak_kind": f"{peak_kind} hbm_gbs"},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": int(launches),
+            "iters_total": int(sum(iters)), "iters_max": int(max(iters)),
+            "largest_alone_ms": min(alone) * 1e3, "batched_over_largest": kavg / min(alone),
+        }
+        print(json.dumps(line), flush=True)
+    res.free()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

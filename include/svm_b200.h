@@ -35,7 +35,14 @@ typedef struct svmb_solve_stats {
     int status;          /* 0 converged, 1 max_iter reached */
     int active_size;     /* active set size at exit (shrinking) */
     int pad;
-    double seconds;      /* device time of the launch that solved it */
+    double seconds;      /* device time (CUDA events) of the launch that solved it */
+    /* work counters of the solve: sum over iterations of the active-set size,
+     * kernel values evaluated, Q-row cache lookups and hits */
+    long long sum_active;
+    long long q_evals;
+    long long lookups;
+    long long hits;
+    long long prof_cycles[8];   /* SM cycles per loop section (diagnostics) */
 } svmb_solve_stats;
 
 /* Parameters of a binary solve (the subset of svm_parameter the solver reads). */
@@ -59,6 +66,10 @@ typedef struct svmb_params {
 #define SVMB_FORM_FP32  1   /* fp32 features, fp32 accumulation (plain CUDA-core form) */
 
 const char *svmb_last_error(void);
+/* Number of device kernels this library has launched in this process. */
+long long svmb_kernel_launches(void);
+/* Bytes this library has copied host->device and device->host in this process. */
+void svmb_transfer_bytes(long long *h2d, long long *d2h);
 int svmb_version(void);                         /* LIBSVM_VERSION * 100 + engine revision */
 int svmb_device_available(void);                /* 1 if a CUDA device can be used */
 

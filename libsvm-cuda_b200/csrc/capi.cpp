@@ -125,6 +125,11 @@ int solve_many(const svmb::DeviceRows &rows, int ninst, const int *inst_ptr, con
             st.status = R.out.status;
             st.active_size = R.out.active_size;
             st.seconds = R.seconds;
+            st.sum_active = R.out.sum_active;
+            st.q_evals = R.out.q_evals;
+            st.lookups = R.out.lookups;
+            st.hits = R.out.hits;
+            for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
             for (int i = 0; i < l; i++) {
                 const double v = alpha_out[a + i];
                 if (v != 0) {
@@ -142,6 +147,8 @@ int solve_many(const svmb::DeviceRows &rows, int ninst, const int *inst_ptr, con
 extern "C" {
 
 const char *svmb_last_error(void) { return svmb::last_error(); }
+long long svmb_kernel_launches(void) { return svmb::launch_count(); }
+void svmb_transfer_bytes(long long *h2d, long long *d2h) { svmb::transfer_bytes(h2d, d2h); }
 int svmb_version(void) { return LIBSVM_VERSION * 100 + 1; }
 
 int svmb_device_available(void)

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 
 #include "svm.h"
@@ -32,6 +33,52 @@ const char *last_error() { return g_last_error.c_str(); }
             return -1;                                                                    \
         }                                                                                 \
     } while (0)
+
+static std::atomic<long long> g_launches{0};
+static std::atomic<long long> g_h2d{0}, g_d2h{0};
+void count_launch(long long n) { g_launches += n; }
+long long launch_count() { return g_launches.load(); }
+void transfer_bytes(long long *h2d, long long *d2h)
+{
+    if (h2d) *h2d = g_h2d.load();
+    if (d2h) *d2h = g_d2h.load();
+}
+
+// host<->device copies, counted per direction
+cudaError_t xfer_async(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s)
+{
+    if (kind == cudaMemcpyHostToDevice) g_h2d += (long long)bytes;
+    if (kind == cudaMemcpyDeviceToHost) g_d2h += (long long)bytes;
+    return cudaMemcpyAsync(dst, src, bytes, kind, s);
+}
+cudaError_t xfer(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind)
+{
+    if (kind == cudaMemcpyHostToDevice) g_h2d += (long long)bytes;
+    if (kind == cudaMemcpyDeviceToHost) g_d2h += (long long)bytes;
+    return cudaMemcpy(dst, src, bytes, kind);
+}
+
+// Page-locked staging for row uploads, grown on demand and reused by later
+// calls (copies from it run at full PCIe/C2C bandwidth).
+namespace {
+std::mutex g_pin_mu;
+void *g_pin = nullptr;
+size_t g_pin_bytes = 0;
+}  // namespace
+void *pinned_staging(size_t bytes)
+{
+    if (bytes <= g_pin_bytes) return g_pin;
+    if (g_pin) cudaFreeHost(g_pin);
+    g_pin = nullptr;
+    g_pin_bytes = 0;
+    size_t want = std::max<size_t>(bytes, 1 << 20);
+    if (cudaHostAlloc(&g_pin, want, cudaHostAllocDefault) != cudaSuccess) {
+        g_pin = nullptr;
+        return nullptr;
+    }
+    g_pin_bytes = want;
+    return g_pin;
+}
 
 int device_sm_count()
 {
@@ -76,33 +123,42 @@ int upload_csr(const long long *rowptr, const int *col, const float *val, int n,
     out.d = d > 0 ? d : 1;
     const long long nnz = rowptr[n];
     out.ld = (out.d + 3) & ~3;
+    // Dense rows only when they are not larger than the CSR arrays: a kernel
+    // row streams the whole stored row of every active position, so the byte
+    // count is what matters.
     const double dense_bytes = (double)n * out.ld * 4.0;
-    const double density = n > 0 ? (double)nnz / ((double)n * out.d) : 1.0;
-    bool dense = force == 1 || (force < 0 && (density >= 0.25 || dense_bytes <= 64.0 * (1 << 20)));
+    const double csr_bytes = (double)(n + 1) * 8.0 + (double)nnz * 8.0;
+    bool dense = force == 1 || (force < 0 && dense_bytes <= 1.2 * csr_bytes);
     if (dense && dense_bytes > 60e9) dense = false;
     out.dense = dense;
+    // the CSR arrays always travel; dense rows are scattered on the device
+    CK(cudaMalloc(&out.rowptr, (size_t)(n + 1) * sizeof(long long)));
+    CK(cudaMalloc(&out.col, (size_t)std::max<long long>(nnz, 1) * sizeof(int)));
+    CK(cudaMalloc(&out.val, (size_t)std::max<long long>(nnz, 1) * sizeof(float)));
+    CK(xfer_async(out.rowptr, rowptr, (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
+    if (nnz) {
+        CK(xfer_async(out.col, col, (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(xfer_async(out.val, val, (size_t)nnz * sizeof(float), cudaMemcpyHostToDevice, s));
+    }
+    out.h2d_bytes = (size_t)(n + 1) * 8 + (size_t)nnz * 8;
     if (dense) {
-        std::vector<float> h((size_t)n * out.ld, 0.0f);
-        for (int r = 0; r < n; r++)
-            for (long long e = rowptr[r]; e < rowptr[r + 1]; e++) h[(size_t)r * out.ld + col[e]] = val[e];
-        CK(cudaMalloc(&out.X, std::max<size_t>(h.size(), 4) * sizeof(float)));
-        if (!h.empty()) CK(cudaMemcpyAsync(out.X, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, s));
-        out.bytes = h.size() * sizeof(float);
-        CK(cudaStreamSynchronize(s));
-    } else {
-        CK(cudaMalloc(&out.rowptr, (size_t)(n + 1) * sizeof(long long)));
-        CK(cudaMalloc(&out.col, (size_t)std::max<long long>(nnz, 1) * sizeof(int)));
-        CK(cudaMalloc(&out.val, (size_t)std::max<long long>(nnz, 1) * sizeof(float)));
-        CK(cudaMemcpyAsync(out.rowptr, rowptr, (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
-        if (nnz) {
-            CK(cudaMemcpyAsync(out.col, col, (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, s));
-            CK(cudaMemcpyAsync(out.val, val, (size_t)nnz * sizeof(float), cudaMemcpyHostToDevice, s));
+        const size_t elems = std::max<size_t>((size_t)n * out.ld, 4);
+        CK(cudaMalloc(&out.X, elems * sizeof(float)));
+        CK(cudaMemsetAsync(out.X, 0, elems * sizeof(float), s));
+        if (n) {
+            CK(launch_scatter_dense(out.rowptr, out.col, out.val, n, out.ld, out.X, s));
+            count_launch();
         }
+        out.bytes = (size_t)n * out.ld * sizeof(float);
+    } else {
         out.bytes = (size_t)(n + 1) * 8 + (size_t)nnz * 8;
     }
     for (int f = 0; f < 2; f++) {
         CK(cudaMalloc(&out.xsq[f], (size_t)std::max(n, 1) * sizeof(double)));
-        if (n) CK(launch_xsq(out.view(f), n, out.xsq[f], f, s));
+        if (n) {
+            CK(launch_xsq(out.view(f), n, out.xsq[f], f, s));
+            count_launch();
+        }
     }
     CK(cudaStreamSynchronize(s));
     return 0;
@@ -124,9 +180,18 @@ int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cud
         return -1;
     }
     const int base = (nnz && min_index == 0) ? 0 : 1;
-    std::vector<long long> rp((size_t)n + 1, 0);
-    std::vector<int> col((size_t)nnz);
-    std::vector<float> val((size_t)nnz);
+    // CSR arrays built directly in page-locked staging memory
+    std::lock_guard<std::mutex> g(g_pin_mu);
+    const size_t bytes = ((size_t)n + 1) * 8 + (size_t)nnz * 8 + 64;
+    char *pin = (char *)pinned_staging(bytes);
+    std::vector<char> fallback;
+    if (!pin) {
+        fallback.resize(bytes);
+        pin = fallback.data();
+    }
+    long long *rp = (long long *)pin;
+    int *col = (int *)(pin + (((size_t)n + 1) * 8));
+    float *val = (float *)(pin + (((size_t)n + 1) * 8) + (size_t)nnz * 4);
     long long k = 0;
     for (int r = 0; r < n; r++) {
         rp[r] = k;
@@ -138,7 +203,7 @@ int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cud
     }
     rp[n] = k;
     const int d = nnz ? max_index - base + 1 : 1;
-    return upload_csr(rp.data(), col.data(), val.data(), n, d, out, force, s);
+    return upload_csr(rp, col, val, n, d, out, force, s);
 }
 
 namespace {
@@ -173,54 +238,93 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         set_error("no CUDA device");
         return -1;
     }
-    // shared-memory staging of source rows
+    // Shared memory of a block: [source staging][chunk state, kChunkBytes per position].
+    constexpr int kChunkBytes = 3 * 8 + 2 * 4 + 2;     // G, alpha, QD, col, row, y, status
+    int smem_total = 0, dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&smem_total, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const long long budget = (long long)smem_total - smo_static_smem() - 1024;
     int stage_cap, stage_lds;
     if (rows.dense) {
         stage_lds = rows.ld;
-        stage_cap = (int)std::min<long long>(kSrcBatch, (100LL << 10) / ((long long)rows.ld * 4));
+        stage_cap = (int)std::min<long long>(kSrcBatch, (48LL << 10) / ((long long)rows.ld * 4));
     } else {
         stage_lds = rows.d;
-        stage_cap = (int)std::min<long long>(kSrcBatch, (180LL << 10) / ((long long)std::max(rows.d, 1) * 4));
+        stage_cap = (int)std::min<long long>(kSrcBatch, (budget / 2) / ((long long)std::max(rows.d, 1) * 4));
     }
     if (stage_cap < 2) stage_cap = 0;
-    const size_t dyn_smem = (size_t)stage_cap * stage_lds * sizeof(float);
+    const long long stage_bytes = (((long long)stage_cap * stage_lds * 4) + 15) & ~15LL;
+    const long long chunk_max = (budget - stage_bytes) / kChunkBytes;
+    if (chunk_max < 64) {
+        set_error("not enough shared memory for the solver state");
+        return -1;
+    }
+    const size_t max_dyn = (size_t)(stage_bytes + chunk_max * kChunkBytes);
     int per_sm = 0;
-    CK(smo_max_blocks(prm.form, dyn_smem, &per_sm));
+    CK(smo_max_blocks(prm.form, max_dyn, &per_sm));
     if (per_sm < 1) {
         set_error("solver kernel does not fit on an SM");
         return -1;
     }
     const int capacity = per_sm * sms;
+    for (const SubProblem &sp : subs)
+        if ((long long)sp.rows.size() > chunk_max * capacity) {
+            set_error("problem too large: more positions than the device's blocks can hold in shared memory");
+            return -1;
+        }
 
     // process instances in waves that fit the co-resident capacity
     int first = 0;
     while (first < ninst) {
-        // choose the wave and the blocks per instance (proportional to l, >= 1)
+        // blocks per instance: enough to hold the state in shared memory, more
+        // for large problems, shared proportionally when instances run together
         std::vector<int> nb;
-        long long total_l = 0;
+        long long total_l = 0, need = 0;
         int last = first;
-        while (last < ninst && (last - first) < capacity) total_l += subs[last++].rows.size();
+        while (last < ninst) {
+            const long long l = (long long)subs[last].rows.size();
+            const long long nmin = std::max<long long>(1, (l + chunk_max - 1) / chunk_max);
+            if (need + nmin > capacity) break;
+            need += nmin;
+            total_l += l;
+            last++;
+        }
         const int count = last - first;
         nb.assign(count, 1);
         for (int k = 0; k < count; k++) {
             const long long l = (long long)subs[first + k].rows.size();
+            const int nmin = (int)std::max<long long>(1, (l + chunk_max - 1) / chunk_max);
             int want;
             if (prm.blocks_override > 0) want = prm.blocks_override;
-            else want = (int)std::max<long long>(1, std::min<long long>(sms, l / 2048));
-            // share the device proportionally when several instances run together
+            else want = (int)std::max<long long>(1, std::min<long long>(sms, (l + 1499) / 1500));
             if (count > 1) {
-                long long share = (long long)std::floor((double)capacity * (double)l / (double)std::max<long long>(total_l, 1));
-                want = (int)std::max<long long>(1, std::min<long long>(want, share));
+                const long long share = (long long)std::floor((double)capacity * (double)l / (double)std::max<long long>(total_l, 1));
+                want = (int)std::min<long long>(want, std::max<long long>(1, share));
             }
-            nb[k] = want;
+            want = (int)std::min<long long>(want, std::max<long long>(1, l));
+            nb[k] = std::max(want, nmin);
         }
         int used = 0;
         for (int v : nb) used += v;
         while (used > capacity) {
-            int big = (int)(std::max_element(nb.begin(), nb.end()) - nb.begin());
+            // trim the instance with the most blocks above its minimum
+            int big = -1;
+            long long slack = 0;
+            for (int k = 0; k < count; k++) {
+                const long long l = (long long)subs[first + k].rows.size();
+                const long long nmin = std::max<long long>(1, (l + chunk_max - 1) / chunk_max);
+                if (nb[k] - nmin > slack) { slack = nb[k] - nmin; big = k; }
+            }
+            if (big < 0) break;
             nb[big]--;
             used--;
         }
+        long long chunk_cap = 1;
+        for (int k = 0; k < count; k++) {
+            const long long l = (long long)subs[first + k].rows.size();
+            chunk_cap = std::max<long long>(chunk_cap, (l + nb[k] - 1) / nb[k]);
+        }
+        const size_t dyn_smem = (size_t)(stage_bytes + chunk_cap * kChunkBytes);
 
         std::vector<InstanceAlloc> allocs(count);
         std::vector<InstanceDesc> desc(count);
@@ -245,6 +349,7 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
             D.nblocks = nb[k];
             D.stage_cap = stage_cap;
             D.stage_lds = stage_lds;
+            D.chunk_cap = (int)chunk_cap;
             for (int b = 0; b < nb[k]; b++) block_inst[b0 + b] = k;
             b0 += nb[k];
             // cache geometry: rows of l floats, at least 4, at most 2l slots
@@ -296,12 +401,13 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
             // initial state
             std::vector<int> iota(l);
             for (int q = 0; q < l; q++) iota[q] = q;
-            CK(cudaMemcpyAsync(D.alpha, sp.alpha0.data(), sizeof(double) * l, cudaMemcpyHostToDevice, s));
-            CK(cudaMemcpyAsync(D.p, sp.p.data(), sizeof(double) * l, cudaMemcpyHostToDevice, s));
-            CK(cudaMemcpyAsync(D.y, sp.y.data(), l, cudaMemcpyHostToDevice, s));
-            CK(cudaMemcpyAsync(D.pos_local, iota.data(), sizeof(int) * l, cudaMemcpyHostToDevice, s));
-            CK(cudaMemcpyAsync(D.pos_row, sp.rows.data(), sizeof(int) * l, cudaMemcpyHostToDevice, s));
+            CK(xfer_async(D.alpha, sp.alpha0.data(), sizeof(double) * l, cudaMemcpyHostToDevice, s));
+            CK(xfer_async(D.p, sp.p.data(), sizeof(double) * l, cudaMemcpyHostToDevice, s));
+            CK(xfer_async(D.y, sp.y.data(), l, cudaMemcpyHostToDevice, s));
+            CK(xfer_async(D.pos_local, iota.data(), sizeof(int) * l, cudaMemcpyHostToDevice, s));
+            CK(xfer_async(D.pos_row, sp.rows.data(), sizeof(int) * l, cudaMemcpyHostToDevice, s));
             CK(cudaMemsetAsync(D.sync, 0, sizeof(GroupSync), s));
+            CK(cudaMemsetAsync(D.partials, 0, sizeof(Partial) * 2 * (size_t)nb[k], s));
             CK(cudaMemsetAsync(D.cache.tag, 0xff, sizeof(int) * (size_t)sets * ways, s));
             CK(cudaMemsetAsync(D.cache.epoch, 0, sizeof(int) * (size_t)sets * ways, s));
             CK(cudaMemsetAsync(D.cache.stamp, 0, sizeof(unsigned long long) * (size_t)sets * ways, s));
@@ -310,12 +416,20 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         int *d_block_inst = nullptr;
         CK(cudaMalloc(&d_desc, sizeof(InstanceDesc) * count));
         CK(cudaMalloc(&d_block_inst, sizeof(int) * used));
-        CK(cudaMemcpyAsync(d_desc, desc.data(), sizeof(InstanceDesc) * count, cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(d_block_inst, block_inst.data(), sizeof(int) * used, cudaMemcpyHostToDevice, s));
-        auto t0 = std::chrono::steady_clock::now();
+        CK(xfer_async(d_desc, desc.data(), sizeof(InstanceDesc) * count, cudaMemcpyHostToDevice, s));
+        CK(xfer_async(d_block_inst, block_inst.data(), sizeof(int) * used, cudaMemcpyHostToDevice, s));
+        cudaEvent_t ev0, ev1;
+        CK(cudaEventCreate(&ev0));
+        CK(cudaEventCreate(&ev1));
+        CK(cudaEventRecord(ev0, s));
         cudaError_t le = launch_smo(prm.form, d_desc, d_block_inst, used, dyn_smem, true, s);
+        if (le == cudaSuccess) count_launch();
+        cudaEventRecord(ev1, s);
         cudaError_t se = le == cudaSuccess ? cudaStreamSynchronize(s) : le;
-        auto t1 = std::chrono::steady_clock::now();
+        float ms = 0;
+        if (se == cudaSuccess) cudaEventElapsedTime(&ms, ev0, ev1);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
         int rc = 0;
         if (se != cudaSuccess) {
             set_error(std::string("solver launch failed: ") + cudaGetErrorString(se));
@@ -325,13 +439,13 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
             SolveResult &R = res[first + k];
             const int l = desc[k].l;
             R.alpha.resize(l);
-            if (cudaMemcpy(R.alpha.data(), desc[k].alpha_local, sizeof(double) * l, cudaMemcpyDeviceToHost) != cudaSuccess ||
-                cudaMemcpy(&R.out, desc[k].out, sizeof(SolveOut), cudaMemcpyDeviceToHost) != cudaSuccess) {
+            if (xfer(R.alpha.data(), desc[k].alpha_local, sizeof(double) * l, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                xfer(&R.out, desc[k].out, sizeof(SolveOut), cudaMemcpyDeviceToHost) != cudaSuccess) {
                 set_error("copy of solver results failed");
                 rc = -1;
                 break;
             }
-            R.seconds = std::chrono::duration<double>(t1 - t0).count();
+            R.seconds = ms * 1e-3;
             if (R.out.status < 0) {
                 set_error("solver group barrier timed out");
                 rc = -1;

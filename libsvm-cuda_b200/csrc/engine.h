@@ -68,11 +68,15 @@ struct GroupSync {
 // reduced value and position it carries the winner's per-variable data
 // (alpha, QD, label, local index, row id) so that no block has to read
 // another block's chunk of the state arrays.
+// `seq` is written last with release semantics: a reader that observes
+// seq == k (acquire) sees the record of exchange k, so the record exchange is
+// also the group barrier.
 struct Partial {
     double v[8];
     int n[8];
     float q[2];
-    int pad[6];
+    int seq;
+    int pad[5];
 };
 static_assert(sizeof(Partial) == 128, "Partial must stay 128 bytes");
 
@@ -84,7 +88,15 @@ struct SolveOut {
     int unshrink;
     int nr_free;
     double gap;                 // m(alpha) - M(alpha) at exit
+    // work counters (for the roofline): sum over iterations of the active
+    // size, Q values evaluated, and cache lookups that hit
+    long long sum_active;
+    long long q_evals;
+    long long lookups, hits;
+    // SM cycles spent by block 0 in each section of the loop (kProf* below)
+    long long prof[8];
 };
+enum { kProfAReduce = 0, kProfAFill, kProfAScan, kProfBReduce, kProfBFill, kProfBUpdate, kProfShrink, kProfTotal };
 
 struct InstanceDesc {
     int l;
@@ -113,6 +125,7 @@ struct InstanceDesc {
     // source-row staging in dynamic shared memory
     int stage_cap;              // rows staged at once (1..kSrcBatch); 0: read sources from global memory
     int stage_lds;              // floats per staged row (dense: ld; sparse: d)
+    int chunk_cap;              // positions of per-block state held in shared memory (>= ceil(l/nblocks))
 };
 
 }  // namespace svmb

@@ -26,7 +26,8 @@ struct DeviceRows {
     int *col = nullptr;
     float *val = nullptr;
     double *xsq[2] = {nullptr, nullptr};   // per RowForm
-    size_t bytes = 0;
+    size_t bytes = 0;          // device bytes of the layout the solver reads
+    size_t h2d_bytes = 0;      // bytes copied from the host by the upload
     ~DeviceRows();
     DevX view(int form) const;
 };
@@ -68,9 +69,17 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
                 std::vector<SolveResult> &res, cudaStream_t s);
 
 int device_sm_count();
+void count_launch(long long n = 1);
+void transfer_bytes(long long *h2d, long long *d2h);
+cudaError_t xfer_async(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
+cudaError_t xfer(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind);
+long long launch_count();
 
 // device-side launchers (smo_kernel.cu)
 cudaError_t launch_xsq(const DevX &x, int n, double *out, int form, cudaStream_t s);
+cudaError_t launch_scatter_dense(const long long *rowptr, const int *col, const float *val, int n, int ld, float *X,
+                                 cudaStream_t s);
+int smo_static_smem();
 cudaError_t launch_smo(int form, const InstanceDesc *d_insts, const int *d_block_inst, int nblocks,
                        size_t dyn_smem, bool cooperative, cudaStream_t s);
 cudaError_t smo_max_blocks(int form, size_t dyn_smem, int *blocks_per_sm);

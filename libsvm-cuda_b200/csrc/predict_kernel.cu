@@ -216,7 +216,7 @@ int upload_nodes(const svm_node *const *x, int n, int d, int base, bool dense, R
                 if (c >= 0 && c < out.ld) h[(size_t)r * out.ld + c] = (float)p->value;
             }
         PK(cudaMalloc(&out.X, h.size() * sizeof(float)));
-        PK(cudaMemcpy(out.X, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+        PK(xfer(out.X, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
     } else {
         std::vector<long long> rp(n + 1, 0);
         std::vector<int> col;
@@ -233,9 +233,9 @@ int upload_nodes(const svm_node *const *x, int n, int d, int base, bool dense, R
         PK(cudaMalloc(&out.rowptr, rp.size() * sizeof(long long)));
         PK(cudaMalloc(&out.col, col.size() * sizeof(int)));
         PK(cudaMalloc(&out.val, val.size() * sizeof(float)));
-        PK(cudaMemcpy(out.rowptr, rp.data(), rp.size() * sizeof(long long), cudaMemcpyHostToDevice));
-        PK(cudaMemcpy(out.col, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice));
-        PK(cudaMemcpy(out.val, val.data(), val.size() * sizeof(float), cudaMemcpyHostToDevice));
+        PK(xfer(out.rowptr, rp.data(), rp.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        PK(xfer(out.col, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice));
+        PK(xfer(out.val, val.data(), val.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
     return 0;
 }
@@ -280,10 +280,10 @@ Session *get_session(const svm_model *m)
         s->release();
         return nullptr;
     }
-    cudaMemcpy(s->coef, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->start, start.data(), start.size() * 4, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->nsv, nsv.data(), nsv.size() * 4, cudaMemcpyHostToDevice);
+    xfer(s->coef, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice);
+    xfer(s->rho, rho.data(), rho.size() * 8, cudaMemcpyHostToDevice);
+    xfer(s->start, start.data(), start.size() * 4, cudaMemcpyHostToDevice);
+    xfer(s->nsv, nsv.data(), nsv.size() * 4, cudaMemcpyHostToDevice);
     Session *raw = s.get();
     g_sessions[m] = std::move(s);
     return raw;
@@ -346,6 +346,7 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
                 }
                 cudaFuncSetAttribute(kvalue_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 kvalue_dense<<<grid, 256, smem>>>(kp, T.X, tn, s->sv.X, m->l, s->sv.ld, kv);
+                count_launch();
             } else {
                 Rows Sc = s->sv;
                 Rows svcsr;
@@ -356,12 +357,14 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
                 }
                 if (upload_nodes(rows + t0, tn, maxi + 1, s->base, false, T) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
                 kvalue_csr<<<std::min<long long>(((long long)tn * m->l + 255) / 256, 148 * 16), 256>>>(kp, T, Sc, kv);
+                count_launch();
                 if (s->sv.dense) {
                     cudaDeviceSynchronize();
                     svcsr.release();
                 }
             }
             pair_sums<<<std::min<long long>(((long long)tn * npair + 127) / 128, 148 * 8), 128>>>(kv, tn, m->l, k, s->start, s->nsv, s->coef, s->rho, d_dec);
+            count_launch();
             cudaError_t e = cudaDeviceSynchronize();
             T.release();
             if (e != cudaSuccess) {
@@ -369,7 +372,7 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
                 cudaFree(kv); cudaFree(d_dec);
                 return -1;
             }
-            PK(cudaMemcpy(dec.data() + (size_t)t0 * npair, d_dec, (size_t)tn * npair * 8, cudaMemcpyDeviceToHost));
+            PK(xfer(dec.data() + (size_t)t0 * npair, d_dec, (size_t)tn * npair * 8, cudaMemcpyDeviceToHost));
         }
         cudaFree(kv);
         cudaFree(d_dec);

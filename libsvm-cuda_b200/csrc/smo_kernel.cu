@@ -3,30 +3,38 @@
 // One persistent launch runs the whole solve of one or more instances (each a
 // binary subproblem).  Every instance is owned by a group of `nblocks` thread
 // blocks; block `rank` of the group owns a contiguous chunk of the active
-// positions [0, A) and a chunk of the inactive tail [A, l).  Per SMO iteration
-// there are exactly two group barriers:
+// positions [0, A) and a chunk of the inactive tail [A, l).  The state of its
+// active chunk (G, alpha, QD, label, bound status, cache column, row id) lives
+// in the block's shared memory between shrink events.  Per SMO iteration there
+// are exactly two group exchanges:
 //
-//   phase A  reduce the per-block I_up maxima  -> working index i (and, for
-//            nu-SVC, the two track maxima ip/in), look up / evaluate the Q row(s)
-//            for the block's chunk, scan the chunk for the second-order j
-//            candidate (WSS3, reference svm.cpp:833-930 / :1076-1186)
-//   --- barrier ---
-//   phase B  reduce the j candidates, stopping test, look up / evaluate Q_j,
+//   phase A  reduce the per-block I_up maxima -> working index i (nu-SVC: the
+//            two track maxima ip/in), look up or evaluate the Q row(s) on the
+//            block's chunk, scan the chunk for the second-order j candidate
+//            (WSS3, reference svm.cpp:833-930 / :1076-1186)
+//   --- exchange ---
+//   phase B  reduce the j candidates, stopping test, look up or evaluate Q_j,
 //            two-variable analytic step with box clipping (svm.cpp:636-721,
 //            computed redundantly and identically by every block), gradient
-//            update G += dQ (svm.cpp:729-735) and G_bar update (:744-769) on
-//            the block's chunk, fused with the I_up scan for the next i
-//   --- barrier ---
+//            update G += dQ (svm.cpp:729-735) and G_bar update (:744-769) on the
+//            block's chunk, fused with the I_up scan for the next i
+//   --- exchange ---
 //
-// Shrinking (svm.cpp:932-1011), unshrinking and gradient reconstruction
-// (:473-513) and the initial gradient (:545-572) run inside the same launch as
-// group-collective sections.  The position permutation of shrinking is the
-// reference's (hole i paired with the last non-shrunk position), so
+// An exchange publishes a 128-byte record per block whose last field is a
+// sequence number written with release semantics; every block polls all
+// records with acquire loads.  The exchange is therefore also the group
+// barrier.  Records alternate between two buffers.
+//
+// Shrinking (svm.cpp:932-1011), gradient reconstruction (:473-513) and the
+// initial gradient (:545-572) run inside the same launch as group-collective
+// sections on the global copies of the state.  The position permutation of
+// shrinking is the reference's (each shrunk position below the new active
+// size is swapped with the highest kept position above it), so the
 // position-based tie-breaks are identical.  All double arithmetic keeps the
 // reference's operand order; the file is compiled with -fmad=false so that no
 // multiply-add is contracted.
 //
-// Barriers are bounded: a wait that exceeds kBarrierTimeout cycles sets the
+// Every wait is bounded: a poll that exceeds kWaitTimeout cycles sets the
 // group's error flag and every block of the group returns.
 #include "engine.h"
 
@@ -37,56 +45,27 @@
 namespace svmb {
 
 #define SVMB_INF __longlong_as_double(0x7ff0000000000000ULL)
-constexpr double kTau = 1e-12;                       // reference svm.cpp:42
-constexpr long long kBarrierTimeout = 60000000000LL; // ~30 s of SM clock
+constexpr double kTau = 1e-12;                     // reference svm.cpp:42
+constexpr long long kWaitTimeout = 60000000000LL;  // ~30 s of SM clock
 
 // --------------------------------------------------------------------------
-// group barrier (sense by generation counter, bounded spin)
+// memory-model helpers
 // --------------------------------------------------------------------------
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+__device__ __forceinline__ int ld_acquire_i32(const int *p)
 {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
+}
+__device__ __forceinline__ void st_release_i32(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ int ld_relaxed_i32(const int *p)
 {
     int v;
     asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
-}
-
-__device__ bool group_barrier(GroupSync *s, int nblocks, int *okflag)
-{
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int good = 1;
-        if (nblocks > 1) {
-            __threadfence();
-            unsigned gen = ld_acquire_u32(&s->gen);
-            unsigned arrived = atomicAdd(&s->count, 1u);
-            if (arrived == (unsigned)(nblocks - 1)) {
-                atomicExch(&s->count, 0u);
-                __threadfence();
-                atomicAdd(&s->gen, 1u);
-            } else {
-                long long t0 = clock64();
-                while (ld_acquire_u32(&s->gen) == gen) {
-                    if (ld_relaxed_i32(&s->error) != 0 || clock64() - t0 > kBarrierTimeout) {
-                        atomicExch(&s->error, 1);
-                        good = 0;
-                        break;
-                    }
-                }
-            }
-            __threadfence();
-        } else {
-            __threadfence_block();
-        }
-        *okflag = good;
-    }
-    __syncthreads();
-    return *okflag != 0;
 }
 
 // --------------------------------------------------------------------------
@@ -132,7 +111,7 @@ struct StageSlots {
     int ns;
 };
 
-__device__ void stage_sources(const InstanceDesc &D, float *dyn, StageSlots &ss, const int *rows, int ns)
+__device__ void stage_sources(const InstanceDesc &D, float *stage, StageSlots &ss, const int *rows, int ns)
 {
     const DevX &x = D.x;
     if (threadIdx.x < ns) ss.rows[threadIdx.x] = rows[threadIdx.x];
@@ -142,17 +121,17 @@ __device__ void stage_sources(const InstanceDesc &D, float *dyn, StageSlots &ss,
         for (int k = 0; k < ns; k++) {
             const float4 *src = reinterpret_cast<const float4 *>(x.X + (long long)rows[k] * x.ld);
             if (D.stage_cap > 0) {
-                float4 *dst = reinterpret_cast<float4 *>(dyn + (long long)k * D.stage_lds);
+                float4 *dst = reinterpret_cast<float4 *>(stage + (long long)k * D.stage_lds);
                 for (int t = threadIdx.x; t < ld4; t += blockDim.x) dst[t] = __ldg(src + t);
-                if (threadIdx.x == 0) ss.sp[k] = dyn + (long long)k * D.stage_lds;
+                if (threadIdx.x == 0) ss.sp[k] = stage + (long long)k * D.stage_lds;
             } else if (threadIdx.x == 0) {
                 ss.sp[k] = x.X + (long long)rows[k] * x.ld;
             }
         }
     } else if (D.stage_cap > 0) {
         for (int k = 0; k < ns; k++) {
-            long long a = x.rowptr[rows[k]], b = x.rowptr[rows[k] + 1];
-            float *dst = dyn + (long long)k * D.stage_lds;
+            const long long a = x.rowptr[rows[k]], b = x.rowptr[rows[k] + 1];
+            float *dst = stage + (long long)k * D.stage_lds;
             for (long long e = a + threadIdx.x; e < b; e += blockDim.x) dst[x.col[e]] = x.val[e];
             if (threadIdx.x == 0) ss.sp[k] = dst;
         }
@@ -161,80 +140,120 @@ __device__ void stage_sources(const InstanceDesc &D, float *dyn, StageSlots &ss,
 }
 
 // Undo a sparse scatter so that the dense vectors are all-zero again.
-__device__ void unstage_sources(const InstanceDesc &D, float *dyn, StageSlots &ss)
+__device__ void unstage_sources(const InstanceDesc &D, float *stage, StageSlots &ss)
 {
     __syncthreads();
     const DevX &x = D.x;
     if (!x.X && D.stage_cap > 0) {
         for (int k = 0; k < ss.ns; k++) {
-            long long a = x.rowptr[ss.rows[k]], b = x.rowptr[ss.rows[k] + 1];
-            float *dst = dyn + (long long)k * D.stage_lds;
+            const long long a = x.rowptr[ss.rows[k]], b = x.rowptr[ss.rows[k] + 1];
+            float *dst = stage + (long long)k * D.stage_lds;
             for (long long e = a + threadIdx.x; e < b; e += blockDim.x) dst[x.col[e]] = 0.0f;
         }
     }
     __syncthreads();
 }
 
-// Dot products of target row `r` with the staged sources, accumulated in
+template <int FORM>
+struct Acc {
+    typedef typename std::conditional<FORM == FORM_EXACT, double, float>::type type;
+};
+
+template <int FORM>
+__device__ __forceinline__ typename Acc<FORM>::type mac(float a, float b, typename Acc<FORM>::type acc)
+{
+    if (FORM == FORM_EXACT) return fma((double)a, (double)b, (double)acc);
+    return fmaf(a, b, (float)acc);
+}
+
+// Dot products of target row `r` with NS staged sources, accumulated in
 // feature order (the order of the reference's Kernel::dot, svm.cpp:305-325:
 // only matching indices contribute; zero products leave the sum unchanged).
-template <int FORM>
-__device__ __forceinline__ void row_dots(const InstanceDesc &D, const StageSlots &ss, int ns, int r,
-                                         double (&out)[kSrcBatch])
+// Dense rows are streamed 8 x 16 bytes at a time per thread.
+template <int FORM, int NS>
+__device__ __forceinline__ void row_dots_n(const InstanceDesc &D, const StageSlots &ss, int ns, int r,
+                                           double (&out)[kSrcBatch])
 {
     const DevX &x = D.x;
-    typedef typename std::conditional<FORM == FORM_EXACT, double, float>::type acc_t;
-    acc_t acc[kSrcBatch];
+    typedef typename Acc<FORM>::type acc_t;
+    acc_t acc[NS];
 #pragma unroll
-    for (int k = 0; k < kSrcBatch; k++) acc[k] = acc_t(0);
+    for (int k = 0; k < NS; k++) acc[k] = acc_t(0);
     if (x.X) {
         const float4 *row = reinterpret_cast<const float4 *>(x.X + (long long)r * x.ld);
+        const float4 *src[NS];
+#pragma unroll
+        for (int k = 0; k < NS; k++) src[k] = reinterpret_cast<const float4 *>(ss.sp[k < ns ? k : 0]);
         const int ld4 = x.ld >> 2;
-        for (int c = 0; c < ld4; c++) {
+        int c = 0;
+        for (; c + 8 <= ld4; c += 8) {
+            float4 v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = __ldg(row + c + u);
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+#pragma unroll
+                for (int k = 0; k < NS; k++) {
+                    if (NS == kSrcBatch && k >= ns) continue;
+                    const float4 w = src[k][c + u];
+                    acc[k] = mac<FORM>(v[u].x, w.x, acc[k]);
+                    acc[k] = mac<FORM>(v[u].y, w.y, acc[k]);
+                    acc[k] = mac<FORM>(v[u].z, w.z, acc[k]);
+                    acc[k] = mac<FORM>(v[u].w, w.w, acc[k]);
+                }
+            }
+        }
+        for (; c < ld4; c++) {
             const float4 v = __ldg(row + c);
 #pragma unroll
-            for (int k = 0; k < kSrcBatch; k++) {
-                if (k < ns) {
-                    const float4 w = reinterpret_cast<const float4 *>(ss.sp[k])[c];
-                    if (FORM == FORM_EXACT) {
-                        acc[k] = fma((double)v.x, (double)w.x, (double)acc[k]);
-                        acc[k] = fma((double)v.y, (double)w.y, (double)acc[k]);
-                        acc[k] = fma((double)v.z, (double)w.z, (double)acc[k]);
-                        acc[k] = fma((double)v.w, (double)w.w, (double)acc[k]);
-                    } else {
-                        acc[k] = fmaf(v.x, w.x, (float)acc[k]);
-                        acc[k] = fmaf(v.y, w.y, (float)acc[k]);
-                        acc[k] = fmaf(v.z, w.z, (float)acc[k]);
-                        acc[k] = fmaf(v.w, w.w, (float)acc[k]);
-                    }
-                }
+            for (int k = 0; k < NS; k++) {
+                if (NS == kSrcBatch && k >= ns) continue;
+                const float4 w = src[k][c];
+                acc[k] = mac<FORM>(v.x, w.x, acc[k]);
+                acc[k] = mac<FORM>(v.y, w.y, acc[k]);
+                acc[k] = mac<FORM>(v.z, w.z, acc[k]);
+                acc[k] = mac<FORM>(v.w, w.w, acc[k]);
             }
         }
     } else if (D.stage_cap > 0) {
         const long long a = x.rowptr[r], b = x.rowptr[r + 1];
-        for (long long e = a; e < b; e++) {
-            const int c = __ldg(x.col + e);
-            const float v = __ldg(x.val + e);
+        long long e = a;
+        for (; e + 4 <= b; e += 4) {
+            int cc[4];
+            float vv[4];
 #pragma unroll
-            for (int k = 0; k < kSrcBatch; k++) {
-                if (k < ns) {
-                    if (FORM == FORM_EXACT) acc[k] = fma((double)v, (double)ss.sp[k][c], (double)acc[k]);
-                    else acc[k] = fmaf(v, ss.sp[k][c], (float)acc[k]);
+            for (int u = 0; u < 4; u++) { cc[u] = __ldg(x.col + e + u); vv[u] = __ldg(x.val + e + u); }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+#pragma unroll
+                for (int k = 0; k < NS; k++) {
+                    if (NS == kSrcBatch && k >= ns) continue;
+                    acc[k] = mac<FORM>(vv[u], ss.sp[k][cc[u]], acc[k]);
                 }
+            }
+        }
+        for (; e < b; e++) {
+            const int cc = __ldg(x.col + e);
+            const float vv = __ldg(x.val + e);
+#pragma unroll
+            for (int k = 0; k < NS; k++) {
+                if (NS == kSrcBatch && k >= ns) continue;
+                acc[k] = mac<FORM>(vv, ss.sp[k][cc], acc[k]);
             }
         }
     } else {
         // merge walk of two sorted index lists in global memory
         const long long a = x.rowptr[r], b = x.rowptr[r + 1];
-        for (int k = 0; k < ns; k++) {
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            if (k >= ns) continue;
             const long long sa = x.rowptr[ss.rows[k]], sb = x.rowptr[ss.rows[k] + 1];
             long long e = a, f = sa;
             acc_t s = acc_t(0);
             while (e < b && f < sb) {
                 const int ce = __ldg(x.col + e), cf = __ldg(x.col + f);
                 if (ce == cf) {
-                    if (FORM == FORM_EXACT) s = fma((double)__ldg(x.val + e), (double)__ldg(x.val + f), (double)s);
-                    else s = fmaf(__ldg(x.val + e), __ldg(x.val + f), (float)s);
+                    s = mac<FORM>(__ldg(x.val + e), __ldg(x.val + f), s);
                     ++e;
                     ++f;
                 } else if (ce > cf) {
@@ -247,7 +266,16 @@ __device__ __forceinline__ void row_dots(const InstanceDesc &D, const StageSlots
         }
     }
 #pragma unroll
-    for (int k = 0; k < kSrcBatch; k++) out[k] = (double)acc[k];
+    for (int k = 0; k < NS; k++) out[k] = (double)acc[k];
+}
+
+template <int FORM>
+__device__ __forceinline__ void row_dots(const InstanceDesc &D, const StageSlots &ss, int ns, int r,
+                                         double (&out)[kSrcBatch])
+{
+    if (ns == 1) row_dots_n<FORM, 1>(D, ss, ns, r, out);
+    else if (ns == 2) row_dots_n<FORM, 2>(D, ss, ns, r, out);
+    else row_dots_n<FORM, kSrcBatch>(D, ss, ns, r, out);
 }
 
 // --------------------------------------------------------------------------
@@ -268,8 +296,8 @@ __device__ __forceinline__ void warp_argmax(double &v, int &i)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        double v2 = __shfl_xor_sync(0xffffffffu, v, o);
-        int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
         better_max(v, i, v2, i2);
     }
 }
@@ -277,8 +305,8 @@ __device__ __forceinline__ void warp_argmin(double &v, int &i)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        double v2 = __shfl_xor_sync(0xffffffffu, v, o);
-        int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
         better_min(v, i, v2, i2);
     }
 }
@@ -300,7 +328,8 @@ struct RedScratch {
     int i[4][kWarps];
 };
 
-// Reduce up to 4 (value,index) pairs over the block.  kind[k]: 0 argmax, 1 argmin, 2 max (index ignored).
+// Reduce up to 4 (value,index) pairs over the block; the result is in every
+// thread.  kind[k]: 0 argmax, 1 argmin, 2 max (index ignored).
 template <int N>
 __device__ void block_reduce(RedScratch &s, double (&v)[N], int (&idx)[N], const int (&kind)[N])
 {
@@ -317,20 +346,17 @@ __device__ void block_reduce(RedScratch &s, double (&v)[N], int (&idx)[N], const
         for (int k = 0; k < N; k++) { s.v[k][w] = v[k]; s.i[k][w] = idx[k]; }
     }
     __syncthreads();
-    if (w == 0) {
 #pragma unroll
-        for (int k = 0; k < N; k++) {
-            double vv = kind[k] == 1 ? SVMB_INF : -SVMB_INF;
-            int ii = -1;
-            if (lane < kWarps) { vv = s.v[k][lane]; ii = s.i[k][lane]; }
-            if (kind[k] == 0) warp_argmax(vv, ii);
-            else if (kind[k] == 1) warp_argmin(vv, ii);
-            else vv = warp_max(vv);
-            v[k] = vv;
-            idx[k] = ii;
-        }
+    for (int k = 0; k < N; k++) {
+        double vv = kind[k] == 1 ? SVMB_INF : -SVMB_INF;
+        int ii = -1;
+        if (lane < kWarps) { vv = s.v[k][lane]; ii = s.i[k][lane]; }
+        if (kind[k] == 0) warp_argmax(vv, ii);
+        else if (kind[k] == 1) warp_argmin(vv, ii);
+        else vv = warp_max(vv);
+        v[k] = vv;
+        idx[k] = ii;
     }
-    __syncthreads();
 }
 
 __device__ int block_sum_i(RedScratch &s, int v)
@@ -340,25 +366,25 @@ __device__ int block_sum_i(RedScratch &s, int v)
     __syncthreads();
     if (lane == 0) s.i[0][w] = v;
     __syncthreads();
-    int tot = 0;
-    for (int k = 0; k < kWarps; k++) tot += s.i[0][k];
+    int tot = lane < kWarps ? s.i[0][lane] : 0;
+    tot = warp_sum_i(tot);
     __syncthreads();
     return tot;
 }
 
-// exclusive prefix over the block of a 0/1 flag, in thread order; returns the
-// prefix for this thread and the block total in *total.
+// exclusive prefix over the block of a 0/1 flag, in thread order; the block
+// total goes to *total.
 __device__ int block_excl_scan(RedScratch &s, int flag, int *total)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    unsigned bal = __ballot_sync(0xffffffffu, flag);
-    int in_warp = __popc(bal & ((1u << lane) - 1u));
+    const unsigned bal = __ballot_sync(0xffffffffu, flag);
+    const int in_warp = __popc(bal & ((1u << lane) - 1u));
     __syncthreads();
     if (lane == 0) s.i[0][w] = __popc(bal);
     __syncthreads();
     int before = 0, tot = 0;
     for (int k = 0; k < kWarps; k++) {
-        int c = s.i[0][k];
+        const int c = s.i[0][k];
         if (k < w) before += c;
         tot += c;
     }
@@ -384,18 +410,17 @@ struct CacheState {
 };
 
 struct Lookup {
-    long long slot;     // slot index
+    long long slot;
     int valid_active;   // positions [0,A) already valid
-    int full;           // all positions valid
 };
 
 __device__ void cache_rotate(CacheState &cs, const CacheView &cv, int rank)
 {
-    // called by thread 0 right after a barrier: publish the previous phase's records
+    // thread 0, right after an exchange: publish the previous phase's records
     if (rank == 0) {
         for (int k = 0; k < cs.ncur; k++) {
             const CacheRec &r = cs.cur[k];
-            long long s = (long long)r.set * cv.nways + r.way;
+            const long long s = (long long)r.set * cv.nways + r.way;
             cv.tag[s] = r.tag;
             cv.epoch[s] = r.epoch;
             cv.stamp[s] = r.stamp;
@@ -410,21 +435,29 @@ __device__ void cache_read_set(const CacheState &cs, const CacheView &cv, int se
                                unsigned long long *st)
 {
     for (int w = 0; w < cv.nways; w++) {
-        long long s = (long long)set * cv.nways + w;
-        tag[w] = *(volatile int *)&cv.tag[s];
-        ep[w] = *(volatile int *)&cv.epoch[s];
-        st[w] = *(volatile unsigned long long *)&cv.stamp[s];
+        const long long s = (long long)set * cv.nways + w;
+        tag[w] = __ldcg(&cv.tag[s]);
+        ep[w] = __ldcg(&cv.epoch[s]);
+        st[w] = __ldcg(&cv.stamp[s]);
     }
     for (int k = 0; k < cs.nprev; k++)
-        if (cs.prev[k].set == set) { tag[cs.prev[k].way] = cs.prev[k].tag; ep[cs.prev[k].way] = cs.prev[k].epoch; st[cs.prev[k].way] = cs.prev[k].stamp; }
+        if (cs.prev[k].set == set) {
+            tag[cs.prev[k].way] = cs.prev[k].tag;
+            ep[cs.prev[k].way] = cs.prev[k].epoch;
+            st[cs.prev[k].way] = cs.prev[k].stamp;
+        }
     for (int k = 0; k < cs.ncur; k++)
-        if (cs.cur[k].set == set) { tag[cs.cur[k].way] = cs.cur[k].tag; ep[cs.cur[k].way] = cs.cur[k].epoch; st[cs.cur[k].way] = cs.cur[k].stamp; }
+        if (cs.cur[k].set == set) {
+            tag[cs.cur[k].way] = cs.cur[k].tag;
+            ep[cs.cur[k].way] = cs.cur[k].epoch;
+            st[cs.cur[k].way] = cs.cur[k].stamp;
+        }
 }
 
-// Decide where row `local` lives; records the decision.  need_full: the caller
-// will make the row complete (positions [0,l)).
+// Decide where row `local` lives; records the decision.  whole: the rows
+// evaluated now cover every position (A == l), so they are complete.
 __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, int cur_epoch,
-                               unsigned long long clk, int need_full)
+                               unsigned long long clk, int whole)
 {
     int tag[kMaxWays], ep[kMaxWays];
     unsigned long long st[kMaxWays];
@@ -439,12 +472,10 @@ __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, i
     rec.stamp = clk;
     rec.tag = local;
     if (way >= 0) {
-        int full = ep[way] == kEpochFull;
-        int va = full || ep[way] == cur_epoch;
+        const int va = ep[way] == kEpochFull || ep[way] == cur_epoch;
         L.valid_active = va;
-        L.full = full;
         rec.way = way;
-        rec.epoch = need_full ? kEpochFull : (va ? ep[way] : cur_epoch);
+        rec.epoch = whole ? kEpochFull : (va ? ep[way] : cur_epoch);
     } else {
         int victim = -1;
         for (int w = 0; w < cv.nways; w++)
@@ -455,9 +486,8 @@ __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, i
                 if (st[w] < st[victim]) victim = w;
         }
         L.valid_active = 0;
-        L.full = 0;
         rec.way = victim;
-        rec.epoch = need_full ? kEpochFull : cur_epoch;
+        rec.epoch = whole ? kEpochFull : cur_epoch;
         way = victim;
     }
     L.slot = (long long)set * cv.nways + way;
@@ -485,7 +515,6 @@ struct Shared {
     RedScratch red;
     CacheState cs;
     StageSlots ss;
-    int okflag;
     double bd[24];
     int bi[24];
     long long bl[8];
@@ -497,13 +526,18 @@ struct Shared {
 
 struct Ctx {
     const InstanceDesc *D;
-    float *dyn;
+    float *stage;           // source staging area (dynamic smem)
+    // my chunk of [0,A) held in shared memory
+    double *sG, *sA, *sQD;
+    int *sCol, *sRow;
+    signed char *sY;
+    unsigned char *sS;
     int rank, nb;
     int A;                  // active size
     int a0, a1;             // my chunk of [0,A)
     int t0, t1;             // my chunk of [A,l)
     int epoch;
-    int phase;              // barrier count: selects the partial buffer
+    int phase;              // exchange counter: selects the record buffer and sequence number
 };
 
 __device__ __forceinline__ void set_chunks(Ctx &c)
@@ -516,17 +550,44 @@ __device__ __forceinline__ void set_chunks(Ctx &c)
     c.t1 = c.A + (int)(m * (c.rank + 1) / c.nb);
 }
 
-// records written in the current phase / read from the previous phase
 __device__ __forceinline__ Partial *my_partial(const Ctx &c) { return c.D->partials + (long long)(c.phase & 1) * c.nb + c.rank; }
 __device__ __forceinline__ const Partial *prev_partials(const Ctx &c) { return c.D->partials + (long long)((c.phase - 1) & 1) * c.nb; }
 
-__device__ bool sync_group(Ctx &c, Shared &sh)
+// Publish my record of this phase and wait for everybody's (group barrier).
+__device__ bool exchange(Ctx &c, Shared &sh)
 {
-    bool ok = group_barrier(c.D->sync, c.nb, &sh.okflag);
-    if (threadIdx.x == 0) cache_rotate(sh.cs, c.D->cache, c.rank);
+    __syncthreads();
+    const int want = c.phase + 1;
+    Partial *mine = my_partial(c);
+    int ok = 1;
+    if (c.nb > 1) {
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release_i32(&mine->seq, want);
+        }
+        const Partial *all = c.D->partials + (long long)(c.phase & 1) * c.nb;
+        for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
+            const long long t0 = clock64();
+            long long spins = 0;
+            while (ld_acquire_i32(&all[b].seq) != want) {
+                if ((++spins & 63) == 0) {
+                    if (ld_relaxed_i32(&c.D->sync->error) != 0 || clock64() - t0 > kWaitTimeout) {
+                        atomicExch(&c.D->sync->error, 1);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+    }
+    ok = __syncthreads_and(ok);
+    if (threadIdx.x == 0) {
+        if (c.nb > 1) __threadfence();
+        cache_rotate(sh.cs, c.D->cache, c.rank);
+    }
     c.phase++;
     __syncthreads();
-    return ok;
+    return ok != 0;
 }
 
 __device__ __forceinline__ double get_C(const InstanceDesc &D, int y) { return y > 0 ? D.Cp : D.Cn; }
@@ -538,12 +599,41 @@ __device__ __forceinline__ unsigned char status_of(double a, double C)
     return ST_FREE;
 }
 
-// Sum over the group's blocks of per-block counters (block-parallel read).
-__device__ void group_counts(const Ctx &c, Shared &sh, const Partial *all, int slot, int *below, int *above, int *total)
+// chunk state: global -> shared / shared -> global (mutable fields only)
+__device__ void chunk_load(Ctx &c)
 {
+    const InstanceDesc &D = *c.D;
+    for (int k = threadIdx.x; k < c.a1 - c.a0; k += blockDim.x) {
+        const int p = c.a0 + k;
+        c.sG[k] = D.G[p];
+        c.sA[k] = D.alpha[p];
+        c.sQD[k] = D.QD[p];
+        c.sCol[k] = D.pos_local[p];
+        c.sRow[k] = D.pos_row[p];
+        c.sY[k] = D.y[p];
+        c.sS[k] = D.status[p];
+    }
+    __syncthreads();
+}
+__device__ void chunk_store(Ctx &c)
+{
+    const InstanceDesc &D = *c.D;
+    __syncthreads();
+    for (int k = threadIdx.x; k < c.a1 - c.a0; k += blockDim.x) {
+        const int p = c.a0 + k;
+        D.G[p] = c.sG[k];
+        D.alpha[p] = c.sA[k];
+        D.status[p] = c.sS[k];
+    }
+}
+
+// Sum over the group's blocks of per-block counters of the previous exchange.
+__device__ void group_counts(const Ctx &c, Shared &sh, int slot, int *below, int *above, int *total)
+{
+    const Partial *all = prev_partials(c);
     int b_lo = 0, b_hi = 0, tot = 0;
     for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-        const int v = all[b].n[slot];
+        const int v = __ldcg(&all[b].n[slot]);
         tot += v;
         if (b < c.rank) b_lo += v;
         if (b > c.rank) b_hi += v;
@@ -554,8 +644,9 @@ __device__ void group_counts(const Ctx &c, Shared &sh, const Partial *all, int s
 }
 
 // --------------------------------------------------------------------------
-// row-block accumulation: for every target position e in [lo,hi), in source
-// order over the positions s < src_end selected by the predicate,
+// row-block accumulation on the global state: for every target position e in
+// [lo,hi), in source order over the positions s < src_end selected by the
+// predicate,
 //   G[e] += alpha_s * Q[s][e]  and, with `with_bar`, for upper-bound s,
 //   G_bar[e] += C_s * Q[s][e].
 // This is the initial gradient (svm.cpp:559-570) and the gradient
@@ -597,7 +688,7 @@ __device__ void accumulate_rows(Ctx &c, Shared &sh, int src_end, int pick_free_o
         if (ns == 0) break;
         if (threadIdx.x < ns) sh.srcrow[threadIdx.x] = D.pos_row[sh.srcpos[threadIdx.x]];
         __syncthreads();
-        stage_sources(D, c.dyn, sh.ss, sh.srcrow, ns);
+        stage_sources(D, c.stage, sh.ss, sh.srcrow, ns);
         for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) {
             double dots[kSrcBatch];
             const int r = D.pos_row[e];
@@ -617,12 +708,13 @@ __device__ void accumulate_rows(Ctx &c, Shared &sh, int src_end, int pick_free_o
             D.G[e] = g;
             if (with_bar) D.G_bar[e] = gb;
         }
-        unstage_sources(D, c.dyn, sh.ss);
+        unstage_sources(D, c.stage, sh.ss);
         if (ns < cap) break;
     }
 }
 
-// gradient reconstruction (reference svm.cpp:473-513); group collective
+// gradient reconstruction (reference svm.cpp:473-513); group collective on the
+// global state (the caller has stored its chunk)
 template <int FORM>
 __device__ bool reconstruct(Ctx &c, Shared &sh)
 {
@@ -631,7 +723,7 @@ __device__ bool reconstruct(Ctx &c, Shared &sh)
     for (int e = c.t0 + threadIdx.x; e < c.t1; e += blockDim.x) D.G[e] = __dadd_rn(D.G_bar[e], D.p[e]);
     __syncthreads();
     accumulate_rows<FORM>(c, sh, c.A, 1, 0, c.t0, c.t1);
-    return sync_group(c, sh);
+    return exchange(c, sh);
 }
 
 // --------------------------------------------------------------------------
@@ -663,20 +755,30 @@ __device__ __forceinline__ void swap_pos(const InstanceDesc &D, int a, int b)
     ti = D.pos_row[a]; D.pos_row[a] = D.pos_row[b]; D.pos_row[b] = ti;
 }
 
+// widen the active set to l after a reconstruction (chunk reloaded)
+__device__ void widen(Ctx &c)
+{
+    c.A = c.D->l;
+    c.epoch++;
+    set_chunks(c);
+    chunk_load(c);
+}
+
 template <int FORM>
 __device__ bool do_shrinking(Ctx &c, Shared &sh, int &unshrink)
 {
     const InstanceDesc &D = *c.D;
     const int nu = D.nu;
+    const int n = c.a1 - c.a0;
     // 1. maximal violations over the active set (C-SVC: Gmax1, Gmax2; nu: Gmax1..4)
     {
         double v[4] = {-SVMB_INF, -SVMB_INF, -SVMB_INF, -SVMB_INF};
         int ix[4] = {-1, -1, -1, -1};
         const int kind[4] = {2, 2, 2, 2};
-        for (int p = c.a0 + threadIdx.x; p < c.a1; p += blockDim.x) {
-            const unsigned char s = D.status[p];
-            const double G = D.G[p];
-            const int y = D.y[p];
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const unsigned char s = c.sS[k];
+            const double G = c.sG[k];
+            const int y = c.sY[k];
             if (!nu) {
                 if (y == +1) {
                     if (s != ST_UPPER) v[0] = fmax(v[0], -G);
@@ -696,7 +798,8 @@ __device__ bool do_shrinking(Ctx &c, Shared &sh, int &unshrink)
             for (int k = 0; k < 4; k++) pp->v[k] = v[k];
         }
     }
-    if (!sync_group(c, sh)) return false;
+    chunk_store(c);     // the swaps and a reconstruction work on the global state
+    if (!exchange(c, sh)) return false;
     double g[4];
     {
         const Partial *all = prev_partials(c);
@@ -704,41 +807,37 @@ __device__ bool do_shrinking(Ctx &c, Shared &sh, int &unshrink)
         int ix[4] = {-1, -1, -1, -1};
         const int kind[4] = {2, 2, 2, 2};
         for (int b = threadIdx.x; b < c.nb; b += blockDim.x)
-            for (int k = 0; k < 4; k++) v[k] = fmax(v[k], all[b].v[k]);
+            for (int k = 0; k < 4; k++) v[k] = fmax(v[k], __ldcg(&all[b].v[k]));
         block_reduce<4>(sh.red, v, ix, kind);
-        if (threadIdx.x == 0) for (int k = 0; k < 4; k++) sh.bd[k] = v[k];
-        __syncthreads();
-        for (int k = 0; k < 4; k++) g[k] = sh.bd[k];
-        __syncthreads();
+        for (int k = 0; k < 4; k++) g[k] = v[k];
     }
     const double gap = nu ? fmax(__dadd_rn(g[0], g[1]), __dadd_rn(g[2], g[3])) : __dadd_rn(g[0], g[1]);
     if (!unshrink && gap <= __dmul_rn(D.eps, 10.0)) {
         unshrink = 1;
         if (!reconstruct<FORM>(c, sh)) return false;
-        c.A = D.l;
-        c.epoch++;
-        set_chunks(c);
+        widen(c);
     }
-    // 2. number of shrunk positions -> new active size K
+    // 2. shrunk positions per block -> new active size K
     {
         int cnt = 0;
-        for (int p = c.a0 + threadIdx.x; p < c.a1; p += blockDim.x)
-            cnt += be_shrunk(nu, D.status[p], D.y[p], D.G[p], g) ? 1 : 0;
+        for (int k = threadIdx.x; k < c.a1 - c.a0; k += blockDim.x)
+            cnt += be_shrunk(nu, c.sS[k], c.sY[k], c.sG[k], g) ? 1 : 0;
         cnt = block_sum_i(sh.red, cnt);
         if (threadIdx.x == 0) my_partial(c)->n[0] = cnt;
     }
-    if (!sync_group(c, sh)) return false;
+    if (!exchange(c, sh)) return false;
     int K;
     {
         int below, above, tot;
-        group_counts(c, sh, prev_partials(c), 0, &below, &above, &tot);
+        group_counts(c, sh, 0, &below, &above, &tot);
         K = c.A - tot;
     }
     // 3. holes = shrunk positions in [0,K) ascending, movers = kept positions in [K,A) descending
     {
         int h = 0, m = 0;
-        for (int p = c.a0 + threadIdx.x; p < c.a1; p += blockDim.x) {
-            const bool s = be_shrunk(nu, D.status[p], D.y[p], D.G[p], g);
+        for (int k = threadIdx.x; k < c.a1 - c.a0; k += blockDim.x) {
+            const int p = c.a0 + k;
+            const bool s = be_shrunk(nu, c.sS[k], c.sY[k], c.sG[k], g);
             if (p < K && s) h++;
             if (p >= K && !s) m++;
         }
@@ -746,18 +845,19 @@ __device__ bool do_shrinking(Ctx &c, Shared &sh, int &unshrink)
         m = block_sum_i(sh.red, m);
         if (threadIdx.x == 0) { Partial *pp = my_partial(c); pp->n[0] = h; pp->n[1] = m; }
     }
-    if (!sync_group(c, sh)) return false;
+    if (!exchange(c, sh)) return false;
     int hole_base, movers_below, movers_above, total_movers, dummy0, dummy1;
-    group_counts(c, sh, prev_partials(c), 0, &hole_base, &dummy0, &dummy1);
-    group_counts(c, sh, prev_partials(c), 1, &movers_below, &movers_above, &total_movers);
+    group_counts(c, sh, 0, &hole_base, &dummy0, &dummy1);
+    group_counts(c, sh, 1, &movers_below, &movers_above, &total_movers);
     int *holes = D.scratch;
     int *movers = D.scratch + D.l;
     {
         int h_run = 0, m_run = 0;
-        for (int base = c.a0; base < c.a1; base += blockDim.x) {
-            const int p = base + threadIdx.x;
+        for (int base = 0; base < c.a1 - c.a0; base += blockDim.x) {
+            const int k = base + threadIdx.x;
+            const int p = c.a0 + k;
             bool s = false;
-            if (p < c.a1) s = be_shrunk(nu, D.status[p], D.y[p], D.G[p], g);
+            if (p < c.a1) s = be_shrunk(nu, c.sS[k], c.sY[k], c.sG[k], g);
             const int isH = (p < c.a1 && p < K && s) ? 1 : 0;
             const int isM = (p < c.a1 && p >= K && !s) ? 1 : 0;
             int totH, totM;
@@ -772,13 +872,14 @@ __device__ bool do_shrinking(Ctx &c, Shared &sh, int &unshrink)
             m_run += totM;
         }
     }
-    if (!sync_group(c, sh)) return false;
+    if (!exchange(c, sh)) return false;
     // 4. swap pair r: holes[r] <-> movers[r] (the reference's swap_index loop)
     for (long long r = (long long)c.rank * blockDim.x + threadIdx.x; r < total_movers; r += (long long)c.nb * blockDim.x)
-        swap_pos(D, holes[r], movers[r]);
-    if (!sync_group(c, sh)) return false;
+        swap_pos(D, __ldcg(&holes[r]), __ldcg(&movers[r]));
+    if (!exchange(c, sh)) return false;
     c.A = K;
     set_chunks(c);
+    chunk_load(c);
     return true;
 }
 
@@ -786,151 +887,167 @@ __device__ bool do_shrinking(Ctx &c, Shared &sh, int &unshrink)
 // I_up scan of my chunk (first half of WSS3): per track the max of -y_t G_t
 // with its payload.  C-SVC uses track 0 only; nu-SVC: track 0 = y=+1, 1 = y=-1.
 // --------------------------------------------------------------------------
-__device__ void iup_write(const Ctx &c, Shared &sh, double (&v)[2], int (&ix)[2])
+__device__ void iup_publish(const Ctx &c, Shared &sh, double (&v)[2], int (&ix)[2])
 {
-    const InstanceDesc &D = *c.D;
     const int kind[2] = {0, 0};
     block_reduce<2>(sh.red, v, ix, kind);
     if (threadIdx.x == 0) {
         Partial *pp = my_partial(c);
         for (int k = 0; k < 2; k++) {
             const int p = ix[k];
+            const int q = p - c.a0;
             pp->v[3 * k + 0] = v[k];
             pp->n[4 * k + 0] = p;
-            pp->v[3 * k + 1] = p >= 0 ? D.alpha[p] : 0.0;
-            pp->v[3 * k + 2] = p >= 0 ? D.QD[p] : 0.0;
-            pp->n[4 * k + 1] = p >= 0 ? D.pos_local[p] : 0;
-            pp->n[4 * k + 2] = p >= 0 ? D.pos_row[p] : 0;
-            pp->n[4 * k + 3] = p >= 0 ? D.y[p] : 0;
+            if (p >= 0) {
+                pp->v[3 * k + 1] = c.sA[q];
+                pp->v[3 * k + 2] = c.sQD[q];
+                pp->n[4 * k + 1] = c.sCol[q];
+                pp->n[4 * k + 2] = c.sRow[q];
+                pp->n[4 * k + 3] = c.sY[q];
+            }
         }
     }
 }
 
 __device__ void scan_iup(Ctx &c, Shared &sh)
 {
-    const InstanceDesc &D = *c.D;
-    const int nu = D.nu;
+    const int nu = c.D->nu;
     double v[2] = {-SVMB_INF, -SVMB_INF};
     int ix[2] = {-1, -1};
-    for (int p = c.a0 + threadIdx.x; p < c.a1; p += blockDim.x) {
-        const unsigned char s = D.status[p];
-        const double G = D.G[p];
-        if (D.y[p] == +1) {
-            if (s != ST_UPPER) better_max(v[0], ix[0], -G, p);
+    for (int k = threadIdx.x; k < c.a1 - c.a0; k += blockDim.x) {
+        const unsigned char s = c.sS[k];
+        const double G = c.sG[k];
+        if (c.sY[k] == +1) {
+            if (s != ST_UPPER) better_max(v[0], ix[0], -G, c.a0 + k);
         } else {
-            if (s != ST_LOWER) better_max(v[nu], ix[nu], G, p);
+            if (s != ST_LOWER) better_max(v[nu], ix[nu], G, c.a0 + k);
         }
     }
-    iup_write(c, sh, v, ix);
+    iup_publish(c, sh, v, ix);
 }
 
-// Evaluate the Q rows of sources (positions src_pos, rows src_row) into cache
-// slots on positions [lo,hi) of my chunk.
+// Evaluate the Q rows of `ns` (<= 2) sources into cache slots on my chunk of
+// [0,A) (tail = 0, from shared memory) or of [A,l) (tail = 1, global state).
 template <int FORM>
-__device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const int *src_y,
-                          const long long *slot, int lo, int hi)
+__device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const int *src_y, const long long *slot,
+                          int tail)
 {
     const InstanceDesc &D = *c.D;
     if (ns == 0) return;
-    stage_sources(D, c.dyn, sh.ss, src_row, ns);
-    double xs[kSrcBatch];
-    for (int k = 0; k < ns; k++) xs[k] = D.x.xsq ? D.x.xsq[src_row[k]] : 0.0;
-    for (int p = lo + threadIdx.x; p < hi; p += blockDim.x) {
+    stage_sources(D, c.stage, sh.ss, src_row, ns);
+    double xs[2];
+    for (int k = 0; k < 2; k++) xs[k] = (k < ns && D.x.xsq) ? D.x.xsq[src_row[k]] : 0.0;
+    float *dst0 = D.cache.data + slot[0] * D.cache.stride;
+    float *dst1 = ns > 1 ? D.cache.data + slot[1] * D.cache.stride : dst0;
+    const int lo = tail ? c.t0 : 0, hi = tail ? c.t1 : c.a1 - c.a0;
+    for (int k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+        int r, yp, col;
+        if (tail) {
+            r = D.pos_row[k];
+            yp = D.y[k];
+            col = D.pos_local[k];
+        } else {
+            r = c.sRow[k];
+            yp = c.sY[k];
+            col = c.sCol[k];
+        }
         double dots[kSrcBatch];
-        const int r = D.pos_row[p];
         row_dots<FORM>(D, sh.ss, ns, r, dots);
         const double xe = D.x.xsq ? D.x.xsq[r] : 0.0;
-        const int yp = D.y[p];
-        const long long col = D.pos_local[p];
-        for (int k = 0; k < ns; k++)
-            D.cache.data[slot[k] * D.cache.stride + col] = q_value(D.kp, src_y[k] * yp, dots[k], xs[k], xe);
+        dst0[col] = q_value(D.kp, src_y[0] * yp, dots[0], xs[0], xe);
+        if (ns > 1) dst1[col] = q_value(D.kp, src_y[1] * yp, dots[1], xs[1], xe);
     }
-    unstage_sources(D, c.dyn, sh.ss);
+    unstage_sources(D, c.stage, sh.ss);
 }
 
 // --------------------------------------------------------------------------
 // the persistent solver
 // --------------------------------------------------------------------------
 template <int FORM>
-__device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, float *dyn)
+__device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsigned char *dyn)
 {
     Ctx c;
     c.D = &D;
-    c.dyn = dyn;
     c.rank = rank;
     c.nb = D.nblocks;
     c.A = D.l;
     c.epoch = 0;
     c.phase = 0;
+    {
+        // dynamic shared memory: [stage][G][alpha][QD][col][row][y][status]
+        size_t off = (size_t)D.stage_cap * D.stage_lds * sizeof(float);
+        off = (off + 15) & ~(size_t)15;
+        c.stage = reinterpret_cast<float *>(dyn);
+        const size_t cap = (size_t)D.chunk_cap;
+        c.sG = reinterpret_cast<double *>(dyn + off); off += cap * 8;
+        c.sA = reinterpret_cast<double *>(dyn + off); off += cap * 8;
+        c.sQD = reinterpret_cast<double *>(dyn + off); off += cap * 8;
+        c.sCol = reinterpret_cast<int *>(dyn + off); off += cap * 4;
+        c.sRow = reinterpret_cast<int *>(dyn + off); off += cap * 4;
+        c.sY = reinterpret_cast<signed char *>(dyn + off); off += cap;
+        c.sS = reinterpret_cast<unsigned char *>(dyn + off);
+    }
     set_chunks(c);
     const int l = D.l;
     const int nu = D.nu;
     long long iter = 0;
     int unshrink = 0;
     int status = 0;
+    // block 0 / thread 0 work counters and section timers
+    long long cnt_active = 0, cnt_q = 0, cnt_look = 0, cnt_hit = 0;
+    long long prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long tmark = clock64();
+    const long long tstart = tmark;
+#define SVMB_PROF(k)                                   \
+    do {                                               \
+        if (threadIdx.x == 0) {                        \
+            const long long now_ = clock64();          \
+            prof[k] += now_ - tmark;                   \
+            tmark = now_;                              \
+        }                                              \
+    } while (0)
     if (threadIdx.x == 0) { sh.cs.nprev = 0; sh.cs.ncur = 0; }
     if (!D.x.X && D.stage_cap > 0)
-        for (long long k = threadIdx.x; k < (long long)D.stage_lds * D.stage_cap; k += blockDim.x) dyn[k] = 0.0f;
+        for (long long k = threadIdx.x; k < (long long)D.stage_lds * D.stage_cap; k += blockDim.x) c.stage[k] = 0.0f;
     __syncthreads();
 
-    // ---- initial state (svm.cpp:525-572, QD svm.cpp:1321-1327) ----
+    // ---- initial state (svm.cpp:525-572, QD svm.cpp:1321-1327) on the global copies ----
     {
-        const int lo = (int)((long long)l * rank / c.nb), hi = (int)((long long)l * (rank + 1) / c.nb);
-        for (int p = lo + threadIdx.x; p < hi; p += blockDim.x) {
+        for (int p = c.a0 + threadIdx.x; p < c.a1; p += blockDim.x) {
             D.status[p] = status_of(D.alpha[p], get_C(D, D.y[p]));
             const int r = D.pos_row[p];
             const double xs = D.x.xsq ? D.x.xsq[r] : 0.0;
-            double dot;
-            if (D.x.xsq) {
-                dot = xs;   // dot(x,x) is exactly what xsq holds
-            } else {
-                double acc = 0.0;
-                float accf = 0.0f;
-                if (D.x.X) {
-                    const float4 *row = reinterpret_cast<const float4 *>(D.x.X + (long long)r * D.x.ld);
-                    for (int k = 0; k < (D.x.ld >> 2); k++) {
-                        const float4 v = __ldg(row + k);
-                        acc = fma((double)v.x, (double)v.x, acc); acc = fma((double)v.y, (double)v.y, acc);
-                        acc = fma((double)v.z, (double)v.z, acc); acc = fma((double)v.w, (double)v.w, acc);
-                        accf = fmaf(v.x, v.x, accf); accf = fmaf(v.y, v.y, accf);
-                        accf = fmaf(v.z, v.z, accf); accf = fmaf(v.w, v.w, accf);
-                    }
-                } else {
-                    for (long long e = D.x.rowptr[r]; e < D.x.rowptr[r + 1]; e++) {
-                        const float v = D.x.val[e];
-                        acc = fma((double)v, (double)v, acc);
-                        accf = fmaf(v, v, accf);
-                    }
-                }
-                dot = FORM == FORM_EXACT ? acc : (double)accf;
-            }
-            D.QD[p] = kernel_from_dot(D.kp, dot, xs, xs);
+            // dot(x,x) in feature order is exactly what xsq holds
+            D.QD[p] = kernel_from_dot(D.kp, xs, xs, xs);
             D.G[p] = D.p[p];
             D.G_bar[p] = 0.0;
         }
-        if (!sync_group(c, sh)) goto fail;
+        if (!exchange(c, sh)) goto fail;
         int any = 0;
         for (int p = threadIdx.x; p < l; p += blockDim.x) any |= D.alpha[p] > 0 ? 1 : 0;
         any = __syncthreads_or(any);
         if (any) {
-            accumulate_rows<FORM>(c, sh, l, 0, 1, lo, hi);
-            if (!sync_group(c, sh)) goto fail;
+            accumulate_rows<FORM>(c, sh, l, 0, 1, c.a0, c.a1);
+            if (!exchange(c, sh)) goto fail;
         }
+        chunk_load(c);
     }
 
     {
         const long long max_iter = D.max_iter;
         int counter = (l < 1000 ? l : 1000) + 1;
         scan_iup(c, sh);
-        if (!sync_group(c, sh)) goto fail;
+        if (!exchange(c, sh)) goto fail;
 
         while (iter < max_iter) {
             if (--counter == 0) {
                 counter = l < 1000 ? l : 1000;
                 if (D.shrinking) {
+                    SVMB_PROF(kProfBUpdate);
                     if (!do_shrinking<FORM>(c, sh, unshrink)) goto fail;
                     scan_iup(c, sh);
-                    if (!sync_group(c, sh)) goto fail;
+                    if (!exchange(c, sh)) goto fail;
+                    SVMB_PROF(kProfShrink);
                 }
             }
             int widened = 0;
@@ -944,27 +1061,25 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                 int ix[2] = {-1, -1};
                 const int kind[2] = {0, 0};
                 for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-                    better_max(v[0], ix[0], all[b].v[0], all[b].n[0]);
-                    better_max(v[1], ix[1], all[b].v[3], all[b].n[4]);
+                    better_max(v[0], ix[0], __ldcg(&all[b].v[0]), __ldcg(&all[b].n[0]));
+                    better_max(v[1], ix[1], __ldcg(&all[b].v[3]), __ldcg(&all[b].n[4]));
                 }
                 block_reduce<2>(sh.red, v, ix, kind);
+                // winners' payload, read by the thread that holds the winning record
+                for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
+                    for (int k = 0; k < 2; k++) {
+                        if (ix[k] >= 0 && __ldcg(&all[b].n[4 * k]) == ix[k]) {
+                            sh.bd[3 * k + 1] = __ldcg(&all[b].v[3 * k + 1]);
+                            sh.bd[3 * k + 2] = __ldcg(&all[b].v[3 * k + 2]);
+                            sh.bi[4 * k + 1] = __ldcg(&all[b].n[4 * k + 1]);
+                            sh.bi[4 * k + 2] = __ldcg(&all[b].n[4 * k + 2]);
+                            sh.bi[4 * k + 3] = __ldcg(&all[b].n[4 * k + 3]);
+                        }
+                    }
+                }
                 if (threadIdx.x == 0) {
                     sh.bd[0] = v[0]; sh.bi[0] = ix[0];
                     sh.bd[3] = v[1]; sh.bi[4] = ix[1];
-                }
-                __syncthreads();
-                // winners' payload, found by the thread that read the winning partial
-                for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-                    for (int k = 0; k < 2; k++) {
-                        const int w = sh.bi[4 * k];
-                        if (w >= 0 && all[b].n[4 * k] == w) {
-                            sh.bd[3 * k + 1] = all[b].v[3 * k + 1];
-                            sh.bd[3 * k + 2] = all[b].v[3 * k + 2];
-                            sh.bi[4 * k + 1] = all[b].n[4 * k + 1];
-                            sh.bi[4 * k + 2] = all[b].n[4 * k + 2];
-                            sh.bi[4 * k + 3] = all[b].n[4 * k + 3];
-                        }
-                    }
                 }
                 __syncthreads();
                 if (threadIdx.x == 0) {
@@ -978,6 +1093,8 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                             Lookup L = cache_lookup(sh.cs, D.cache, sh.bi[4 * k + 1], c.epoch, clk, whole);
                             sh.bl[k] = L.slot;
                             sh.bi[8 + k] = L.valid_active;
+                            cnt_look++;
+                            cnt_hit += L.valid_active;
                         }
                     }
                 }
@@ -990,8 +1107,8 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
             {
                 // evaluate the missing row(s) on my chunk
                 int ns = 0;
-                int srow[2], sy[2];
-                long long sslot[2];
+                int srow[2] = {0, 0}, sy[2] = {0, 0};
+                long long sslot[2] = {0, 0};
                 for (int k = 0; k < 2; k++) {
                     const int ik = k == 0 ? i0 : i1;
                     if (ik >= 0 && !sh.bi[8 + k]) {
@@ -1001,7 +1118,10 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                         ns++;
                     }
                 }
-                fill_rows<FORM>(c, sh, ns, srow, sy, sslot, c.a0, c.a1);
+                SVMB_PROF(kProfAReduce);
+                fill_rows<FORM>(c, sh, ns, srow, sy, sslot, 0);
+                cnt_q += (long long)ns * c.A;
+                SVMB_PROF(kProfAFill);
             }
             {
                 // second-order j scan on my chunk (svm.cpp:869-924 / :1120-1174)
@@ -1012,21 +1132,22 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                 const float *Qi1 = i1 >= 0 ? D.cache.data + sh.bl[1] * D.cache.stride : nullptr;
                 const double QDi0 = sh.bd[2], QDi1 = sh.bd[5];
                 const double two_yi0 = __dmul_rn(2.0, (double)sh.bi[3]);
-                for (int p = c.a0 + threadIdx.x; p < c.a1; p += blockDim.x) {
-                    const unsigned char s = D.status[p];
-                    const double G = D.G[p];
-                    const int col = D.pos_local[p];
-                    if (D.y[p] == +1) {
+                const int n = c.a1 - c.a0;
+                for (int k = threadIdx.x; k < n; k += blockDim.x) {
+                    const unsigned char s = c.sS[k];
+                    const double G = c.sG[k];
+                    const int col = c.sCol[k];
+                    if (c.sY[k] == +1) {
                         if (s != ST_LOWER) {
                             const double grad_diff = __dadd_rn(Gmax0, G);
                             v[1] = fmax(v[1], G);
                             if (grad_diff > 0) {
                                 double quad;
-                                if (!nu) quad = __dsub_rn(__dadd_rn(QDi0, D.QD[p]), __dmul_rn(two_yi0, (double)Qi0[col]));
-                                else quad = __dsub_rn(__dadd_rn(QDi0, D.QD[p]), (double)__fmul_rn(2.0f, Qi0[col]));
+                                if (!nu) quad = __dsub_rn(__dadd_rn(QDi0, c.sQD[k]), __dmul_rn(two_yi0, (double)Qi0[col]));
+                                else quad = __dsub_rn(__dadd_rn(QDi0, c.sQD[k]), (double)__fmul_rn(2.0f, Qi0[col]));
                                 const double num = __dmul_rn(grad_diff, grad_diff);
                                 const double od = quad > 0 ? -__ddiv_rn(num, quad) : -__ddiv_rn(num, kTau);
-                                better_min(v[0], ix[0], od, p);
+                                better_min(v[0], ix[0], od, c.a0 + k);
                             }
                         }
                     } else {
@@ -1035,11 +1156,11 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                             if (nu) v[2] = fmax(v[2], -G); else v[1] = fmax(v[1], -G);
                             if (grad_diff > 0) {
                                 double quad;
-                                if (!nu) quad = __dadd_rn(__dadd_rn(QDi0, D.QD[p]), __dmul_rn(two_yi0, (double)Qi0[col]));
-                                else quad = __dsub_rn(__dadd_rn(QDi1, D.QD[p]), (double)__fmul_rn(2.0f, Qi1[col]));
+                                if (!nu) quad = __dadd_rn(__dadd_rn(QDi0, c.sQD[k]), __dmul_rn(two_yi0, (double)Qi0[col]));
+                                else quad = __dsub_rn(__dadd_rn(QDi1, c.sQD[k]), (double)__fmul_rn(2.0f, Qi1[col]));
                                 const double num = __dmul_rn(grad_diff, grad_diff);
                                 const double od = quad > 0 ? -__ddiv_rn(num, quad) : -__ddiv_rn(num, kTau);
-                                better_min(v[0], ix[0], od, p);
+                                better_min(v[0], ix[0], od, c.a0 + k);
                             }
                         }
                     }
@@ -1051,15 +1172,17 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                     pp->v[0] = v[0]; pp->n[0] = j;
                     pp->v[1] = v[1]; pp->v[2] = v[2];
                     if (j >= 0) {
-                        const int cj = D.pos_local[j];
-                        pp->v[3] = D.G[j]; pp->v[4] = D.alpha[j]; pp->v[5] = D.QD[j];
-                        pp->n[1] = cj; pp->n[2] = D.pos_row[j]; pp->n[3] = D.y[j];
+                        const int q = j - c.a0;
+                        const int cj = c.sCol[q];
+                        pp->v[3] = c.sG[q]; pp->v[4] = c.sA[q]; pp->v[5] = c.sQD[q];
+                        pp->n[1] = cj; pp->n[2] = c.sRow[q]; pp->n[3] = c.sY[q];
                         pp->q[0] = Qi0 ? Qi0[cj] : 0.0f;
                         pp->q[1] = Qi1 ? Qi1[cj] : 0.0f;
                     }
                 }
             }
-            if (!sync_group(c, sh)) goto fail;
+            if (!exchange(c, sh)) goto fail;
+            SVMB_PROF(kProfAScan);
 
             // ======================= phase B =======================
             {
@@ -1068,21 +1191,19 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                 int ix[3] = {-1, -1, -1};
                 const int kind[3] = {1, 2, 2};
                 for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-                    better_min(v[0], ix[0], all[b].v[0], all[b].n[0]);
-                    v[1] = fmax(v[1], all[b].v[1]);
-                    v[2] = fmax(v[2], all[b].v[2]);
+                    better_min(v[0], ix[0], __ldcg(&all[b].v[0]), __ldcg(&all[b].n[0]));
+                    v[1] = fmax(v[1], __ldcg(&all[b].v[1]));
+                    v[2] = fmax(v[2], __ldcg(&all[b].v[2]));
                 }
                 block_reduce<3>(sh.red, v, ix, kind);
-                if (threadIdx.x == 0) { sh.bi[12] = ix[0]; sh.bd[12] = v[1]; sh.bd[13] = v[2]; }
-                __syncthreads();
                 for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-                    const int w = sh.bi[12];
-                    if (w >= 0 && all[b].n[0] == w) {
-                        sh.bd[14] = all[b].v[3]; sh.bd[15] = all[b].v[4]; sh.bd[16] = all[b].v[5];
-                        sh.bi[13] = all[b].n[1]; sh.bi[14] = all[b].n[2]; sh.bi[15] = all[b].n[3];
-                        sh.bd[17] = (double)all[b].q[0]; sh.bd[18] = (double)all[b].q[1];
+                    if (ix[0] >= 0 && __ldcg(&all[b].n[0]) == ix[0]) {
+                        sh.bd[14] = __ldcg(&all[b].v[3]); sh.bd[15] = __ldcg(&all[b].v[4]); sh.bd[16] = __ldcg(&all[b].v[5]);
+                        sh.bi[13] = __ldcg(&all[b].n[1]); sh.bi[14] = __ldcg(&all[b].n[2]); sh.bi[15] = __ldcg(&all[b].n[3]);
+                        sh.bd[17] = (double)__ldcg(&all[b].q[0]); sh.bd[18] = (double)__ldcg(&all[b].q[1]);
                     }
                 }
+                if (threadIdx.x == 0) { sh.bi[12] = ix[0]; sh.bd[12] = v[1]; sh.bd[13] = v[2]; }
                 __syncthreads();
             }
             const int j = sh.bi[12];
@@ -1094,19 +1215,20 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                     if (widened) break;
                     // reconstruct the whole gradient, widen, select again (svm.cpp:598-611)
                     if (c.A < l) {
+                        chunk_store(c);
+                        if (!exchange(c, sh)) goto fail;
                         if (!reconstruct<FORM>(c, sh)) goto fail;
-                        c.A = l;
-                        c.epoch++;
-                        set_chunks(c);
+                        widen(c);
                     }
                     widened = 1;
                     scan_iup(c, sh);
-                    if (!sync_group(c, sh)) goto fail;
+                    if (!exchange(c, sh)) goto fail;
                     goto select_again;
                 }
                 if (widened) counter = 1;
             }
             ++iter;
+            cnt_active += c.A;
             // the working pair; nu-SVC takes i from the track of y_j (svm.cpp:1179-1182)
             const int yj = sh.bi[15];
             const int tr = (nu && yj != +1) ? 1 : 0;
@@ -1125,14 +1247,18 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                 Lookup L = cache_lookup(sh.cs, D.cache, loc_j, c.epoch, clk, c.A == l);
                 sh.bl[2] = L.slot;
                 sh.bi[16] = L.valid_active;
+                cnt_look++;
+                cnt_hit += L.valid_active;
             }
             __syncthreads();
+            SVMB_PROF(kProfBReduce);
             const long long slot_j = sh.bl[2];
             if (!sh.bi[16]) {
-                const int srow[1] = {row_j};
-                const int sy[1] = {yj};
-                const long long ss[1] = {slot_j};
-                fill_rows<FORM>(c, sh, 1, srow, sy, ss, c.a0, c.a1);
+                const int srow[2] = {row_j, 0};
+                const int sy[2] = {yj, 0};
+                const long long ss[2] = {slot_j, 0};
+                fill_rows<FORM>(c, sh, 1, srow, sy, ss, 0);
+                cnt_q += c.A;
             }
             // two-variable analytic step (svm.cpp:636-721), identical in every block
             const double C_i = get_C(D, yi), C_j = get_C(D, yj);
@@ -1199,16 +1325,18 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                 }
                 __syncthreads();
                 int ns = 0;
-                int srow[2], sy[2];
-                long long sslot[2];
+                int srow[2] = {0, 0}, sy[2] = {0, 0};
+                long long sslot[2] = {0, 0};
                 if (sh.bi[17]) { srow[ns] = row_i; sy[ns] = yi; sslot[ns] = slot_i; ns++; }
                 if (sh.bi[18]) { srow[ns] = row_j; sy[ns] = yj; sslot[ns] = slot_j; ns++; }
-                fill_rows<FORM>(c, sh, ns, srow, sy, sslot, c.t0, c.t1);
+                fill_rows<FORM>(c, sh, ns, srow, sy, sslot, 1);
+                cnt_q += (long long)ns * (l - c.A);
             }
+            SVMB_PROF(kProfBFill);
             // owners publish alpha/status of i and j
             if (threadIdx.x == 0) {
-                if (i >= c.a0 && i < c.a1) { D.alpha[i] = ai; D.status[i] = new_si; }
-                if (j >= c.a0 && j < c.a1) { D.alpha[j] = aj; D.status[j] = new_sj; }
+                if (i >= c.a0 && i < c.a1) { c.sA[i - c.a0] = ai; c.sS[i - c.a0] = new_si; }
+                if (j >= c.a0 && j < c.a1) { c.sA[j - c.a0] = aj; c.sS[j - c.a0] = new_sj; }
             }
             __syncthreads();
             // G update on my chunk (svm.cpp:732-735) + G_bar (svm.cpp:744-769) + next I_up scan
@@ -1217,22 +1345,24 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                 const float *Qj = D.cache.data + slot_j * D.cache.stride;
                 double v[2] = {-SVMB_INF, -SVMB_INF};
                 int ix[2] = {-1, -1};
-                for (int p = c.a0 + threadIdx.x; p < c.a1; p += blockDim.x) {
-                    const int col = D.pos_local[p];
+                const int n = c.a1 - c.a0;
+                for (int k = threadIdx.x; k < n; k += blockDim.x) {
+                    const int col = c.sCol[k];
                     const float qi = Qi[col], qj = Qj[col];
-                    const double G = __dadd_rn(D.G[p], __dadd_rn(__dmul_rn((double)qi, dai), __dmul_rn((double)qj, daj)));
-                    D.G[p] = G;
+                    const double G = __dadd_rn(c.sG[k], __dadd_rn(__dmul_rn((double)qi, dai), __dmul_rn((double)qj, daj)));
+                    c.sG[k] = G;
                     if (bar_i || bar_j) {
+                        const int p = c.a0 + k;
                         double gb = D.G_bar[p];
                         if (bar_i) gb = (old_si == ST_UPPER) ? __dsub_rn(gb, __dmul_rn(C_i, (double)qi)) : __dadd_rn(gb, __dmul_rn(C_i, (double)qi));
                         if (bar_j) gb = (old_sj == ST_UPPER) ? __dsub_rn(gb, __dmul_rn(C_j, (double)qj)) : __dadd_rn(gb, __dmul_rn(C_j, (double)qj));
                         D.G_bar[p] = gb;
                     }
-                    const unsigned char s = D.status[p];
-                    if (D.y[p] == +1) {
-                        if (s != ST_UPPER) better_max(v[0], ix[0], -G, p);
+                    const unsigned char s = c.sS[k];
+                    if (c.sY[k] == +1) {
+                        if (s != ST_UPPER) better_max(v[0], ix[0], -G, c.a0 + k);
                     } else {
-                        if (s != ST_LOWER) better_max(v[nu], ix[nu], G, p);
+                        if (s != ST_LOWER) better_max(v[nu], ix[nu], G, c.a0 + k);
                     }
                 }
                 if (bar_i || bar_j) {
@@ -1244,11 +1374,14 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
                         D.G_bar[p] = gb;
                     }
                 }
-                iup_write(c, sh, v, ix);
+                iup_publish(c, sh, v, ix);
             }
-            if (!sync_group(c, sh)) goto fail;
+            if (!exchange(c, sh)) goto fail;
+            SVMB_PROF(kProfBUpdate);
         }
 
+        chunk_store(c);
+        if (!exchange(c, sh)) goto fail;
         if (iter >= max_iter) {
             status = 1;
             if (c.A < l) {
@@ -1261,8 +1394,6 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
     // ---- rho (svm.cpp:1013-1049 / 1260-1308), objective (:795-802), alpha out (:805-808) ----
     // The sums run sequentially in position order (bit-exact with the reference), on block 0.
     if (rank == 0) {
-        double *cv = reinterpret_cast<double *>(sh.red.v);   // not used; keeps the compiler quiet
-        (void)cv;
         __shared__ double chv[kThreads], chg[kThreads];
         __shared__ unsigned char chs[kThreads];
         __shared__ signed char chy[kThreads];
@@ -1317,6 +1448,12 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, floa
             o.unshrink = unshrink;
             o.obj = __ddiv_rn(objv, 2.0);
             o.gap = 0;
+            o.sum_active = cnt_active;
+            o.q_evals = cnt_q;
+            o.lookups = cnt_look;
+            o.hits = cnt_hit;
+            for (int k = 0; k < 7; k++) o.prof[k] = prof[k];
+            o.prof[kProfTotal] = clock64() - tstart;
             if (!nu) {
                 o.rho = nr_free > 0 ? __ddiv_rn(sum_free, (double)nr_free) : __ddiv_rn(__dadd_rn(ub, lb), 2.0);
                 o.r = 0;
@@ -1341,8 +1478,11 @@ fail:
         SolveOut o;
         o.iters = iter; o.rho = 0; o.obj = 0; o.r = 0; o.status = -1; o.active_size = c.A;
         o.unshrink = unshrink; o.nr_free = 0; o.gap = 0;
+        o.sum_active = cnt_active; o.q_evals = cnt_q; o.lookups = cnt_look; o.hits = cnt_hit;
+        for (int k = 0; k < 8; k++) o.prof[k] = prof[k];
         *D.out = o;
     }
+#undef SVMB_PROF
 }
 
 template <int FORM>
@@ -1350,7 +1490,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 smo_persistent(const InstanceDesc *__restrict__ insts, const int *__restrict__ block_inst)
 {
     __shared__ Shared sh;
-    extern __shared__ __align__(16) float dyn[];
+    extern __shared__ __align__(16) unsigned char dyn[];
     const int inst = block_inst[blockIdx.x];
     const InstanceDesc &D = insts[inst];
     const int rank = blockIdx.x - D.block0;
@@ -1369,7 +1509,7 @@ __global__ void xsq_kernel(DevX x, int n, double *out, int form)
         if (x.X) {
             const float4 *row = reinterpret_cast<const float4 *>(x.X + (long long)r * x.ld);
             for (int k = 0; k < (x.ld >> 2); k++) {
-                float4 v = __ldg(row + k);
+                const float4 v = __ldg(row + k);
                 acc = fma((double)v.x, (double)v.x, acc); acc = fma((double)v.y, (double)v.y, acc);
                 acc = fma((double)v.z, (double)v.z, acc); acc = fma((double)v.w, (double)v.w, acc);
                 accf = fmaf(v.x, v.x, accf); accf = fmaf(v.y, v.y, accf);
@@ -1377,13 +1517,21 @@ __global__ void xsq_kernel(DevX x, int n, double *out, int form)
             }
         } else {
             for (long long e = x.rowptr[r]; e < x.rowptr[r + 1]; e++) {
-                float v = x.val[e];
+                const float v = x.val[e];
                 acc = fma((double)v, (double)v, acc);
                 accf = fmaf(v, v, accf);
             }
         }
         out[r] = form == FORM_EXACT ? acc : (double)accf;
     }
+}
+
+// CSR -> dense rows on the device (rows [n][ld] must be zeroed)
+__global__ void scatter_dense_kernel(const long long *rowptr, const int *col, const float *val, int n, int ld, float *X)
+{
+    for (int r = blockIdx.x; r < n; r += gridDim.x)
+        for (long long e = rowptr[r] + threadIdx.x; e < rowptr[r + 1]; e += blockDim.x)
+            X[(long long)r * ld + col[e]] = val[e];
 }
 
 // host-callable launchers ----------------------------------------------------
@@ -1393,6 +1541,14 @@ cudaError_t launch_xsq(const DevX &x, int n, double *out, int form, cudaStream_t
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (blocks < 1) blocks = 1;
     xsq_kernel<<<blocks, 256, 0, s>>>(x, n, out, form);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_dense(const long long *rowptr, const int *col, const float *val, int n, int ld, float *X,
+                                 cudaStream_t s)
+{
+    const int blocks = n < 148 * 16 ? (n > 0 ? n : 1) : 148 * 16;
+    scatter_dense_kernel<<<blocks, 128, 0, s>>>(rowptr, col, val, n, ld, X);
     return cudaGetLastError();
 }
 
@@ -1414,6 +1570,14 @@ cudaError_t smo_max_blocks(int form, size_t dyn_smem, int *blocks_per_sm)
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, kThreads, dyn_smem);
+}
+
+int smo_static_smem()
+{
+    cudaFuncAttributes a, b;
+    if (cudaFuncGetAttributes(&a, (const void *)smo_persistent<FORM_EXACT>) != cudaSuccess) return 16384;
+    if (cudaFuncGetAttributes(&b, (const void *)smo_persistent<FORM_FP32>) != cudaSuccess) return (int)a.sharedSizeBytes;
+    return (int)(a.sharedSizeBytes > b.sharedSizeBytes ? a.sharedSizeBytes : b.sharedSizeBytes);
 }
 
 }  // namespace svmb

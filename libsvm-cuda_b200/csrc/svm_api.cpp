@@ -206,6 +206,11 @@ DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResul
     st.status = R.out.status;
     st.active_size = R.out.active_size;
     st.seconds = R.seconds;
+    st.sum_active = R.out.sum_active;
+    st.q_evals = R.out.q_evals;
+    st.lookups = R.out.lookups;
+    st.hits = R.out.hits;
+    for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
     {
         std::lock_guard<std::mutex> g(g_stats_mu);
         g_last_stats.push_back(st);

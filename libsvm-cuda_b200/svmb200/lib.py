@@ -25,10 +25,14 @@ class EngineError(RuntimeError):
 class SolveStats(C.Structure):
     _fields_ = [("iters", C.c_longlong), ("obj", C.c_double), ("rho", C.c_double), ("r", C.c_double),
                 ("l", C.c_int), ("nr_sv", C.c_int), ("nr_bsv", C.c_int), ("status", C.c_int),
-                ("active_size", C.c_int), ("pad", C.c_int), ("seconds", C.c_double)]
+                ("active_size", C.c_int), ("pad", C.c_int), ("seconds", C.c_double),
+                ("sum_active", C.c_longlong), ("q_evals", C.c_longlong), ("lookups", C.c_longlong),
+                ("hits", C.c_longlong), ("prof_cycles", C.c_longlong * 8)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("pad", "prof_cycles")}
+        d["prof_cycles"] = list(self.prof_cycles)
+        return d
 
 
 class SvmbParams(C.Structure):
@@ -70,6 +74,7 @@ def _load(path: str) -> C.CDLL:
     lib.svm_check_parameter.argtypes = [_P(svm_problem), _P(svm_parameter)]
     lib.svm_set_print_string_function.argtypes = [cabi.PRINT_FUNC]
     lib.svmb_last_error.restype = C.c_char_p
+    lib.svmb_kernel_launches.restype = C.c_longlong
     lib.svmb_set_option.argtypes = [C.c_char_p, C.c_longlong]
     lib.svmb_last_train_stats.argtypes = [_P(SolveStats), C.c_int]
     lib.svmb_predict_batch.argtypes = [_P(svm_model), C.c_void_p, C.c_int, _P(C.c_double), _P(C.c_double)]
@@ -133,6 +138,9 @@ class Engine:
     def _ok(self, rc: int, what: str):
         if rc != 0:
             raise EngineError(f"{what}: {self.error()}")
+
+    def launches(self) -> int:
+        return int(self.lib.svmb_kernel_launches())
 
     def available(self) -> bool:
         return bool(self.lib.svmb_device_available())
