@@ -42,6 +42,9 @@ typedef struct svmb_solve_stats {
     long long q_evals;
     long long lookups;
     long long hits;
+    long long fills;            /* row-evaluation passes */
+    long long prefetched;       /* rows evaluated ahead of need */
+    long long prefetch_used;    /* of those, rows a later lookup hit */
     long long prof_cycles[8];   /* SM cycles per loop section (diagnostics) */
 } svmb_solve_stats;
 
@@ -60,6 +63,7 @@ typedef struct svmb_params {
     double cache_mb;     /* Q-row cache budget per solve, MB (svm_parameter.cache_size) */
     int form;            /* SVMB_FORM_* */
     int blocks;          /* thread blocks per solve; 0 = automatic */
+    int prefetch;        /* kernel rows evaluated per cache-miss pass (1 = only the missing row); 0 = automatic */
 } svmb_params;
 
 #define SVMB_FORM_EXACT 0   /* fp32 features, fp64 accumulation in feature order */
@@ -76,7 +80,8 @@ int svmb_device_available(void);                /* 1 if a CUDA device can be use
 /* Process-wide engine options used by svm_train / svm_cross_validation:
  *   "form"   SVMB_FORM_EXACT (default) or SVMB_FORM_FP32
  *   "blocks" thread blocks per solve (0 = automatic)
- *   "layout" -1 automatic, 0 CSR, 1 dense device layout of the rows */
+ *   "layout" -1 automatic, 0 CSR, 1 dense device layout of the rows
+ *   "prefetch" kernel rows per cache-miss pass (1 = none, 0 = automatic) */
 int svmb_set_option(const char *name, long long value);
 
 /* Per-subproblem statistics of the last svm_train / svm_cross_validation

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -91,13 +92,16 @@ int solve_many(const svmb::DeviceRows &rows, int ninst, const int *inst_ptr, con
     prm.cache_mb = params[0].cache_mb;
     prm.form = params[0].form;
     prm.blocks_override = params[0].blocks;
+    prm.prefetch = params[0].prefetch;
     for (int k = 1; k < ninst; k++)
         if (params[k].eps != prm.eps || params[k].shrinking != prm.shrinking || params[k].cache_mb != prm.cache_mb) {
             svmb::set_error("instances of one launch must share eps, shrinking and cache_mb");
             return -1;
         }
     std::vector<svmb::SolveResult> res;
+    const auto t0 = std::chrono::steady_clock::now();
     if (svmb::solve_batch(rows, subs, prm, res, 0) != 0) return -1;
+    const auto t1 = std::chrono::steady_clock::now();
     for (int k = 0; k < ninst; k++) {
         const svmb::SubProblem &sp = subs[k];
         const svmb::SolveResult &R = res[k];
@@ -129,7 +133,11 @@ int solve_many(const svmb::DeviceRows &rows, int ninst, const int *inst_ptr, con
             st.q_evals = R.out.q_evals;
             st.lookups = R.out.lookups;
             st.hits = R.out.hits;
+            st.fills = R.out.fills;
+            st.prefetched = R.out.prefetched;
+            st.prefetch_used = R.out.prefetch_used;
             for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
+            (void)t0; (void)t1;
             for (int i = 0; i < l; i++) {
                 const double v = alpha_out[a + i];
                 if (v != 0) {

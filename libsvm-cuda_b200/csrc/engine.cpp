@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <cstdlib>
 #include <mutex>
 
 #include "svm.h"
@@ -62,23 +63,54 @@ cudaError_t xfer(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind)
 // calls (copies from it run at full PCIe/C2C bandwidth).
 namespace {
 std::mutex g_pin_mu;
-void *g_pin = nullptr;
-size_t g_pin_bytes = 0;
+void *g_pin[2] = {nullptr, nullptr};
+size_t g_pin_bytes[2] = {0, 0};
 }  // namespace
-void *pinned_staging(size_t bytes)
+// slot 0: row uploads (under g_pin_mu); slot 1: solver state (under the arena lock)
+void *pinned_staging_slot(int slot, size_t bytes)
 {
-    if (bytes <= g_pin_bytes) return g_pin;
-    if (g_pin) cudaFreeHost(g_pin);
-    g_pin = nullptr;
-    g_pin_bytes = 0;
-    size_t want = std::max<size_t>(bytes, 1 << 20);
-    if (cudaHostAlloc(&g_pin, want, cudaHostAllocDefault) != cudaSuccess) {
-        g_pin = nullptr;
+    if (bytes <= g_pin_bytes[slot]) return g_pin[slot];
+    if (g_pin[slot]) cudaFreeHost(g_pin[slot]);
+    g_pin[slot] = nullptr;
+    g_pin_bytes[slot] = 0;
+    const size_t want = std::max<size_t>(bytes + bytes / 4, 1 << 20);
+    if (cudaHostAlloc(&g_pin[slot], want, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        g_pin[slot] = nullptr;
         return nullptr;
     }
-    g_pin_bytes = want;
-    return g_pin;
+    g_pin_bytes[slot] = want;
+    return g_pin[slot];
 }
+void *pinned_staging(size_t bytes) { return pinned_staging_slot(0, bytes); }
+
+// SVMB_TRACE=1 prints host-side stage times of every solve_batch to stderr
+static bool trace_on()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("SVMB_TRACE");
+        on = (e && *e == '1') ? 1 : 0;
+    }
+    return on == 1;
+}
+struct StageClock {
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now(), last = t0;
+    std::string log;
+    void mark(const char *what)
+    {
+        if (!trace_on()) return;
+        const auto now = std::chrono::steady_clock::now();
+        char buf[96];
+        snprintf(buf, sizeof buf, " %s=%.2fms", what, std::chrono::duration<double, std::milli>(now - last).count());
+        log += buf;
+        last = now;
+    }
+    ~StageClock()
+    {
+        if (trace_on() && !log.empty()) fprintf(stderr, "[svmb] solve_batch%s\n", log.c_str());
+    }
+};
 
 int device_sm_count()
 {
@@ -166,15 +198,22 @@ int upload_csr(const long long *rowptr, const int *col, const float *val, int n,
 
 int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cudaStream_t s)
 {
-    // CSR with 0-based columns; libsvm indices start at 1 (index 0 is kept as a column when present)
+    // CSR with 0-based columns; libsvm indices start at 1 (index 0 is kept as a
+    // column when present).  Rows are converted in parallel on the host.
+    std::vector<long long> cnt((size_t)n + 1, 0);
     int min_index = INT_MAX, max_index = 0;
-    long long nnz = 0;
-    for (int r = 0; r < n; r++)
+#pragma omp parallel for schedule(static) reduction(min : min_index) reduction(max : max_index)
+    for (int r = 0; r < n; r++) {
+        long long c = 0;
         for (const svm_node *p = x[r]; p->index != -1; ++p) {
             min_index = std::min(min_index, p->index);
             max_index = std::max(max_index, p->index);
-            nnz++;
+            c++;
         }
+        cnt[r + 1] = c;
+    }
+    for (int r = 0; r < n; r++) cnt[r + 1] += cnt[r];
+    const long long nnz = cnt[n];
     if (nnz && min_index < 0) {
         set_error("feature index < 0");
         return -1;
@@ -192,16 +231,15 @@ int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cud
     long long *rp = (long long *)pin;
     int *col = (int *)(pin + (((size_t)n + 1) * 8));
     float *val = (float *)(pin + (((size_t)n + 1) * 8) + (size_t)nnz * 4);
-    long long k = 0;
+    memcpy(rp, cnt.data(), sizeof(long long) * ((size_t)n + 1));
+#pragma omp parallel for schedule(static)
     for (int r = 0; r < n; r++) {
-        rp[r] = k;
-        for (const svm_node *p = x[r]; p->index != -1; ++p) {
+        long long k = rp[r];
+        for (const svm_node *p = x[r]; p->index != -1; ++p, ++k) {
             col[k] = p->index - base;
             val[k] = (float)p->value;
-            k++;
         }
     }
-    rp[n] = k;
     const int d = nnz ? max_index - base + 1 : 1;
     return upload_csr(rp, col, val, n, d, out, force, s);
 }
@@ -220,12 +258,69 @@ struct Bump {
     }
 };
 
-struct InstanceAlloc {
-    char *base = nullptr;
-    size_t bytes = 0;
+// Byte layout of one instance's device state (all offsets 256-aligned).
+struct InstanceLayout {
+    size_t G, Gb, A, P, QD, Al, Y, S, PL, PR, Sc, Out, Sync, Part, Tag, Ep, St, Data, bytes;
+    int sets, ways;
 };
 
+InstanceLayout instance_layout(int l, int nb, double cache_mb)
+{
+    (void)nb;
+    InstanceLayout L;
+    memset(&L, 0, sizeof(L));
+    // cache geometry: rows of l floats, at least 4, at most 2l slots
+    long long slots = (long long)std::floor(cache_mb * (1 << 20) / (4.0 * std::max(l, 1)));
+    slots = std::max<long long>(slots, 4);
+    slots = std::min<long long>(slots, std::max<long long>(4, 2LL * l));
+    L.ways = (int)std::min<long long>(kMaxWays, slots);
+    L.sets = (int)(slots / L.ways);
+    const size_t ns = (size_t)L.sets * L.ways;
+    Bump b;
+    L.G = b.take<double>(l); L.Gb = b.take<double>(l); L.QD = b.take<double>(l);
+    L.S = b.take<unsigned char>(l);
+    L.PL = b.take<int>(l); L.Sc = b.take<int>(2 * (size_t)l);
+    L.Data = b.take<float>(ns * (size_t)l);
+    L.bytes = (b.off + 255) & ~size_t(255);
+    return L;
+}
+
+// Grow-only device arena for solver state: one buffer reused by every launch
+// (allocating and freeing gigabytes of Q-row caches per call costs more than
+// a small solve).  Calls into the engine are serialised on it.
+std::mutex g_arena_mu;
+char *g_arena = nullptr;
+size_t g_arena_bytes = 0;
+
+char *arena_reserve(size_t bytes)
+{
+    if (bytes <= g_arena_bytes) return g_arena;
+    if (g_arena) cudaFree(g_arena);
+    g_arena = nullptr;
+    g_arena_bytes = 0;
+    const size_t want = bytes + bytes / 4;
+    if (cudaMalloc(&g_arena, want) != cudaSuccess) {
+        cudaGetLastError();
+        if (cudaMalloc(&g_arena, bytes) != cudaSuccess) {
+            g_arena = nullptr;
+            return nullptr;
+        }
+        g_arena_bytes = bytes;
+        return g_arena;
+    }
+    g_arena_bytes = want;
+    return g_arena;
+}
+
 }  // namespace
+
+void release_arena()
+{
+    std::lock_guard<std::mutex> g(g_arena_mu);
+    if (g_arena) cudaFree(g_arena);
+    g_arena = nullptr;
+    g_arena_bytes = 0;
+}
 
 int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm,
                 std::vector<SolveResult> &res, cudaStream_t s)
@@ -233,6 +328,8 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
     const int ninst = (int)subs.size();
     res.assign(ninst, SolveResult());
     if (ninst == 0) return 0;
+    std::lock_guard<std::mutex> arena_lock(g_arena_mu);
+    StageClock clk;
     const int sms = device_sm_count();
     if (sms <= 0) {
         set_error("no CUDA device");
@@ -253,7 +350,8 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         stage_cap = (int)std::min<long long>(kSrcBatch, (budget / 2) / ((long long)std::max(rows.d, 1) * 4));
     }
     if (stage_cap < 2) stage_cap = 0;
-    const long long stage_bytes = (((long long)stage_cap * stage_lds * 4) + 15) & ~15LL;
+    long long stage_bytes = (((long long)stage_cap * stage_lds * 4) + 15) & ~15LL;
+    stage_bytes += kAuxBytes;   // transpose tiles / prefetch candidates
     const long long chunk_max = (budget - stage_bytes) / kChunkBytes;
     if (chunk_max < 64) {
         set_error("not enough shared memory for the solver state");
@@ -267,6 +365,7 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         return -1;
     }
     const int capacity = per_sm * sms;
+    clk.mark("setup");
     for (const SubProblem &sp : subs)
         if ((long long)sp.rows.size() > chunk_max * capacity) {
             set_error("problem too large: more positions than the device's blocks can hold in shared memory");
@@ -291,19 +390,29 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         }
         const int count = last - first;
         nb.assign(count, 1);
+        // expected work of an instance grows like l^2 (rows evaluated x row length):
+        // share the device by l^2 so that the largest instances, which bound the
+        // launch, get the most blocks
+        double total_w = 0;
+        for (int k = 0; k < count; k++) {
+            const double l = (double)subs[first + k].rows.size();
+            total_w += l * l;
+        }
         for (int k = 0; k < count; k++) {
             const long long l = (long long)subs[first + k].rows.size();
             const int nmin = (int)std::max<long long>(1, (l + chunk_max - 1) / chunk_max);
             int want;
             if (prm.blocks_override > 0) want = prm.blocks_override;
-            else want = (int)std::max<long long>(1, std::min<long long>(sms, (l + 1499) / 1500));
+            else want = (int)std::max<long long>(1, std::min<long long>(sms, (l + 499) / 500));
             if (count > 1) {
-                const long long share = (long long)std::floor((double)capacity * (double)l / (double)std::max<long long>(total_l, 1));
+                const long long share = (long long)std::floor((double)capacity * (double)l * (double)l / std::max(total_w, 1.0));
                 want = (int)std::min<long long>(want, std::max<long long>(1, share));
             }
             want = (int)std::min<long long>(want, std::max<long long>(1, l));
+            want = std::min(want, kThreads);
             nb[k] = std::max(want, nmin);
         }
+        (void)total_l;
         int used = 0;
         for (int v : nb) used += v;
         while (used > capacity) {
@@ -326,9 +435,73 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         }
         const size_t dyn_smem = (size_t)(stage_bytes + chunk_cap * kChunkBytes);
 
-        std::vector<InstanceAlloc> allocs(count);
+        // One arena block per wave, laid out so that the host touches it with
+        // one upload, three fills and two downloads:
+        //   upload   [descriptors][block map][alpha][p][row ids][labels]
+        //   download [outputs][alpha by local index]
+        //   zero     [group syncs][exchange records][cache epochs][cache stamps]
+        //   0xff     [cache tags]
+        //   per instance: G, G_bar, QD, status, position->local, shrink lists, Q rows
+        auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
+        std::vector<size_t> loff(count + 1, 0), poff(count + 1, 0), coff(count + 1, 0);
+        std::vector<InstanceLayout> lay(count);
+        for (int k = 0; k < count; k++) {
+            const int l = (int)subs[first + k].rows.size();
+            lay[k] = instance_layout(l, nb[k], prm.cache_mb);
+            loff[k + 1] = loff[k] + (size_t)l;
+            poff[k + 1] = poff[k] + 2 * (size_t)nb[k];
+            coff[k + 1] = coff[k] + (size_t)lay[k].sets * lay[k].ways;
+        }
+        const size_t L = loff[count], P = poff[count], S = coff[count];
+        size_t off = 0;
+        const size_t o_desc = off; off = al(off + sizeof(InstanceDesc) * count);
+        const size_t o_bmap = off; off = al(off + sizeof(int) * used);
+        const size_t o_alpha = off; off = al(off + 8 * L);
+        const size_t o_p = off; off = al(off + 8 * L);
+        const size_t o_row = off; off = al(off + 4 * L);
+        const size_t o_y = off; off = al(off + L);
+        const size_t up_bytes = off;
+        const size_t o_out = off; off = al(off + sizeof(SolveOut) * count);
+        const size_t o_alocal = off; off = al(off + 8 * L);
+        const size_t down_bytes = off - o_out;
+        const size_t o_zero = off;
+        const size_t o_sync = off; off = al(off + sizeof(GroupSync) * count);
+        const size_t o_part = off; off = al(off + sizeof(Partial) * P);
+        const size_t o_ep = off; off = al(off + 4 * S);
+        const size_t o_st = off; off = al(off + 8 * S);
+        const size_t zero_bytes = off - o_zero;
+        const size_t o_tag = off; off = al(off + 4 * S);
+        std::vector<size_t> inst_off(count);
+        for (int k = 0; k < count; k++) {
+            inst_off[k] = off;
+            off += lay[k].bytes;
+        }
+        clk.mark("plan");
+        char *arena = arena_reserve(off);
+        clk.mark("arena");
+        if (!arena) {
+            set_error("device allocation for solver state failed (" + std::to_string(off >> 20) + " MiB)");
+            return -1;
+        }
+        // host side of the upload region, in page-locked memory
+        char *host = nullptr;
+        std::vector<char> host_fallback;
+        {
+            host = (char *)pinned_staging_slot(1, up_bytes + down_bytes);
+            if (!host) {
+                host_fallback.resize(up_bytes + down_bytes);
+                host = host_fallback.data();
+            }
+        }
+        InstanceDesc *h_desc = (InstanceDesc *)(host + o_desc);
+        int *h_bmap = (int *)(host + o_bmap);
+        double *h_alpha = (double *)(host + o_alpha);
+        double *h_p = (double *)(host + o_p);
+        int *h_row = (int *)(host + o_row);
+        signed char *h_y = (signed char *)(host + o_y);
+        InstanceDesc *d_desc = (InstanceDesc *)(arena + o_desc);
+        int *d_block_inst = (int *)(arena + o_bmap);
         std::vector<InstanceDesc> desc(count);
-        std::vector<int> block_inst(used);
         int b0 = 0;
         for (int k = 0; k < count; k++) {
             const SubProblem &sp = subs[first + k];
@@ -350,74 +523,46 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
             D.stage_cap = stage_cap;
             D.stage_lds = stage_lds;
             D.chunk_cap = (int)chunk_cap;
-            for (int b = 0; b < nb[k]; b++) block_inst[b0 + b] = k;
-            b0 += nb[k];
-            // cache geometry: rows of l floats, at least 4, at most 2l slots
-            long long slots = (long long)std::floor(prm.cache_mb * (1 << 20) / (4.0 * std::max(l, 1)));
-            slots = std::max<long long>(slots, 4);
-            slots = std::min<long long>(slots, std::max<long long>(4, 2LL * l));
-            const int ways = (int)std::min<long long>(kMaxWays, slots);
-            const int sets = (int)(slots / ways);
-            Bump bump;
-            size_t oG = bump.take<double>(l), oGb = bump.take<double>(l), oA = bump.take<double>(l);
-            size_t oP = bump.take<double>(l), oQD = bump.take<double>(l), oAl = bump.take<double>(l);
-            size_t oY = bump.take<signed char>(l), oS = bump.take<unsigned char>(l);
-            size_t oPL = bump.take<int>(l), oPR = bump.take<int>(l), oSc = bump.take<int>(2 * (size_t)l);
-            size_t oOut = bump.take<SolveOut>(1), oSync = bump.take<GroupSync>(1);
-            size_t oPart = bump.take<Partial>(2 * (size_t)nb[k]);
-            size_t oTag = bump.take<int>((size_t)sets * ways), oEp = bump.take<int>((size_t)sets * ways);
-            size_t oSt = bump.take<unsigned long long>((size_t)sets * ways);
-            size_t oData = bump.take<float>((size_t)sets * ways * (size_t)l);
-            char *base = nullptr;
-            cudaError_t e = cudaMalloc(&base, bump.off);
-            if (e != cudaSuccess) {
-                for (int q = 0; q < k; q++) cudaFree(allocs[q].base);
-                set_error(std::string("device allocation for solver state failed: ") + cudaGetErrorString(e));
-                return -1;
+            {
+                const int limit = stage_cap > 0 ? std::min(kPrefetchMax, stage_cap) : kPrefetchMax;
+                D.prefetch = prm.prefetch > 0 ? std::min(prm.prefetch, limit) : limit;
             }
-            allocs[k].base = base;
-            allocs[k].bytes = bump.off;
-            D.G = (double *)(base + oG);
-            D.G_bar = (double *)(base + oGb);
-            D.alpha = (double *)(base + oA);
-            D.p = (double *)(base + oP);
-            D.QD = (double *)(base + oQD);
-            D.alpha_local = (double *)(base + oAl);
-            D.y = (signed char *)(base + oY);
-            D.status = (unsigned char *)(base + oS);
-            D.pos_local = (int *)(base + oPL);
-            D.pos_row = (int *)(base + oPR);
-            D.scratch = (int *)(base + oSc);
-            D.out = (SolveOut *)(base + oOut);
-            D.sync = (GroupSync *)(base + oSync);
-            D.partials = (Partial *)(base + oPart);
-            D.cache.tag = (int *)(base + oTag);
-            D.cache.epoch = (int *)(base + oEp);
-            D.cache.stamp = (unsigned long long *)(base + oSt);
-            D.cache.data = (float *)(base + oData);
-            D.cache.nsets = sets;
-            D.cache.nways = ways;
+            for (int b = 0; b < nb[k]; b++) h_bmap[b0 + b] = k;
+            b0 += nb[k];
+            const InstanceLayout &Lk = lay[k];
+            char *base = arena + inst_off[k];
+            D.G = (double *)(base + Lk.G);
+            D.G_bar = (double *)(base + Lk.Gb);
+            D.QD = (double *)(base + Lk.QD);
+            D.status = (unsigned char *)(base + Lk.S);
+            D.pos_local = (int *)(base + Lk.PL);
+            D.scratch = (int *)(base + Lk.Sc);
+            D.cache.data = (float *)(base + Lk.Data);
+            // initial state lives in the shared regions (positions start as local indices)
+            D.alpha = (double *)(arena + o_alpha) + loff[k];
+            D.p = (double *)(arena + o_p) + loff[k];
+            D.pos_row = (int *)(arena + o_row) + loff[k];
+            D.y = (signed char *)(arena + o_y) + loff[k];
+            D.out = (SolveOut *)(arena + o_out) + k;
+            D.alpha_local = (double *)(arena + o_alocal) + loff[k];
+            D.sync = (GroupSync *)(arena + o_sync) + k;
+            D.partials = (Partial *)(arena + o_part) + poff[k];
+            D.cache.tag = (int *)(arena + o_tag) + coff[k];
+            D.cache.epoch = (int *)(arena + o_ep) + coff[k];
+            D.cache.stamp = (unsigned long long *)(arena + o_st) + coff[k];
+            D.cache.nsets = Lk.sets;
+            D.cache.nways = Lk.ways;
             D.cache.stride = l;
-            // initial state
-            std::vector<int> iota(l);
-            for (int q = 0; q < l; q++) iota[q] = q;
-            CK(xfer_async(D.alpha, sp.alpha0.data(), sizeof(double) * l, cudaMemcpyHostToDevice, s));
-            CK(xfer_async(D.p, sp.p.data(), sizeof(double) * l, cudaMemcpyHostToDevice, s));
-            CK(xfer_async(D.y, sp.y.data(), l, cudaMemcpyHostToDevice, s));
-            CK(xfer_async(D.pos_local, iota.data(), sizeof(int) * l, cudaMemcpyHostToDevice, s));
-            CK(xfer_async(D.pos_row, sp.rows.data(), sizeof(int) * l, cudaMemcpyHostToDevice, s));
-            CK(cudaMemsetAsync(D.sync, 0, sizeof(GroupSync), s));
-            CK(cudaMemsetAsync(D.partials, 0, sizeof(Partial) * 2 * (size_t)nb[k], s));
-            CK(cudaMemsetAsync(D.cache.tag, 0xff, sizeof(int) * (size_t)sets * ways, s));
-            CK(cudaMemsetAsync(D.cache.epoch, 0, sizeof(int) * (size_t)sets * ways, s));
-            CK(cudaMemsetAsync(D.cache.stamp, 0, sizeof(unsigned long long) * (size_t)sets * ways, s));
+            memcpy(h_alpha + loff[k], sp.alpha0.data(), sizeof(double) * l);
+            memcpy(h_p + loff[k], sp.p.data(), sizeof(double) * l);
+            memcpy(h_row + loff[k], sp.rows.data(), sizeof(int) * l);
+            memcpy(h_y + loff[k], sp.y.data(), (size_t)l);
         }
-        InstanceDesc *d_desc = nullptr;
-        int *d_block_inst = nullptr;
-        CK(cudaMalloc(&d_desc, sizeof(InstanceDesc) * count));
-        CK(cudaMalloc(&d_block_inst, sizeof(int) * used));
-        CK(xfer_async(d_desc, desc.data(), sizeof(InstanceDesc) * count, cudaMemcpyHostToDevice, s));
-        CK(xfer_async(d_block_inst, block_inst.data(), sizeof(int) * used, cudaMemcpyHostToDevice, s));
+        memcpy(h_desc, desc.data(), sizeof(InstanceDesc) * count);
+        clk.mark("pack");
+        CK(xfer_async(arena, host, up_bytes, cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(arena + o_zero, 0, zero_bytes, s));
+        CK(cudaMemsetAsync(arena + o_tag, 0xff, 4 * S, s));
         cudaEvent_t ev0, ev1;
         CK(cudaEventCreate(&ev0));
         CK(cudaEventCreate(&ev1));
@@ -425,7 +570,10 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         cudaError_t le = launch_smo(prm.form, d_desc, d_block_inst, used, dyn_smem, true, s);
         if (le == cudaSuccess) count_launch();
         cudaEventRecord(ev1, s);
+        if (le == cudaSuccess) le = xfer_async(host + up_bytes, arena + o_out, down_bytes, cudaMemcpyDeviceToHost, s);
+        clk.mark("launch");
         cudaError_t se = le == cudaSuccess ? cudaStreamSynchronize(s) : le;
+        clk.mark("wait");
         float ms = 0;
         if (se == cudaSuccess) cudaEventElapsedTime(&ms, ev0, ev1);
         cudaEventDestroy(ev0);
@@ -435,25 +583,20 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
             set_error(std::string("solver launch failed: ") + cudaGetErrorString(se));
             rc = -1;
         }
+        const SolveOut *h_out = (const SolveOut *)(host + up_bytes);
+        const double *h_alocal = (const double *)(host + up_bytes + (o_alocal - o_out));
         for (int k = 0; k < count && rc == 0; k++) {
             SolveResult &R = res[first + k];
             const int l = desc[k].l;
-            R.alpha.resize(l);
-            if (xfer(R.alpha.data(), desc[k].alpha_local, sizeof(double) * l, cudaMemcpyDeviceToHost) != cudaSuccess ||
-                xfer(&R.out, desc[k].out, sizeof(SolveOut), cudaMemcpyDeviceToHost) != cudaSuccess) {
-                set_error("copy of solver results failed");
-                rc = -1;
-                break;
-            }
+            R.alpha.assign(h_alocal + loff[k], h_alocal + loff[k] + l);
+            R.out = h_out[k];
             R.seconds = ms * 1e-3;
             if (R.out.status < 0) {
                 set_error("solver group barrier timed out");
                 rc = -1;
             }
         }
-        for (auto &a : allocs) cudaFree(a.base);
-        cudaFree(d_desc);
-        cudaFree(d_block_inst);
+        clk.mark("unpack");
         if (rc) return rc;
         first = last;
     }

@@ -17,7 +17,15 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSrcBatch = 8;            // source rows staged per pass in the row-block product
 constexpr int kMaxWays = 8;             // set associativity of the Q-row cache
 constexpr int kEpochFull = -2;          // cache slot holds the complete row
+constexpr int kPrefetchCand = 4;        // prefetch candidates published per block and phase
+constexpr int kPrefetchMax = 8;         // rows evaluated per fill pass (the missing row + prefetched)
 constexpr int kNoTag = -1;
+constexpr int kMaxGroupBlocks = 160;     // blocks per instance (one per SM)
+constexpr int kTileStride = 20;         // floats per row of a warp's 32x16 transpose tile
+// shared memory shared by the transpose tiles and the prefetch candidate table
+constexpr int kTileBytes = kWarps * 32 * kTileStride * 4;
+constexpr int kCandBytes = kMaxGroupBlocks * kPrefetchCand * (8 + 4 * 4);
+constexpr int kAuxBytes = ((kTileBytes > kCandBytes ? kTileBytes : kCandBytes) + 15) / 16 * 16;
 
 enum : uint8_t { ST_LOWER = 0, ST_UPPER = 1, ST_FREE = 2 };   // reference svm.cpp:425
 
@@ -77,8 +85,17 @@ struct Partial {
     float q[2];
     int seq;
     int pad[5];
+    // the block's most violating positions (prefetch candidates): priority,
+    // position, local index, row id, label
+    double cv[kPrefetchCand];
+    int cpos[kPrefetchCand];
+    int cloc[kPrefetchCand];
+    int crow[kPrefetchCand];
+    int cy[kPrefetchCand];
+    int pad2[8];
 };
-static_assert(sizeof(Partial) == 128, "Partial must stay 128 bytes");
+static_assert(sizeof(Partial) == 256, "Partial must stay 256 bytes");
+static_assert(kPrefetchMax <= kSrcBatch, "a fill pass stages at most kSrcBatch rows");
 
 struct SolveOut {
     long long iters;
@@ -93,6 +110,7 @@ struct SolveOut {
     long long sum_active;
     long long q_evals;
     long long lookups, hits;
+    long long fills, prefetched, prefetch_used;   // fill passes, rows prefetched, prefetched rows later hit
     // SM cycles spent by block 0 in each section of the loop (kProf* below)
     long long prof[8];
 };
@@ -126,6 +144,7 @@ struct InstanceDesc {
     int stage_cap;              // rows staged at once (1..kSrcBatch); 0: read sources from global memory
     int stage_lds;              // floats per staged row (dense: ld; sparse: d)
     int chunk_cap;              // positions of per-block state held in shared memory (>= ceil(l/nblocks))
+    int prefetch;               // rows evaluated per fill pass (1 = no prefetch), <= kPrefetchMax
 };
 
 }  // namespace svmb

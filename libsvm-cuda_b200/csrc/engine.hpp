@@ -55,6 +55,7 @@ struct SolveParams {
     double cache_mb = 100;
     int form = FORM_EXACT;
     int blocks_override = 0;        // 0: heuristic
+    int prefetch = 0;               // rows per fill pass; 0: automatic (as many as can be staged)
 };
 
 struct SolveResult {

@@ -115,7 +115,8 @@ extern "C" int svmb_solve_dense_noalloc(int n, int ld, const float *X, const dou
     const long long budget = (long long)smem_total - smo_static_smem() - 1024;
     int stage_cap = (int)std::min<long long>(kSrcBatch, (48LL << 10) / ((long long)ld * 4));
     if (stage_cap < 2) stage_cap = 0;
-    const long long stage_bytes = (((long long)stage_cap * ld * 4) + 15) & ~15LL;
+    long long stage_bytes = (((long long)stage_cap * ld * 4) + 15) & ~15LL;
+    stage_bytes += kAuxBytes;   // transpose tiles / prefetch candidates
     const long long chunk_max = (budget - stage_bytes) / kChunkBytes;
     if (chunk_max < 64) { set_error("not enough shared memory for the solver state"); return -1; }
     int nb = (int)std::max<long long>(1, std::min<long long>(sms, (n + 1499) / 1500));
@@ -195,6 +196,8 @@ extern "C" int svmb_solve_dense_noalloc(int n, int ld, const float *X, const dou
     D.stage_cap = stage_cap;
     D.stage_lds = ld;
     D.chunk_cap = (int)chunk_cap;
+    D.prefetch = stage_cap > 0 ? std::min(kPrefetchMax, stage_cap) : kPrefetchMax;
+    if (params->prefetch > 0) D.prefetch = std::min(D.prefetch, params->prefetch);
     int block_inst[kNoAllocMaxBlocks];
     for (int b = 0; b < nb; b++) block_inst[b] = 0;
 

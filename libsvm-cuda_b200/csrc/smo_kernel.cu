@@ -405,14 +405,19 @@ struct CacheRec {
 };
 
 struct CacheState {
-    CacheRec prev[6], cur[6];
+    CacheRec prev[16], cur[16];
     int nprev, ncur;
 };
 
 struct Lookup {
-    long long slot;
+    long long slot;     // -1: no slot could be taken (prefetch only)
     int valid_active;   // positions [0,A) already valid
+    int was_prefetched; // hit on a row that a prefetch filled and nobody used yet
 };
+
+// LRU stamps: 2*iter+1 for phase A, 2*iter+2 for phase B; bit 62 marks rows
+// filled by prefetch and not yet used.
+constexpr unsigned long long kPrefetchMark = 1ull << 62;
 
 __device__ void cache_rotate(CacheState &cs, const CacheView &cv, int rank)
 {
@@ -456,8 +461,13 @@ __device__ void cache_read_set(const CacheState &cs, const CacheView &cv, int se
 
 // Decide where row `local` lives; records the decision.  whole: the rows
 // evaluated now cover every position (A == l), so they are complete.
+// Victims are taken only among ways whose stamp is below `protect` (rows
+// claimed in the phases still using them are never evicted).  A prefetch
+// lookup (`prefetch`) takes a slot only if its set keeps at least two
+// evictable ways, so that the rows the solver must place later always find
+// one; otherwise it returns slot -1.
 __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, int cur_epoch,
-                               unsigned long long clk, int whole)
+                               unsigned long long clk, int whole, unsigned long long protect, int prefetch)
 {
     int tag[kMaxWays], ep[kMaxWays];
     unsigned long long st[kMaxWays];
@@ -467,23 +477,31 @@ __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, i
     for (int w = 0; w < cv.nways; w++)
         if (tag[w] == local) way = w;
     Lookup L;
+    L.was_prefetched = 0;
     CacheRec rec;
     rec.set = set;
-    rec.stamp = clk;
+    rec.stamp = prefetch ? (clk | kPrefetchMark) : clk;
     rec.tag = local;
     if (way >= 0) {
         const int va = ep[way] == kEpochFull || ep[way] == cur_epoch;
         L.valid_active = va;
+        L.was_prefetched = va && (st[way] & kPrefetchMark) ? 1 : 0;
+        if (prefetch && va) rec.stamp = st[way];   // a prefetch hit changes nothing
         rec.way = way;
         rec.epoch = whole ? kEpochFull : (va ? ep[way] : cur_epoch);
     } else {
-        int victim = -1;
-        for (int w = 0; w < cv.nways; w++)
-            if (tag[w] == kNoTag) { victim = w; break; }
-        if (victim < 0) {
-            victim = 0;
-            for (int w = 1; w < cv.nways; w++)
-                if (st[w] < st[victim]) victim = w;
+        int victim = -1, evictable = 0;
+        for (int w = 0; w < cv.nways; w++) {
+            if (tag[w] != kNoTag && (st[w] & ~kPrefetchMark) >= protect) continue;
+            evictable++;
+            if (victim < 0 || tag[w] == kNoTag ||
+                (tag[victim] != kNoTag && (st[w] & ~kPrefetchMark) < (st[victim] & ~kPrefetchMark)))
+                victim = w;
+        }
+        if (victim < 0 || (prefetch && evictable < 3)) {
+            L.slot = -1;
+            L.valid_active = 0;
+            return L;
         }
         L.valid_active = 0;
         rec.way = victim;
@@ -522,11 +540,31 @@ struct Shared {
     int srcrow[kSrcBatch];
     int nsrc;
     int stop_at;
+    Partial lrec[2];
+    double cand_v[kWarps];
+    int cand_p[kWarps];
+    // rows of the current fill pass: row id, label, slot
+    int frow[kPrefetchMax], fy[kPrefetchMax];
+    long long fslot[kPrefetchMax];
+    int nfill;
+    int pick[kPrefetchMax];
+    int npick;
+};
+
+// The group's prefetch candidates (kPrefetchCand per block).  They live in
+// the same shared memory as the transpose tiles: candidates are read, chosen
+// and looked up before the fill pass reuses the space.
+struct PrefetchTable {
+    double v[kMaxGroupBlocks * kPrefetchCand];
+    int pos[kMaxGroupBlocks * kPrefetchCand], loc[kMaxGroupBlocks * kPrefetchCand];
+    int row[kMaxGroupBlocks * kPrefetchCand], y[kMaxGroupBlocks * kPrefetchCand];
 };
 
 struct Ctx {
     const InstanceDesc *D;
     float *stage;           // source staging area (dynamic smem)
+    float *tile;            // per-warp 32-row transpose tiles (dense rows) ...
+    PrefetchTable *pt;      // ... sharing their space with the prefetch candidates
     // my chunk of [0,A) held in shared memory
     double *sG, *sA, *sQD;
     int *sCol, *sRow;
@@ -538,6 +576,7 @@ struct Ctx {
     int t0, t1;             // my chunk of [A,l)
     int epoch;
     int phase;              // exchange counter: selects the record buffer and sequence number
+    Partial *lrec;          // single-block groups keep their two records in shared memory
 };
 
 __device__ __forceinline__ void set_chunks(Ctx &c)
@@ -550,8 +589,50 @@ __device__ __forceinline__ void set_chunks(Ctx &c)
     c.t1 = c.A + (int)(m * (c.rank + 1) / c.nb);
 }
 
-__device__ __forceinline__ Partial *my_partial(const Ctx &c) { return c.D->partials + (long long)(c.phase & 1) * c.nb + c.rank; }
-__device__ __forceinline__ const Partial *prev_partials(const Ctx &c) { return c.D->partials + (long long)((c.phase - 1) & 1) * c.nb; }
+__device__ __forceinline__ Partial *my_partial(const Ctx &c)
+{
+    if (c.nb == 1) return c.lrec + (c.phase & 1);
+    return c.D->partials + (long long)(c.phase & 1) * c.nb + c.rank;
+}
+__device__ __forceinline__ const Partial *prev_partials(const Ctx &c)
+{
+    if (c.nb == 1) return c.lrec + ((c.phase - 1) & 1);
+    return c.D->partials + (long long)((c.phase - 1) & 1) * c.nb;
+}
+
+// Record fields read by the reductions.  Multi-block records were written by
+// other SMs: read them at L2 (ld.global.cg); single-block records live in
+// shared memory.
+struct RecVals {
+    double v[6];
+    int n[8];
+    float q[2];
+};
+__device__ __forceinline__ void rec_load(const Ctx &c, const Partial *p, RecVals &r, int with_n_hi, int with_q)
+{
+    if (c.nb == 1) {
+        for (int k = 0; k < 6; k++) r.v[k] = p->v[k];
+        for (int k = 0; k < 8; k++) r.n[k] = p->n[k];
+        r.q[0] = p->q[0];
+        r.q[1] = p->q[1];
+        return;
+    }
+    const double2 a = __ldcg(reinterpret_cast<const double2 *>(&p->v[0]));
+    const double2 b = __ldcg(reinterpret_cast<const double2 *>(&p->v[2]));
+    const double2 d = __ldcg(reinterpret_cast<const double2 *>(&p->v[4]));
+    const int4 n0 = __ldcg(reinterpret_cast<const int4 *>(&p->n[0]));
+    r.v[0] = a.x; r.v[1] = a.y; r.v[2] = b.x; r.v[3] = b.y; r.v[4] = d.x; r.v[5] = d.y;
+    r.n[0] = n0.x; r.n[1] = n0.y; r.n[2] = n0.z; r.n[3] = n0.w;
+    if (with_n_hi) {
+        const int4 n1 = __ldcg(reinterpret_cast<const int4 *>(&p->n[4]));
+        r.n[4] = n1.x; r.n[5] = n1.y; r.n[6] = n1.z; r.n[7] = n1.w;
+    }
+    if (with_q) {
+        const float2 q = __ldcg(reinterpret_cast<const float2 *>(&p->q[0]));
+        r.q[0] = q.x;
+        r.q[1] = q.y;
+    }
+}
 
 // Publish my record of this phase and wait for everybody's (group barrier).
 __device__ bool exchange(Ctx &c, Shared &sh)
@@ -633,7 +714,7 @@ __device__ void group_counts(const Ctx &c, Shared &sh, int slot, int *below, int
     const Partial *all = prev_partials(c);
     int b_lo = 0, b_hi = 0, tot = 0;
     for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-        const int v = __ldcg(&all[b].n[slot]);
+        const int v = c.nb == 1 ? all[b].n[slot] : __ldcg(&all[b].n[slot]);
         tot += v;
         if (b < c.rank) b_lo += v;
         if (b > c.rank) b_hi += v;
@@ -806,8 +887,11 @@ __device__ bool do_shrinking(Ctx &c, Shared &sh, int &unshrink)
         double v[4] = {-SVMB_INF, -SVMB_INF, -SVMB_INF, -SVMB_INF};
         int ix[4] = {-1, -1, -1, -1};
         const int kind[4] = {2, 2, 2, 2};
-        for (int b = threadIdx.x; b < c.nb; b += blockDim.x)
-            for (int k = 0; k < 4; k++) v[k] = fmax(v[k], __ldcg(&all[b].v[k]));
+        for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
+            RecVals r;
+            rec_load(c, &all[b], r, 0, 0);
+            for (int k = 0; k < 4; k++) v[k] = fmax(v[k], r.v[k]);
+        }
         block_reduce<4>(sh.red, v, ix, kind);
         for (int k = 0; k < 4; k++) g[k] = v[k];
     }
@@ -887,10 +971,59 @@ __device__ bool do_shrinking(Ctx &c, Shared &sh, int &unshrink)
 // I_up scan of my chunk (first half of WSS3): per track the max of -y_t G_t
 // with its payload.  C-SVC uses track 0 only; nu-SVC: track 0 = y=+1, 1 = y=-1.
 // --------------------------------------------------------------------------
-__device__ void iup_publish(const Ctx &c, Shared &sh, double (&v)[2], int (&ix)[2])
+// Prefetch priority of a position: how strongly it violates optimality on
+// either side, max(-y G over I_up, y G over I_low) -- the quantities whose
+// extremes WSS picks from, so high-priority rows are likely to be needed soon.
+__device__ __forceinline__ double prefetch_priority(int y, unsigned char s, double G)
+{
+    double up = -SVMB_INF, low = -SVMB_INF;
+    if (y == +1) {
+        if (s != ST_UPPER) up = -G;
+        if (s != ST_LOWER) low = G;
+    } else {
+        if (s != ST_LOWER) up = G;
+        if (s != ST_UPPER) low = -G;
+    }
+    return fmax(up, low);
+}
+
+// Publish the block's I_up maxima (with payload) and its most violating
+// positions (prefetch candidates: the best of each warp, top kPrefetchCand).
+__device__ void iup_publish(const Ctx &c, Shared &sh, double (&v)[2], int (&ix)[2], double pv, int pix)
 {
     const int kind[2] = {0, 0};
-    block_reduce<2>(sh.red, v, ix, kind);
+    // warp winners of the prefetch priority
+    warp_argmax(pv, pix);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        sh.cand_v[w] = pv;
+        sh.cand_p[w] = pix;
+    }
+    block_reduce<2>(sh.red, v, ix, kind);   // its barriers also publish cand_*
+    if (threadIdx.x < 32) {
+        double cv = lane < kWarps ? sh.cand_v[lane] : -SVMB_INF;
+        int cp = lane < kWarps ? sh.cand_p[lane] : -1;
+        Partial *pp = my_partial(c);
+        for (int t = 0; t < kPrefetchCand; t++) {
+            double bv = cv;
+            int bp = cp;
+            warp_argmax(bv, bp);
+            if (bp >= 0 && bv > -SVMB_INF) {
+                if (cp == bp) cv = -SVMB_INF;        // remove the winner
+                if (lane == 0) {
+                    const int q = bp - c.a0;
+                    pp->cv[t] = bv;
+                    pp->cpos[t] = bp;
+                    pp->cloc[t] = c.sCol[q];
+                    pp->crow[t] = c.sRow[q];
+                    pp->cy[t] = c.sY[q];
+                }
+            } else if (lane == 0) {
+                pp->cv[t] = -SVMB_INF;
+                pp->cpos[t] = -1;
+            }
+        }
+    }
     if (threadIdx.x == 0) {
         Partial *pp = my_partial(c);
         for (int k = 0; k < 2; k++) {
@@ -914,20 +1047,77 @@ __device__ void scan_iup(Ctx &c, Shared &sh)
     const int nu = c.D->nu;
     double v[2] = {-SVMB_INF, -SVMB_INF};
     int ix[2] = {-1, -1};
+    double pv = -SVMB_INF;
+    int pix = -1;
     for (int k = threadIdx.x; k < c.a1 - c.a0; k += blockDim.x) {
         const unsigned char s = c.sS[k];
         const double G = c.sG[k];
-        if (c.sY[k] == +1) {
+        const int y = c.sY[k];
+        if (y == +1) {
             if (s != ST_UPPER) better_max(v[0], ix[0], -G, c.a0 + k);
         } else {
             if (s != ST_LOWER) better_max(v[nu], ix[nu], G, c.a0 + k);
         }
+        better_max(pv, pix, prefetch_priority(y, s, G), c.a0 + k);
     }
-    iup_publish(c, sh, v, ix);
+    iup_publish(c, sh, v, ix, pv, pix);
 }
 
-// Evaluate the Q rows of `ns` (<= 2) sources into cache slots on my chunk of
-// [0,A) (tail = 0, from shared memory) or of [A,l) (tail = 1, global state).
+// Dot products of the 32 rows of a warp (lane L owns row r) with ns <= 2
+// staged dense sources.  Each 32-float column slice of the 32 rows is loaded
+// with one coalesced 128-byte load per row into a padded 32x33 shared tile,
+// then every lane accumulates ITS row in feature order from the tile -- the
+// reference's summation order, with coalesced memory traffic.
+template <int FORM, int NS>
+__device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const StageSlots &ss, int ns, int r, float *tile,
+                                               double (&out)[kPrefetchMax])
+{
+    typedef typename Acc<FORM>::type acc_t;
+    const int lane = threadIdx.x & 31;
+    const int ld = D.x.ld;   // multiple of 4
+    const float *X = D.x.X;
+    acc_t acc[NS];
+    const float *src[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+        acc[k] = acc_t(0);
+        src[k] = ss.sp[k < ns ? k : 0];
+    }
+    // 16-column slices: lanes 0-15 load row 2q, lanes 16-31 row 2q+1, 64
+    // contiguous bytes each; row t of the tile = the row of lane t
+    const int half = lane >> 4, cl = lane & 15;
+    for (int c0 = 0; c0 < ld; c0 += 16) {
+        const int col = c0 + cl;
+        float v[16];
+#pragma unroll
+        for (int qq = 0; qq < 16; qq++) {
+            const int rq = __shfl_sync(0xffffffffu, r, 2 * qq + half);
+            v[qq] = col < ld ? __ldg(X + (long long)rq * ld + col) : 0.0f;
+        }
+#pragma unroll
+        for (int qq = 0; qq < 16; qq++) tile[(2 * qq + half) * kTileStride + cl] = v[qq];
+        __syncwarp();
+        const int lim = ld - c0 < 16 ? ld - c0 : 16;    // multiple of 4
+        for (int q = 0; q < lim; q += 4) {
+            const float4 xv = *reinterpret_cast<const float4 *>(tile + lane * kTileStride + q);
+#pragma unroll
+            for (int k = 0; k < NS; k++) {
+                const float4 w = *reinterpret_cast<const float4 *>(src[k] + c0 + q);
+                acc[k] = mac<FORM>(xv.x, w.x, acc[k]);
+                acc[k] = mac<FORM>(xv.y, w.y, acc[k]);
+                acc[k] = mac<FORM>(xv.z, w.z, acc[k]);
+                acc[k] = mac<FORM>(xv.w, w.w, acc[k]);
+            }
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int k = 0; k < NS; k++) out[k] = (double)acc[k];
+}
+
+// Evaluate the Q rows of `ns` (<= kPrefetchMax, <= stage_cap when staged)
+// sources into cache slots on my chunk of [0,A) (tail = 0, from shared
+// memory) or of [A,l) (tail = 1, global state).
 template <int FORM>
 __device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const int *src_y, const long long *slot,
                           int tail)
@@ -935,30 +1125,72 @@ __device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const 
     const InstanceDesc &D = *c.D;
     if (ns == 0) return;
     stage_sources(D, c.stage, sh.ss, src_row, ns);
-    double xs[2];
-    for (int k = 0; k < 2; k++) xs[k] = (k < ns && D.x.xsq) ? D.x.xsq[src_row[k]] : 0.0;
-    float *dst0 = D.cache.data + slot[0] * D.cache.stride;
-    float *dst1 = ns > 1 ? D.cache.data + slot[1] * D.cache.stride : dst0;
+    double xs[kPrefetchMax];
+    float *dst[kPrefetchMax];
+    int sy[kPrefetchMax];
+#pragma unroll
+    for (int k = 0; k < kPrefetchMax; k++) {
+        const int kk = k < ns ? k : 0;
+        xs[k] = D.x.xsq ? D.x.xsq[src_row[kk]] : 0.0;
+        dst[k] = D.cache.data + slot[kk] * D.cache.stride;
+        sy[k] = src_y[kk];
+    }
     const int lo = tail ? c.t0 : 0, hi = tail ? c.t1 : c.a1 - c.a0;
-    for (int k = lo + threadIdx.x; k < hi; k += blockDim.x) {
-        int r, yp, col;
-        if (tail) {
-            r = D.pos_row[k];
-            yp = D.y[k];
-            col = D.pos_local[k];
-        } else {
-            r = c.sRow[k];
-            yp = c.sY[k];
-            col = c.sCol[k];
+    if (D.x.X && D.stage_cap > 0) {
+        // dense rows, staged sources: warp-tiled, whole warps per 32 positions
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        float *tile = c.tile + warp * (32 * kTileStride);
+        for (int base = lo + warp * 32; base < hi; base += blockDim.x) {
+            const int k = base + lane;
+            const bool valid = k < hi;
+            const int kk = valid ? k : base;     // idle lanes repeat a valid row
+            int r, yp, col;
+            if (tail) {
+                r = D.pos_row[kk];
+                yp = D.y[kk];
+                col = D.pos_local[kk];
+            } else {
+                r = c.sRow[kk];
+                yp = c.sY[kk];
+                col = c.sCol[kk];
+            }
+            double dots[kPrefetchMax];
+            if (ns == 1) warp_tile_dots<FORM, 1>(D, sh.ss, ns, r, tile, dots);
+            else if (ns == 2) warp_tile_dots<FORM, 2>(D, sh.ss, ns, r, tile, dots);
+            else if (ns <= 4) warp_tile_dots<FORM, 4>(D, sh.ss, ns, r, tile, dots);
+            else warp_tile_dots<FORM, 8>(D, sh.ss, ns, r, tile, dots);
+            if (valid) {
+                const double xe = D.x.xsq ? D.x.xsq[r] : 0.0;
+#pragma unroll
+                for (int s2 = 0; s2 < kPrefetchMax; s2++)
+                    if (s2 < ns) dst[s2][col] = q_value(D.kp, sy[s2] * yp, dots[s2], xs[s2], xe);
+            }
         }
-        double dots[kSrcBatch];
-        row_dots<FORM>(D, sh.ss, ns, r, dots);
-        const double xe = D.x.xsq ? D.x.xsq[r] : 0.0;
-        dst0[col] = q_value(D.kp, src_y[0] * yp, dots[0], xs[0], xe);
-        if (ns > 1) dst1[col] = q_value(D.kp, src_y[1] * yp, dots[1], xs[1], xe);
+    } else {
+        for (int k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+            int r, yp, col;
+            if (tail) {
+                r = D.pos_row[k];
+                yp = D.y[k];
+                col = D.pos_local[k];
+            } else {
+                r = c.sRow[k];
+                yp = c.sY[k];
+                col = c.sCol[k];
+            }
+            double dots[kSrcBatch];
+            row_dots<FORM>(D, sh.ss, ns, r, dots);
+            const double xe = D.x.xsq ? D.x.xsq[r] : 0.0;
+#pragma unroll
+            for (int s2 = 0; s2 < kPrefetchMax; s2++)
+                if (s2 < ns) dst[s2][col] = q_value(D.kp, sy[s2] * yp, dots[s2], xs[s2], xe);
+        }
     }
     unstage_sources(D, c.stage, sh.ss);
 }
+
+// position of the phase-A winner of track k (excluded from prefetching)
+__device__ __forceinline__ int i0_prev_guard(const Shared &sh, int k) { return sh.bi[4 * k]; }
 
 // --------------------------------------------------------------------------
 // the persistent solver
@@ -973,11 +1205,15 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
     c.A = D.l;
     c.epoch = 0;
     c.phase = 0;
+    c.lrec = sh.lrec;
     {
-        // dynamic shared memory: [stage][G][alpha][QD][col][row][y][status]
+        // dynamic shared memory: [stage][tiles][G][alpha][QD][col][row][y][status]
         size_t off = (size_t)D.stage_cap * D.stage_lds * sizeof(float);
         off = (off + 15) & ~(size_t)15;
         c.stage = reinterpret_cast<float *>(dyn);
+        c.tile = reinterpret_cast<float *>(dyn + off);
+        c.pt = reinterpret_cast<PrefetchTable *>(dyn + off);
+        off += kAuxBytes;
         const size_t cap = (size_t)D.chunk_cap;
         c.sG = reinterpret_cast<double *>(dyn + off); off += cap * 8;
         c.sA = reinterpret_cast<double *>(dyn + off); off += cap * 8;
@@ -994,7 +1230,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
     int unshrink = 0;
     int status = 0;
     // block 0 / thread 0 work counters and section timers
-    long long cnt_active = 0, cnt_q = 0, cnt_look = 0, cnt_hit = 0;
+    long long cnt_active = 0, cnt_q = 0, cnt_look = 0, cnt_hit = 0, cnt_fill = 0, cnt_pf = 0, cnt_pf_used = 0;
     long long prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long tmark = clock64();
     const long long tstart = tmark;
@@ -1014,6 +1250,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
     // ---- initial state (svm.cpp:525-572, QD svm.cpp:1321-1327) on the global copies ----
     {
         for (int p = c.a0 + threadIdx.x; p < c.a1; p += blockDim.x) {
+            D.pos_local[p] = p;      // positions start as local indices
             D.status[p] = status_of(D.alpha[p], get_C(D, D.y[p]));
             const int r = D.pos_row[p];
             const double xs = D.x.xsq ? D.x.xsq[r] : 0.0;
@@ -1055,25 +1292,44 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
             int i0, i1;
         select_again:
             // ======================= phase A =======================
+            const unsigned long long clkA = 4ull * (unsigned long long)iter + 1ull + (unsigned long long)widened;
             {
                 const Partial *all = prev_partials(c);
                 double v[2] = {-SVMB_INF, -SVMB_INF};
                 int ix[2] = {-1, -1};
                 const int kind[2] = {0, 0};
-                for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-                    better_max(v[0], ix[0], __ldcg(&all[b].v[0]), __ldcg(&all[b].n[0]));
-                    better_max(v[1], ix[1], __ldcg(&all[b].v[3]), __ldcg(&all[b].n[4]));
+                RecVals r;
+                r.n[0] = r.n[4] = -1;
+                if (threadIdx.x < c.nb) {
+                    rec_load(c, &all[threadIdx.x], r, 1, 0);
+                    better_max(v[0], ix[0], r.v[0], r.n[0]);
+                    better_max(v[1], ix[1], r.v[3], r.n[4]);
+                    if (D.prefetch > 1) {
+                        // this block's prefetch candidates into shared memory
+                        const Partial *pr = &all[threadIdx.x];
+                        for (int t = 0; t < kPrefetchCand; t++) {
+                            const int e = threadIdx.x * kPrefetchCand + t;
+                            if (c.nb == 1) {
+                                c.pt->v[e] = pr->cv[t]; c.pt->pos[e] = pr->cpos[t];
+                                c.pt->loc[e] = pr->cloc[t]; c.pt->row[e] = pr->crow[t]; c.pt->y[e] = pr->cy[t];
+                            } else {
+                                c.pt->v[e] = __ldcg(&pr->cv[t]); c.pt->pos[e] = __ldcg(&pr->cpos[t]);
+                                c.pt->loc[e] = __ldcg(&pr->cloc[t]); c.pt->row[e] = __ldcg(&pr->crow[t]);
+                                c.pt->y[e] = __ldcg(&pr->cy[t]);
+                            }
+                        }
+                    }
                 }
                 block_reduce<2>(sh.red, v, ix, kind);
-                // winners' payload, read by the thread that holds the winning record
-                for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
+                // the thread holding a winning record publishes its payload
+                if (threadIdx.x < c.nb) {
                     for (int k = 0; k < 2; k++) {
-                        if (ix[k] >= 0 && __ldcg(&all[b].n[4 * k]) == ix[k]) {
-                            sh.bd[3 * k + 1] = __ldcg(&all[b].v[3 * k + 1]);
-                            sh.bd[3 * k + 2] = __ldcg(&all[b].v[3 * k + 2]);
-                            sh.bi[4 * k + 1] = __ldcg(&all[b].n[4 * k + 1]);
-                            sh.bi[4 * k + 2] = __ldcg(&all[b].n[4 * k + 2]);
-                            sh.bi[4 * k + 3] = __ldcg(&all[b].n[4 * k + 3]);
+                        if (ix[k] >= 0 && r.n[4 * k] == ix[k]) {
+                            sh.bd[3 * k + 1] = r.v[3 * k + 1];
+                            sh.bd[3 * k + 2] = r.v[3 * k + 2];
+                            sh.bi[4 * k + 1] = r.n[4 * k + 1];
+                            sh.bi[4 * k + 2] = r.n[4 * k + 2];
+                            sh.bi[4 * k + 3] = r.n[4 * k + 3];
                         }
                     }
                 }
@@ -1083,44 +1339,84 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 }
                 __syncthreads();
                 if (threadIdx.x == 0) {
-                    // cache decisions for the row(s) of phase A
-                    const unsigned long long clk = 2ull * (unsigned long long)iter + 1ull;
+                    // cache decisions for the row(s) of phase A; missing rows go to the fill list
                     const int whole = c.A == l;
+                    sh.nfill = 0;
                     for (int k = 0; k < 2; k++) {
                         sh.bl[k] = -1;
                         sh.bi[8 + k] = 1;
                         if (sh.bi[4 * k] >= 0 && (k == 0 || nu)) {
-                            Lookup L = cache_lookup(sh.cs, D.cache, sh.bi[4 * k + 1], c.epoch, clk, whole);
+                            Lookup L = cache_lookup(sh.cs, D.cache, sh.bi[4 * k + 1], c.epoch, clkA, whole, clkA, 0);
                             sh.bl[k] = L.slot;
                             sh.bi[8 + k] = L.valid_active;
                             cnt_look++;
                             cnt_hit += L.valid_active;
+                            cnt_pf_used += L.was_prefetched;
+                            if (!L.valid_active) {
+                                sh.frow[sh.nfill] = sh.bi[4 * k + 2];
+                                sh.fy[sh.nfill] = sh.bi[4 * k + 3];
+                                sh.fslot[sh.nfill] = L.slot;
+                                sh.nfill++;
+                            }
                         }
                     }
                 }
                 __syncthreads();
+                // speculative prefetch: a missing row is evaluated together with
+                // the rows of the group's most violating positions (this only
+                // fills the cache; it never changes which pair is chosen)
+                if (sh.nfill > 0 && D.prefetch > sh.nfill) {
+                    const int ncand = c.nb * kPrefetchCand;
+                    const int want = D.prefetch - sh.nfill;
+                    if (threadIdx.x == 0) sh.npick = 0;
+                    for (int round = 0; round < want; round++) {
+                        double bv[1] = {-SVMB_INF};
+                        int be[1] = {-1};
+                        const int kind1[1] = {0};
+                        for (int e = threadIdx.x; e < ncand; e += blockDim.x) {
+                            const int pos = c.pt->pos[e];
+                            if (pos >= 0 && pos != i0_prev_guard(sh, 0) && pos != i0_prev_guard(sh, 1) && c.pt->v[e] > -SVMB_INF)
+                                better_max(bv[0], be[0], c.pt->v[e], e);
+                        }
+                        block_reduce<1>(sh.red, bv, be, kind1);
+                        if (be[0] < 0) break;
+                        if (threadIdx.x == 0) {
+                            sh.pick[sh.npick++] = be[0];
+                            c.pt->v[be[0]] = -SVMB_INF;
+                        }
+                        __syncthreads();
+                    }
+                    __syncthreads();
+                    if (threadIdx.x == 0) {
+                        const int whole = c.A == l;
+                        for (int t = 0; t < sh.npick && sh.nfill < D.prefetch; t++) {
+                            const int e = sh.pick[t];
+                            Lookup L = cache_lookup(sh.cs, D.cache, c.pt->loc[e], c.epoch, clkA, whole, clkA, 1);
+                            if (L.slot >= 0 && !L.valid_active) {
+                                sh.frow[sh.nfill] = c.pt->row[e];
+                                sh.fy[sh.nfill] = c.pt->y[e];
+                                sh.fslot[sh.nfill] = L.slot;
+                                sh.nfill++;
+                                cnt_pf++;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
             }
             Gmax0 = sh.bd[0];
             Gmax1 = sh.bd[3];
             i0 = sh.bi[0];
             i1 = nu ? sh.bi[4] : -1;
             {
-                // evaluate the missing row(s) on my chunk
-                int ns = 0;
-                int srow[2] = {0, 0}, sy[2] = {0, 0};
-                long long sslot[2] = {0, 0};
-                for (int k = 0; k < 2; k++) {
-                    const int ik = k == 0 ? i0 : i1;
-                    if (ik >= 0 && !sh.bi[8 + k]) {
-                        srow[ns] = sh.bi[4 * k + 2];
-                        sy[ns] = sh.bi[4 * k + 3];
-                        sslot[ns] = sh.bl[k];
-                        ns++;
-                    }
-                }
+                // evaluate the missing (and prefetched) rows on my chunk
+                const int ns = sh.nfill;
                 SVMB_PROF(kProfAReduce);
-                fill_rows<FORM>(c, sh, ns, srow, sy, sslot, 0);
-                cnt_q += (long long)ns * c.A;
+                if (ns > 0) {
+                    fill_rows<FORM>(c, sh, ns, sh.frow, sh.fy, sh.fslot, 0);
+                    cnt_q += (long long)ns * c.A;
+                    cnt_fill++;
+                }
                 SVMB_PROF(kProfAFill);
             }
             {
@@ -1190,18 +1486,19 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 double v[3] = {SVMB_INF, -SVMB_INF, -SVMB_INF};
                 int ix[3] = {-1, -1, -1};
                 const int kind[3] = {1, 2, 2};
-                for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-                    better_min(v[0], ix[0], __ldcg(&all[b].v[0]), __ldcg(&all[b].n[0]));
-                    v[1] = fmax(v[1], __ldcg(&all[b].v[1]));
-                    v[2] = fmax(v[2], __ldcg(&all[b].v[2]));
+                RecVals r;
+                r.n[0] = -1;
+                if (threadIdx.x < c.nb) {
+                    rec_load(c, &all[threadIdx.x], r, 0, 1);
+                    better_min(v[0], ix[0], r.v[0], r.n[0]);
+                    v[1] = r.v[1];
+                    v[2] = r.v[2];
                 }
                 block_reduce<3>(sh.red, v, ix, kind);
-                for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-                    if (ix[0] >= 0 && __ldcg(&all[b].n[0]) == ix[0]) {
-                        sh.bd[14] = __ldcg(&all[b].v[3]); sh.bd[15] = __ldcg(&all[b].v[4]); sh.bd[16] = __ldcg(&all[b].v[5]);
-                        sh.bi[13] = __ldcg(&all[b].n[1]); sh.bi[14] = __ldcg(&all[b].n[2]); sh.bi[15] = __ldcg(&all[b].n[3]);
-                        sh.bd[17] = (double)__ldcg(&all[b].q[0]); sh.bd[18] = (double)__ldcg(&all[b].q[1]);
-                    }
+                if (threadIdx.x < c.nb && ix[0] >= 0 && r.n[0] == ix[0]) {
+                    sh.bd[14] = r.v[3]; sh.bd[15] = r.v[4]; sh.bd[16] = r.v[5];
+                    sh.bi[13] = r.n[1]; sh.bi[14] = r.n[2]; sh.bi[15] = r.n[3];
+                    sh.bd[17] = (double)r.q[0]; sh.bd[18] = (double)r.q[1];
                 }
                 if (threadIdx.x == 0) { sh.bi[12] = ix[0]; sh.bd[12] = v[1]; sh.bd[13] = v[2]; }
                 __syncthreads();
@@ -1242,23 +1539,26 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
             const double Gj = sh.bd[14], alpha_j = sh.bd[15], QDj = sh.bd[16];
             const int loc_j = sh.bi[13], row_j = sh.bi[14];
             // Q_j row
+            // phase-B stamp: above every phase-A stamp of this iteration, below the next
+            const unsigned long long clkB = 4ull * (unsigned long long)iter - 1ull;
             if (threadIdx.x == 0) {
-                const unsigned long long clk = 2ull * (unsigned long long)iter;
-                Lookup L = cache_lookup(sh.cs, D.cache, loc_j, c.epoch, clk, c.A == l);
+                Lookup L = cache_lookup(sh.cs, D.cache, loc_j, c.epoch, clkB, c.A == l, clkA, 0);
                 sh.bl[2] = L.slot;
                 sh.bi[16] = L.valid_active;
                 cnt_look++;
                 cnt_hit += L.valid_active;
+                cnt_pf_used += L.was_prefetched;
             }
             __syncthreads();
             SVMB_PROF(kProfBReduce);
             const long long slot_j = sh.bl[2];
             if (!sh.bi[16]) {
-                const int srow[2] = {row_j, 0};
-                const int sy[2] = {yj, 0};
-                const long long ss[2] = {slot_j, 0};
+                const int srow[1] = {row_j};
+                const int sy[1] = {yj};
+                const long long ss[1] = {slot_j};
                 fill_rows<FORM>(c, sh, 1, srow, sy, ss, 0);
                 cnt_q += c.A;
+                cnt_fill++;
             }
             // two-variable analytic step (svm.cpp:636-721), identical in every block
             const double C_i = get_C(D, yi), C_j = get_C(D, yj);
@@ -1307,7 +1607,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
             // complete rows for the G_bar update: fill the tail [A,l) where missing
             if ((bar_i || bar_j) && c.A < l) {
                 if (threadIdx.x == 0) {
-                    const unsigned long long clk = 2ull * (unsigned long long)iter;
+                    const unsigned long long clk = clkB;
                     int tg[kMaxWays], ep[kMaxWays];
                     unsigned long long stp[kMaxWays];
                     sh.bi[17] = 0;
@@ -1345,6 +1645,8 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 const float *Qj = D.cache.data + slot_j * D.cache.stride;
                 double v[2] = {-SVMB_INF, -SVMB_INF};
                 int ix[2] = {-1, -1};
+                double pv = -SVMB_INF;
+                int pix = -1;
                 const int n = c.a1 - c.a0;
                 for (int k = threadIdx.x; k < n; k += blockDim.x) {
                     const int col = c.sCol[k];
@@ -1364,6 +1666,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                     } else {
                         if (s != ST_LOWER) better_max(v[nu], ix[nu], G, c.a0 + k);
                     }
+                    better_max(pv, pix, prefetch_priority(c.sY[k], s, G), c.a0 + k);
                 }
                 if (bar_i || bar_j) {
                     for (int p = c.t0 + threadIdx.x; p < c.t1; p += blockDim.x) {
@@ -1374,7 +1677,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                         D.G_bar[p] = gb;
                     }
                 }
-                iup_publish(c, sh, v, ix);
+                iup_publish(c, sh, v, ix, pv, pix);
             }
             if (!exchange(c, sh)) goto fail;
             SVMB_PROF(kProfBUpdate);
@@ -1452,6 +1755,9 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
             o.q_evals = cnt_q;
             o.lookups = cnt_look;
             o.hits = cnt_hit;
+            o.fills = cnt_fill;
+            o.prefetched = cnt_pf;
+            o.prefetch_used = cnt_pf_used;
             for (int k = 0; k < 7; k++) o.prof[k] = prof[k];
             o.prof[kProfTotal] = clock64() - tstart;
             if (!nu) {
@@ -1479,6 +1785,7 @@ fail:
         o.iters = iter; o.rho = 0; o.obj = 0; o.r = 0; o.status = -1; o.active_size = c.A;
         o.unshrink = unshrink; o.nr_free = 0; o.gap = 0;
         o.sum_active = cnt_active; o.q_evals = cnt_q; o.lookups = cnt_look; o.hits = cnt_hit;
+        o.fills = cnt_fill; o.prefetched = cnt_pf; o.prefetch_used = cnt_pf_used;
         for (int k = 0; k < 8; k++) o.prof[k] = prof[k];
         *D.out = o;
     }

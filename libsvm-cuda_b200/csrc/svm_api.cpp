@@ -56,6 +56,7 @@ struct Options {
     int form = svmb::FORM_EXACT;
     int blocks = 0;
     int force_layout = -1;
+    int prefetch = 0;
 } g_opt;
 
 // statistics of the last svm_train call (svmb_last_train_stats)
@@ -146,6 +147,7 @@ svmb::SolveParams make_solve_params(const svm_parameter *param)
     prm.cache_mb = param->cache_size;
     prm.form = g_opt.form;
     prm.blocks_override = g_opt.blocks;
+    prm.prefetch = g_opt.prefetch;
     return prm;
 }
 
@@ -210,6 +212,9 @@ DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResul
     st.q_evals = R.out.q_evals;
     st.lookups = R.out.lookups;
     st.hits = R.out.hits;
+    st.fills = R.out.fills;
+    st.prefetched = R.out.prefetched;
+    st.prefetch_used = R.out.prefetch_used;
     for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
     {
         std::lock_guard<std::mutex> g(g_stats_mu);
@@ -232,6 +237,9 @@ int api_set_option(const char *name, long long value)
         g_opt.blocks = (int)value;
     } else if (!strcmp(name, "layout")) {
         g_opt.force_layout = (int)value;
+    } else if (!strcmp(name, "prefetch")) {
+        if (value < 0 || value > kPrefetchMax) return -1;
+        g_opt.prefetch = (int)value;
     } else {
         return -1;
     }

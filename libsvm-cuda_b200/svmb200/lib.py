@@ -27,7 +27,8 @@ class SolveStats(C.Structure):
                 ("l", C.c_int), ("nr_sv", C.c_int), ("nr_bsv", C.c_int), ("status", C.c_int),
                 ("active_size", C.c_int), ("pad", C.c_int), ("seconds", C.c_double),
                 ("sum_active", C.c_longlong), ("q_evals", C.c_longlong), ("lookups", C.c_longlong),
-                ("hits", C.c_longlong), ("prof_cycles", C.c_longlong * 8)]
+                ("hits", C.c_longlong), ("fills", C.c_longlong), ("prefetched", C.c_longlong),
+                ("prefetch_used", C.c_longlong), ("prof_cycles", C.c_longlong * 8)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("pad", "prof_cycles")}
@@ -39,16 +40,16 @@ class SvmbParams(C.Structure):
     _fields_ = [("svm_type", C.c_int), ("kernel_type", C.c_int), ("degree", C.c_int), ("shrinking", C.c_int),
                 ("gamma", C.c_double), ("coef0", C.c_double), ("C_pos", C.c_double), ("C_neg", C.c_double),
                 ("nu", C.c_double), ("eps", C.c_double), ("cache_mb", C.c_double), ("form", C.c_int),
-                ("blocks", C.c_int)]
+                ("blocks", C.c_int), ("prefetch", C.c_int)]
 
 
 def make_params(svm_type=0, kernel_type=2, degree=3, gamma=0.0, coef0=0.0, C_pos=1.0, C_neg=None, nu=0.5,
-                eps=1e-3, cache_mb=100.0, shrinking=1, form=FORM_EXACT, blocks=0) -> SvmbParams:
+                eps=1e-3, cache_mb=100.0, shrinking=1, form=FORM_EXACT, blocks=0, prefetch=0) -> SvmbParams:
     p = SvmbParams()
     p.svm_type, p.kernel_type, p.degree, p.shrinking = svm_type, kernel_type, degree, shrinking
     p.gamma, p.coef0, p.C_pos = gamma, coef0, C_pos
     p.C_neg = C_pos if C_neg is None else C_neg
-    p.nu, p.eps, p.cache_mb, p.form, p.blocks = nu, eps, cache_mb, form, blocks
+    p.nu, p.eps, p.cache_mb, p.form, p.blocks, p.prefetch = nu, eps, cache_mb, form, blocks, prefetch
     return p
 
 
