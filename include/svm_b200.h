@@ -64,10 +64,21 @@ typedef struct svmb_params {
     int form;            /* SVMB_FORM_* */
     int blocks;          /* thread blocks per solve; 0 = automatic */
     int prefetch;        /* kernel rows evaluated per cache-miss pass (1 = only the missing row); 0 = automatic */
+    int gbar_mode;       /* SVMB_GBAR_*: how the gradient of the inactive variables is kept */
 } svmb_params;
+
+#define SVMB_GBAR_AUTO        0  /* incremental for EXACT and FP32, recomputed for the tensor forms */
+#define SVMB_GBAR_INCREMENTAL 1  /* G_bar updated on every bound change (reference svm.cpp:744-769) */
+#define SVMB_GBAR_RECOMPUTE   2  /* no G_bar; reconstruction recomputes G = p + Q*alpha on the inactive
+                                    variables as one block product, so no full-length rows are needed */
 
 #define SVMB_FORM_EXACT 0   /* fp32 features, fp64 accumulation in feature order */
 #define SVMB_FORM_FP32  1   /* fp32 features, fp32 accumulation (plain CUDA-core form) */
+#define SVMB_FORM_BF16X3 2  /* tensor cores: features split x = hi + lo (bf16), dot = hi.hi + hi.lo + lo.hi
+                               accumulated in fp32 (about 16 significant bits per product);
+                               the split copy holds every row densely */
+#define SVMB_FORM_FP16X3 3  /* tensor cores: each row scaled by a power of two and split x*2^e = hi + lo
+                               (fp16), same three products in fp32 (about 22 significant bits) */
 
 const char *svmb_last_error(void);
 /* Number of device kernels this library has launched in this process. */
@@ -138,6 +149,14 @@ int svmb_rows_solve_many(const svmb_rows *rows, int ninst, const int *inst_ptr, 
                          const double *inst_y, const svmb_params *params, double *alpha_out,
                          svmb_solve_stats *stats);
 void svmb_rows_free(svmb_rows *rows);
+
+/* Kernel-matrix block out[i][j] = K(x_ia[i], x_ib[j]) (row-major [ma][nb],
+ * float64) of resident rows, with params' kernel and form: the block form of
+ * the reference's Kernel::k_function / SVC_Q::get_Q (svm.cpp:235-254,
+ * :305-325, :1316-1340).  SVMB_FORM_BF16X3 and SVMB_FORM_FP16X3 run on the
+ * tensor cores, the other forms on CUDA cores.  ia, ib, out are host arrays. */
+int svmb_rows_kernel_block(const svmb_rows *rows, const svmb_params *params, int ma, const int *ia, int nb,
+                           const int *ib, double *out);
 
 #ifdef __cplusplus
 }

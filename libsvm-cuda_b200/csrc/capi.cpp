@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "engine.hpp"
@@ -34,7 +35,9 @@ int check_params(const svmb_params *p)
     if (p->cache_mb <= 0) { svmb::set_error("cache_size <= 0"); return -1; }
     if (p->svm_type == C_SVC && (p->C_pos <= 0 || p->C_neg <= 0)) { svmb::set_error("C <= 0"); return -1; }
     if (p->svm_type == NU_SVC && (p->nu <= 0 || p->nu > 1)) { svmb::set_error("nu <= 0 or nu > 1"); return -1; }
-    if (p->form != SVMB_FORM_EXACT && p->form != SVMB_FORM_FP32) { svmb::set_error("unknown form"); return -1; }
+    if (p->form != SVMB_FORM_EXACT && p->form != SVMB_FORM_FP32 && p->form != SVMB_FORM_BF16X3 &&
+        p->form != SVMB_FORM_FP16X3) { svmb::set_error("unknown form"); return -1; }
+    if (p->gbar_mode < SVMB_GBAR_AUTO || p->gbar_mode > SVMB_GBAR_RECOMPUTE) { svmb::set_error("unknown gbar_mode"); return -1; }
     return 0;
 }
 
@@ -45,7 +48,8 @@ int solve_many(const svmb::DeviceRows &rows, int ninst, const int *inst_ptr, con
     for (int k = 0; k < ninst; k++) {
         if (check_params(&params[k])) return -1;
         if (params[k].kernel_type != params[0].kernel_type || params[k].gamma != params[0].gamma ||
-            params[k].coef0 != params[0].coef0 || params[k].degree != params[0].degree || params[k].form != params[0].form) {
+            params[k].coef0 != params[0].coef0 || params[k].degree != params[0].degree || params[k].form != params[0].form ||
+            params[k].gbar_mode != params[0].gbar_mode) {
             svmb::set_error("instances of one launch must share kernel parameters and form");
             return -1;
         }
@@ -93,6 +97,7 @@ int solve_many(const svmb::DeviceRows &rows, int ninst, const int *inst_ptr, con
     prm.form = params[0].form;
     prm.blocks_override = params[0].blocks;
     prm.prefetch = params[0].prefetch;
+    prm.lazy_gbar = params[0].gbar_mode == SVMB_GBAR_INCREMENTAL ? 0 : params[0].gbar_mode == SVMB_GBAR_RECOMPUTE ? 1 : -1;
     for (int k = 1; k < ninst; k++)
         if (params[k].eps != prm.eps || params[k].shrinking != prm.shrinking || params[k].cache_mb != prm.cache_mb) {
             svmb::set_error("instances of one launch must share eps, shrinking and cache_mb");
@@ -222,6 +227,50 @@ int svmb_rows_solve_many(const svmb_rows *rows, int ninst, const int *inst_ptr, 
 }
 
 void svmb_rows_free(svmb_rows *rows) { delete rows; }
+
+int svmb_rows_kernel_block(const svmb_rows *rows, const svmb_params *params, int ma, const int *ia, int nb,
+                           const int *ib, double *out)
+{
+    if (!rows || !params || ma < 0 || nb < 0 || (ma && (!ia || !out)) || (nb && !ib)) {
+        svmb::set_error("invalid arguments");
+        return -1;
+    }
+    if (params->kernel_type < LINEAR || params->kernel_type > SIGMOID) { svmb::set_error("kernel_type must be LINEAR, POLY, RBF or SIGMOID"); return -1; }
+    if (params->form < SVMB_FORM_EXACT || params->form > SVMB_FORM_FP16X3) { svmb::set_error("unknown form"); return -1; }
+    const int n = rows->dev.n;
+    for (int i = 0; i < ma; i++)
+        if (ia[i] < 0 || ia[i] >= n) { svmb::set_error("row index out of range"); return -1; }
+    for (int j = 0; j < nb; j++)
+        if (ib[j] < 0 || ib[j] >= n) { svmb::set_error("row index out of range"); return -1; }
+    if (ma == 0 || nb == 0) return 0;
+    svmb::DeviceRows &dev = const_cast<svmb::DeviceRows &>(rows->dev);
+    if (dev.prepare_form(params->form, 0) != 0) return -1;
+    svmb::KernelParams kp{params->kernel_type, params->degree, params->gamma, params->coef0};
+    int *d_ia = nullptr, *d_ib = nullptr, *d_err = nullptr;
+    double *d_out = nullptr;
+    int herr = 0;
+    cudaError_t e = cudaMalloc(&d_ia, sizeof(int) * (size_t)ma);
+    if (e == cudaSuccess) e = cudaMalloc(&d_ib, sizeof(int) * (size_t)nb);
+    if (e == cudaSuccess) e = cudaMalloc(&d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(double) * (size_t)ma * nb);
+    if (e == cudaSuccess) e = svmb::xfer(d_ia, ia, sizeof(int) * (size_t)ma, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = svmb::xfer(d_ib, ib, sizeof(int) * (size_t)nb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_err, 0, sizeof(int));
+    if (e == cudaSuccess) e = svmb::launch_kernel_block(dev, kp, params->form, d_ia, ma, d_ib, nb, d_out, nb, d_err, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = svmb::xfer(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = svmb::xfer(out, d_out, sizeof(double) * (size_t)ma * nb, cudaMemcpyDeviceToHost);
+    cudaFree(d_ia); cudaFree(d_ib); cudaFree(d_err); cudaFree(d_out);
+    if (e != cudaSuccess) {
+        svmb::set_error(std::string("kernel block: ") + cudaGetErrorString(e));
+        return -1;
+    }
+    if (herr) {
+        svmb::set_error("kernel block: a tensor-core wait timed out");
+        return -1;
+    }
+    return 0;
+}
 
 int svmb_solve_many_csr(int n, int d, const long long *rowptr, const int *col, const float *val, int ninst,
                         const int *inst_ptr, const int *inst_rows, const double *inst_y, const svmb_params *params,

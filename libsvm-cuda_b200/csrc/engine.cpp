@@ -133,6 +133,40 @@ DeviceRows::~DeviceRows()
     cudaFree(val);
     cudaFree(xsq[0]);
     cudaFree(xsq[1]);
+    cudaFree(Xs);
+    cudaFree(xinv);
+}
+
+int DeviceRows::prepare_form(int form, cudaStream_t s)
+{
+    if (!is_tc_form(form)) return 0;
+    if ((Xs && split_form == form) || n == 0) return 0;
+    cudaFree(Xs);
+    cudaFree(xinv);
+    Xs = nullptr;
+    xinv = nullptr;
+    split_form = -1;
+    // the tensor forms read every row densely (d features, padded to 64)
+    const int nc = std::max(1, (d + kSplitChunk - 1) / kSplitChunk);
+    const size_t b = (size_t)n * nc * 2 * kSplitChunk * sizeof(uint16_t);
+    uint16_t *p = nullptr;
+    double *q = nullptr;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess && form == FORM_FP16X3) e = cudaMalloc(&q, (size_t)n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, b, s);
+    if (e == cudaSuccess) e = launch_split(*this, form, nc, p, q, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaFree(p);
+        cudaFree(q);
+        set_error(std::string("split rows: ") + cudaGetErrorString(e));
+        return -1;
+    }
+    Xs = p;
+    xinv = q;
+    nchunk = nc;
+    split_form = form;
+    return 0;
 }
 
 DevX DeviceRows::view(int form) const
@@ -144,7 +178,13 @@ DevX DeviceRows::view(int form) const
     v.col = dense ? nullptr : col;
     v.val = dense ? nullptr : val;
     v.d = d;
-    v.xsq = xsq[form];
+    // the tensor forms use the float64 norms: they cost nothing and keep the
+    // RBF distance as accurate as the split dot products allow
+    v.xsq = xsq[is_tc_form(form) ? FORM_EXACT : form];
+    const bool split = is_tc_form(form) && split_form == form;
+    v.Xs = split ? Xs : nullptr;
+    v.nchunk = split ? nchunk : 0;
+    v.xinv = split ? xinv : nullptr;
     return v;
 }
 
@@ -164,6 +204,7 @@ int upload_csr(const long long *rowptr, const int *col, const float *val, int n,
     if (dense && dense_bytes > 60e9) dense = false;
     out.dense = dense;
     // the CSR arrays always travel; dense rows are scattered on the device
+    out.nnz = nnz;
     CK(cudaMalloc(&out.rowptr, (size_t)(n + 1) * sizeof(long long)));
     CK(cudaMalloc(&out.col, (size_t)std::max<long long>(nnz, 1) * sizeof(int)));
     CK(cudaMalloc(&out.val, (size_t)std::max<long long>(nnz, 1) * sizeof(float)));
@@ -328,6 +369,8 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
     const int ninst = (int)subs.size();
     res.assign(ninst, SolveResult());
     if (ninst == 0) return 0;
+    // the split bf16 copy of the rows is a derived cache of the rows, built on first use
+    if (const_cast<DeviceRows &>(rows).prepare_form(prm.form, s) != 0) return -1;
     std::lock_guard<std::mutex> arena_lock(g_arena_mu);
     StageClock clk;
     const int sms = device_sm_count();
@@ -350,7 +393,19 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         stage_cap = (int)std::min<long long>(kSrcBatch, (budget / 2) / ((long long)std::max(rows.d, 1) * 4));
     }
     if (stage_cap < 2) stage_cap = 0;
-    long long stage_bytes = (((long long)stage_cap * stage_lds * 4) + 15) & ~15LL;
+    int tc_n = 0;
+    long long stage_bytes;
+    if (is_tc_form(prm.form)) {
+        // tensor form: the operand stages of the tensor-core pipeline replace the
+        // source staging; as many sources per block-product pass as leave room for
+        // a useful chunk of state
+        stage_cap = 0;
+        tc_n = kTcMaxN;
+        while (tc_n > 16 && (budget - tc_area_bytes(tc_n) - kAuxBytes) / kChunkBytes < 1024) tc_n /= 2;
+        stage_bytes = tc_area_bytes(tc_n);
+    } else {
+        stage_bytes = (((long long)stage_cap * stage_lds * 4) + 15) & ~15LL;
+    }
     stage_bytes += kAuxBytes;   // transpose tiles / prefetch candidates
     const long long chunk_max = (budget - stage_bytes) / kChunkBytes;
     if (chunk_max < 64) {
@@ -526,6 +581,8 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
             {
                 const int limit = stage_cap > 0 ? std::min(kPrefetchMax, stage_cap) : kPrefetchMax;
                 D.prefetch = prm.prefetch > 0 ? std::min(prm.prefetch, limit) : limit;
+                D.lazy_gbar = prm.lazy_gbar < 0 ? (is_tc_form(prm.form) ? 1 : 0) : prm.lazy_gbar;
+                D.tc_n = tc_n;
             }
             for (int b = 0; b < nb[k]; b++) h_bmap[b0 + b] = k;
             b0 += nb[k];

@@ -10,6 +10,12 @@
 #include <cstdint>
 #include <cstddef>
 
+#ifdef __CUDACC__
+#define SVMB_HD __host__ __device__
+#else
+#define SVMB_HD
+#endif
+
 namespace svmb {
 
 constexpr int kThreads = 512;           // threads per block of the persistent solver
@@ -27,13 +33,26 @@ constexpr int kTileBytes = kWarps * 32 * kTileStride * 4;
 constexpr int kCandBytes = kMaxGroupBlocks * kPrefetchCand * (8 + 4 * 4);
 constexpr int kAuxBytes = ((kTileBytes > kCandBytes ? kTileBytes : kCandBytes) + 15) / 16 * 16;
 
+// tensor-core (FORM_BF16X3) block products inside the solver
+constexpr int kTcM = 128;               // targets per tile (MMA M); rows are TMEM lanes
+constexpr int kTcStages = 3;            // operand stages of the cp.async -> MMA pipeline
+constexpr int kTcMaxN = 64;             // sources per block-product pass (MMA N, TMEM columns)
+// bytes of one operand stage: target tile (128 rows x 64 bf16, hi and lo) + n source rows (hi and lo)
+SVMB_HD constexpr int tc_stage_bytes(int n) { return 2 * kTcM * 128 + n * 256; }
+SVMB_HD constexpr int tc_area_bytes(int n) { return 1024 + kTcStages * tc_stage_bytes(n); }
+
 enum : uint8_t { ST_LOWER = 0, ST_UPPER = 1, ST_FREE = 2 };   // reference svm.cpp:425
 
 // arithmetic form of the kernel-row evaluation
 enum RowForm : int {
     FORM_EXACT = 0,   // fp32 X, fp64 accumulation in feature order (matches the reference's Kernel::dot)
     FORM_FP32 = 1,    // fp32 X, fp32 accumulation (the plain CUDA-core form)
+    FORM_BF16X3 = 2,  // tensor cores: x = hi + lo in bf16, dot = hi.hi + hi.lo + lo.hi, fp32 accumulation
+    FORM_FP16X3 = 3,  // tensor cores: x*2^e = hi + lo in fp16 (power-of-2 scale per row), same three products
 };
+constexpr int kNumForms = 4;
+SVMB_HD constexpr bool is_tc_form(int f) { return f == FORM_BF16X3 || f == FORM_FP16X3; }
+constexpr int kSplitChunk = 64;         // bf16 features per K-chunk of the split rows (hi 64 then lo 64)
 
 struct KernelParams {
     int type;         // LINEAR, POLY, RBF, SIGMOID
@@ -51,6 +70,9 @@ struct DevX {
     const float *val;           // CSR value
     int d;                      // number of feature columns
     const double *xsq;          // [n_rows] dot(x,x) in the reference's order
+    const uint16_t *Xs;         // split rows [n_rows][nchunk][hi 64 | lo 64] (tensor forms), or nullptr
+    int nchunk;                 // 64-feature chunks per split row
+    const double *xinv;         // FORM_FP16X3: per-row 2^-e undoing the split's scale (nullptr: 1)
 };
 
 // Q-row cache of one instance: `nsets` x `nways` slots of `stride` floats;
@@ -145,6 +167,11 @@ struct InstanceDesc {
     int stage_lds;              // floats per staged row (dense: ld; sparse: d)
     int chunk_cap;              // positions of per-block state held in shared memory (>= ceil(l/nblocks))
     int prefetch;               // rows evaluated per fill pass (1 = no prefetch), <= kPrefetchMax
+    // 0: G_bar maintained on every bound change, as the reference does (svm.cpp:744-769);
+    // 1: no G_bar -- reconstruction recomputes G = p + sum over alpha>0 of alpha*Q on the
+    //    inactive positions as one block product (no full-length rows during the loop)
+    int lazy_gbar;
+    int tc_n;                   // FORM_BF16X3: sources per tensor-core pass (16, 32 or 64); 0 otherwise
 };
 
 }  // namespace svmb

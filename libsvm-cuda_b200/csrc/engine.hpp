@@ -25,11 +25,18 @@ struct DeviceRows {
     long long *rowptr = nullptr;
     int *col = nullptr;
     float *val = nullptr;
-    double *xsq[2] = {nullptr, nullptr};   // per RowForm
+    double *xsq[2] = {nullptr, nullptr};   // FORM_EXACT, FORM_FP32 (the tensor form uses the FP32 norms)
+    uint16_t *Xs = nullptr;    // split rows of a tensor form (split_form), built on first use
+    double *xinv = nullptr;    // FORM_FP16X3 per-row inverse scales
+    int split_form = -1;
+    long long nnz = 0;         // stored values (CSR)
+    int nchunk = 0;
     size_t bytes = 0;          // device bytes of the layout the solver reads
     size_t h2d_bytes = 0;      // bytes copied from the host by the upload
     ~DeviceRows();
     DevX view(int form) const;
+    // build Xs if the form needs it; -1 (error set) when the rows cannot take the form
+    int prepare_form(int form, cudaStream_t s);
 };
 
 // Upload rows given as libsvm svm_node lists (index >= 1, terminated by -1).
@@ -56,6 +63,7 @@ struct SolveParams {
     int form = FORM_EXACT;
     int blocks_override = 0;        // 0: heuristic
     int prefetch = 0;               // rows per fill pass; 0: automatic (as many as can be staged)
+    int lazy_gbar = -1;             // -1: by form (recomputed for FORM_BF16X3), 0: incremental, 1: recomputed
 };
 
 struct SolveResult {
@@ -81,6 +89,10 @@ cudaError_t launch_xsq(const DevX &x, int n, double *out, int form, cudaStream_t
 cudaError_t launch_scatter_dense(const long long *rowptr, const int *col, const float *val, int n, int ld, float *X,
                                  cudaStream_t s);
 int smo_static_smem();
+// kernel-matrix blocks (gram_kernel.cu)
+cudaError_t launch_split(const DeviceRows &rows, int form, int nchunk, uint16_t *Xs, double *xinv, cudaStream_t s);
+cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, int form, const int *d_ia, int ma,
+                                const int *d_ib, int nb, double *d_out, long long ldo, int *d_err, cudaStream_t s);
 cudaError_t launch_smo(int form, const InstanceDesc *d_insts, const int *d_block_inst, int nblocks,
                        size_t dyn_smem, bool cooperative, cudaStream_t s);
 cudaError_t smo_max_blocks(int form, size_t dyn_smem, int *blocks_per_sm);

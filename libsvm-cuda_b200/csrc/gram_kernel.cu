@@ -1,0 +1,350 @@
+// gram_kernel.cu -- kernel-matrix blocks K(x_a, x_b) over sets of resident
+// rows: the block form of the reference's Kernel::k_function / SVC_Q::get_Q
+// (reference libsvm/svm.cpp:235-254, :305-325, :1316-1340).
+//
+// Three arithmetic forms:
+//   FORM_EXACT   float64 accumulation in feature order (CUDA cores);
+//   FORM_FP32    float32 accumulation (CUDA cores, the plain form);
+//   FORM_BF16X3  tensor cores.  Every feature is split x = hi + lo with hi, lo
+//                bf16 (hi = bf16(x), lo = bf16(x - hi); x - hi is exact in
+//                float32), and dot(a, b) = hi_a.hi_b + hi_a.lo_b + lo_a.hi_b
+//                accumulated in float32 in TMEM by tcgen05.mma (kind::f16).
+//                The dropped lo.lo term and the residual of the split are
+//                about 2^-16 of each product;
+//   FORM_FP16X3  tensor cores, the same three products over an fp16 split of
+//                each row scaled by a power of two (max |x| 2^e in [2^14, 2^15)):
+//                x 2^e = hi + lo, about 2^-22 of each product; the dot is
+//                multiplied back by 2^-e_a 2^-e_b (exact).
+// The split copy is dense (CSR rows are scattered into it), d padded to a
+// multiple of 64.  RBF distances use the float64 row norms.
+// The kernel value itself is always formed in float64 from the dot product.
+//
+// Tensor-core tiling: one CTA computes a 128 x 128 tile of dots; K runs in
+// chunks of 64 features (the split rows store, per chunk, 64 hi then 64 lo
+// bf16 = 256 contiguous bytes), staged by cp.async into 128B-swizzled
+// K-major shared-memory tiles, three stages deep; thread 0 issues the 12 MMAs
+// of a chunk (4 K-steps x 3 products, M=128 N=128 K=16) and commits them to
+// the stage's mbarrier, which releases the stage for the next chunk's loads.
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+
+#include "engine.hpp"
+#include "kernel_math.cuh"
+#include "tc_sm100.cuh"
+
+namespace svmb {
+
+namespace {
+
+constexpr int kGM = 128;
+constexpr int kGN = 128;
+constexpr int kGStages = 3;
+constexpr int kGTile = 128 * 128;                       // bytes of one 128-row x 64-bf16 operand tile
+constexpr int kGStageBytes = 4 * kGTile;                // A hi, A lo, B hi, B lo
+constexpr int kGSmem = kGStages * kGStageBytes + 1024;  // + alignment slack
+
+struct GramArgs {
+    const uint16_t *xs;         // split rows [n][nchunk][128]
+    const double *xinv;         // per-row inverse scales (fp16 split) or nullptr
+    long long rs;               // row stride in bf16 elements (nchunk * 128)
+    int nchunk;
+    const int *ia;              // row ids of the tile rows (nullptr: identity)
+    int ma;
+    const int *ib;
+    int nb;
+    KernelParams kp;
+    const double *xsq;          // norms by row id
+    double *out;                // [ma][ldo]
+    long long ldo;
+    int *err;
+};
+
+template <bool BF16>
+__global__ void __launch_bounds__(128, 1) gram_split_kernel(GramArgs a)
+{
+    extern __shared__ uint8_t g_smem_raw[];
+    __shared__ uint64_t bars[kGStages + 1];
+    __shared__ uint32_t tmem_base;
+    __shared__ long long offA[kGM], offB[kGN];
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * kGM, n0 = blockIdx.x * kGN;
+    const uint32_t raw = tc::smem_addr(g_smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+
+    {
+        const int r = m0 + tid, c = n0 + tid;
+        offA[tid] = r < a.ma ? (long long)(a.ia ? a.ia[r] : r) * a.rs : -1;
+        offB[tid] = c < a.nb ? (long long)(a.ib ? a.ib[c] : c) * a.rs : -1;
+    }
+    if (tid == 0) {
+        for (int s = 0; s <= kGStages; s++) tc::mbar_init(&bars[s], 1);
+        tc::mbar_init_fence();
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_base, kGN);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_base;
+
+    // stage s <- chunk kc of the 128 A rows and 128 B rows (16 pieces of 16 B per row)
+    auto load = [&](int s, int kc) {
+        const uint32_t sa = base + s * kGStageBytes;
+#pragma unroll 4
+        for (int i = 0; i < 16; i++) {
+            const int idx = tid + 128 * i, r = idx >> 4, q = idx & 15;
+            const uint32_t so = (q >= 8 ? kGTile : 0) + tc::sw128_offset(r, q & 7);
+            const long long oa = offA[r], ob = offB[r];
+            tc::cp_async16(sa + so, a.xs + (oa < 0 ? 0 : oa) + kc * 128 + q * 8, oa < 0 ? 0u : 16u);
+            tc::cp_async16(sa + 2 * kGTile + so, a.xs + (ob < 0 ? 0 : ob) + kc * 128 + q * 8, ob < 0 ? 0u : 16u);
+        }
+    };
+
+    const uint32_t idesc = tc::idesc_f16_f32(kGM, kGN, BF16);
+    const int nk = a.nchunk;
+    bool ok = true;
+    for (int s = 0; s < kGStages - 1; s++) {
+        if (s < nk) load(s, s);
+        tc::cp_async_commit();
+    }
+    for (int kc = 0; kc < nk; kc++) {
+        const int s = kc % kGStages;
+        tc::cp_async_wait<kGStages - 2>();
+        tc::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tc::tc_fence_after();
+            const uint32_t sa = base + s * kGStageBytes;
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                const uint64_t ahi = tc::sw128_desc(sa + kk * 32), alo = tc::sw128_desc(sa + kGTile + kk * 32);
+                const uint64_t bhi = tc::sw128_desc(sa + 2 * kGTile + kk * 32);
+                const uint64_t blo = tc::sw128_desc(sa + 3 * kGTile + kk * 32);
+                tc::mma_bf16(tmem, ahi, bhi, idesc, kc > 0 || kk > 0);
+                tc::mma_bf16(tmem, ahi, blo, idesc, true);
+                tc::mma_bf16(tmem, alo, bhi, idesc, true);
+            }
+            tc::mma_commit(&bars[s]);
+            if (kc == nk - 1) tc::mma_commit(&bars[kGStages]);
+        }
+        const int nxt = kc + kGStages - 1;
+        if (nxt < nk) {
+            // the stage of chunk nxt was last read by the MMAs of chunk kc-1
+            if (kc >= 1 && ok && !tc::mbar_wait(&bars[(kc - 1) % kGStages], ((kc - 1) / kGStages) & 1)) ok = false;
+            if (ok) load(nxt % kGStages, nxt);
+        }
+        tc::cp_async_commit();
+    }
+    tc::cp_async_wait<0>();
+    if (nk > 0 && ok && !tc::mbar_wait(&bars[kGStages], 0)) ok = false;
+    if (!ok) atomicExch(a.err, 1);
+    tc::tc_fence_after();
+
+    // epilogue: warp w holds tile rows 32w..32w+31 (TMEM lanes), 16 columns per load
+    const int row = m0 + warp * 32 + lane;
+    const bool rok = ok && nk > 0 && row < a.ma;
+    const int ra = rok ? (a.ia ? a.ia[row] : row) : 0;
+    const double xa = rok ? a.xsq[ra] : 0.0;
+    const double sa_inv = (rok && a.xinv) ? a.xinv[ra] : 1.0;
+    for (int c0 = 0; c0 < kGN; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
+        if (rok) {
+            double *dst = a.out + (long long)row * a.ldo;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int col = n0 + c0 + k;
+                if (col < a.nb) {
+                    const int rb = a.ib ? a.ib[col] : col;
+                    const double sb_inv = a.xinv ? a.xinv[rb] : 1.0;
+                    dst[col] = kernel_from_dot(a.kp, __dmul_rn(__dmul_rn((double)v[k], sa_inv), sb_inv), xa, a.xsq[rb]);
+                }
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, kGN);
+}
+
+// CUDA-core kernel block: one thread per output, 16 x 16 threads per CTA
+template <int FORM>
+__global__ void kblock_cuda_kernel(DevX x, const int *ia, int ma, const int *ib, int nb, KernelParams kp, double *out,
+                                   long long ldo)
+{
+    const int i = blockIdx.y * 16 + threadIdx.y, j = blockIdx.x * 16 + threadIdx.x;
+    if (i >= ma || j >= nb) return;
+    const int ra = ia ? ia[i] : i, rb = ib ? ib[j] : j;
+    double dot;
+    if (x.X) {
+        const float *pa = x.X + (long long)ra * x.ld, *pb = x.X + (long long)rb * x.ld;
+        if (FORM == FORM_EXACT) {
+            double s = 0.0;
+            for (int k = 0; k < x.d; k++) s = __dadd_rn(s, __dmul_rn((double)pa[k], (double)pb[k]));
+            dot = s;
+        } else {
+            float s = 0.0f;
+            for (int k = 0; k < x.d; k++) s = fmaf(pa[k], pb[k], s);
+            dot = s;
+        }
+    } else {
+        long long e = x.rowptr[ra], ee = x.rowptr[ra + 1], f = x.rowptr[rb], ff = x.rowptr[rb + 1];
+        double s = 0.0;
+        float sf = 0.0f;
+        while (e < ee && f < ff) {
+            const int ce = x.col[e], cf = x.col[f];
+            if (ce == cf) {
+                if (FORM == FORM_EXACT) s = __dadd_rn(s, __dmul_rn((double)x.val[e], (double)x.val[f]));
+                else sf = fmaf(x.val[e], x.val[f], sf);
+                ++e; ++f;
+            } else if (ce > cf) {
+                ++f;
+            } else {
+                ++e;
+            }
+        }
+        dot = FORM == FORM_EXACT ? s : (double)sf;
+    }
+    out[(long long)i * ldo + j] = kernel_from_dot(kp, dot, x.xsq[ra], x.xsq[rb]);
+}
+
+// per-row scale of the fp16 split: xinv[r] = 2^-e with max_k |x_rk| 2^e in
+// [2^14, 2^15) (1 for an all-zero row); one warp per row
+__global__ void row_scale_kernel(DevX x, int n, double *__restrict__ xinv)
+{
+    const int lane = threadIdx.x & 31;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
+        float m = 0.0f;
+        if (x.X) {
+            for (int k = lane; k < x.d; k += 32) m = fmaxf(m, fabsf(x.X[(long long)r * x.ld + k]));
+        } else {
+            for (long long e = x.rowptr[r] + lane; e < x.rowptr[r + 1]; e += 32) m = fmaxf(m, fabsf(x.val[e]));
+        }
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) {
+            int k = 0;
+            if (m > 0.0f) frexpf(m, &k);            // m = f 2^k, f in [0.5, 1)
+            xinv[r] = m > 0.0f ? ldexp(1.0, k - 15) : 1.0;
+        }
+    }
+}
+
+template <bool BF16>
+__device__ __forceinline__ void split_store(float v, float s, uint16_t *dst)
+{
+    if (BF16) {
+        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+        dst[0] = __bfloat16_as_ushort(hi);
+        dst[kSplitChunk] = __bfloat16_as_ushort(lo);
+    } else {
+        const float w = v * s;                       // exact: s is a power of two
+        const __half hi = __float2half_rn(w);
+        const __half lo = __float2half_rn(w - __half2float(hi));
+        dst[0] = __half_as_ushort(hi);
+        dst[kSplitChunk] = __half_as_ushort(lo);
+    }
+}
+
+// split dense rows: Xs[r][c][e] = hi(X[r][64c+e]), Xs[r][c][64+e] = lo(...); Xs zeroed beforehand
+template <bool BF16>
+__global__ void split_dense_kernel(const float *__restrict__ X, int n, int ld, int d, int nchunk,
+                                   const double *__restrict__ xinv, uint16_t *__restrict__ Xs)
+{
+    const long long rs = (long long)nchunk * 2 * kSplitChunk;
+    const long long total = (long long)n * d;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long r = idx / d;
+        const int k = (int)(idx - r * d);
+        const float s = BF16 ? 1.0f : (float)(1.0 / xinv[r]);
+        split_store<BF16>(X[r * ld + k], s, Xs + r * rs + (long long)(k / kSplitChunk) * (2 * kSplitChunk) + (k % kSplitChunk));
+    }
+}
+
+// split CSR rows (Xs zeroed beforehand): one thread per stored value
+template <bool BF16>
+__global__ void split_csr_kernel(const long long *__restrict__ rowptr, const int *__restrict__ col,
+                                 const float *__restrict__ val, int n, int nchunk, const double *__restrict__ xinv,
+                                 uint16_t *__restrict__ Xs)
+{
+    const long long nnz = rowptr[n];
+    const long long rs = (long long)nchunk * 2 * kSplitChunk;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+        int a = 0, b = n;                            // row of e: last a with rowptr[a] <= e
+        while (b - a > 1) {
+            const int m = (a + b) >> 1;
+            if (rowptr[m] <= e) a = m; else b = m;
+        }
+        const int k = col[e];
+        const float s = BF16 ? 1.0f : (float)(1.0 / xinv[a]);
+        split_store<BF16>(val[e], s, Xs + a * rs + (long long)(k / kSplitChunk) * (2 * kSplitChunk) + (k % kSplitChunk));
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_split(const DeviceRows &rows, int form, int nchunk, uint16_t *Xs, double *xinv, cudaStream_t s)
+{
+    const int n = rows.n;
+    if (n <= 0) return cudaSuccess;
+    const bool bf16 = form == FORM_BF16X3;
+    const DevX x = rows.view(FORM_EXACT);
+    if (!bf16) {
+        row_scale_kernel<<<(int)std::min<long long>(((long long)n * 32 + 255) / 256, 148LL * 32), 256, 0, s>>>(x, n, xinv);
+        count_launch();
+    }
+    if (rows.dense) {
+        const long long total = (long long)n * rows.d;
+        const int blocks = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32));
+        if (bf16) split_dense_kernel<true><<<blocks, 256, 0, s>>>(rows.X, n, rows.ld, rows.d, nchunk, xinv, Xs);
+        else split_dense_kernel<false><<<blocks, 256, 0, s>>>(rows.X, n, rows.ld, rows.d, nchunk, xinv, Xs);
+    } else {
+        const int blocks = (int)std::max<long long>(1, std::min<long long>((rows.nnz + 255) / 256, 148LL * 32));
+        if (bf16) split_csr_kernel<true><<<blocks, 256, 0, s>>>(rows.rowptr, rows.col, rows.val, n, nchunk, xinv, Xs);
+        else split_csr_kernel<false><<<blocks, 256, 0, s>>>(rows.rowptr, rows.col, rows.val, n, nchunk, xinv, Xs);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, int form, const int *d_ia, int ma,
+                                const int *d_ib, int nb, double *d_out, long long ldo, int *d_err, cudaStream_t s)
+{
+    if (ma <= 0 || nb <= 0) return cudaSuccess;
+    if (is_tc_form(form)) {
+        const bool bf16 = form == FORM_BF16X3;
+        const void *fn = bf16 ? (const void *)gram_split_kernel<true> : (const void *)gram_split_kernel<false>;
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem);
+        if (e != cudaSuccess) return e;
+        GramArgs a;
+        a.xs = rows.Xs;
+        a.xinv = rows.xinv;
+        a.nchunk = rows.nchunk;
+        a.rs = (long long)rows.nchunk * 2 * kSplitChunk;
+        a.ia = d_ia; a.ma = ma; a.ib = d_ib; a.nb = nb;
+        a.kp = kp;
+        a.xsq = rows.xsq[FORM_EXACT];
+        a.out = d_out; a.ldo = ldo;
+        a.err = d_err;
+        dim3 grid((nb + kGN - 1) / kGN, (ma + kGM - 1) / kGM);
+        if (bf16) gram_split_kernel<true><<<grid, 128, kGSmem, s>>>(a);
+        else gram_split_kernel<false><<<grid, 128, kGSmem, s>>>(a);
+    } else {
+        dim3 grid((nb + 15) / 16, (ma + 15) / 16), block(16, 16);
+        if (form == FORM_EXACT)
+            kblock_cuda_kernel<FORM_EXACT><<<grid, block, 0, s>>>(rows.view(FORM_EXACT), d_ia, ma, d_ib, nb, kp, d_out, ldo);
+        else
+            kblock_cuda_kernel<FORM_FP32><<<grid, block, 0, s>>>(rows.view(FORM_FP32), d_ia, ma, d_ib, nb, kp, d_out, ldo);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace svmb

@@ -186,6 +186,9 @@ extern "C" int svmb_solve_dense_noalloc(int n, int ld, const float *X, const dou
     D.x.val = nullptr;
     D.x.d = ld;
     D.x.xsq = xsq;
+    D.x.Xs = nullptr;
+    D.x.nchunk = 0;
+    D.x.xinv = nullptr;
     D.G = G; D.G_bar = G_bar; D.alpha = alpha; D.p = pvec; D.QD = QD;
     D.y = yy; D.status = status; D.pos_local = pos_local; D.pos_row = pos_row;
     D.alpha_local = alpha_local; D.out = d_out;
@@ -198,6 +201,8 @@ extern "C" int svmb_solve_dense_noalloc(int n, int ld, const float *X, const dou
     D.chunk_cap = (int)chunk_cap;
     D.prefetch = stage_cap > 0 ? std::min(kPrefetchMax, stage_cap) : kPrefetchMax;
     if (params->prefetch > 0) D.prefetch = std::min(D.prefetch, params->prefetch);
+    D.lazy_gbar = 0;
+    D.tc_n = 0;
     int block_inst[kNoAllocMaxBlocks];
     for (int b = 0; b < nb; b++) block_inst[b] = 0;
 

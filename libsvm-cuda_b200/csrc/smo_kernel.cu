@@ -37,6 +37,8 @@
 // Every wait is bounded: a poll that exceeds kWaitTimeout cycles sets the
 // group's error flag and every block of the group returns.
 #include "engine.h"
+#include "kernel_math.cuh"
+#include "tc_sm100.cuh"
 
 #include <cuda_runtime.h>
 
@@ -66,36 +68,6 @@ __device__ __forceinline__ int ld_relaxed_i32(const int *p)
     int v;
     asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
-}
-
-// --------------------------------------------------------------------------
-// kernel values (reference svm.cpp:30-40, 235-254), no contraction
-// --------------------------------------------------------------------------
-__device__ __forceinline__ double powi_d(double base, int times)
-{
-    double tmp = base, ret = 1.0;
-    for (int t = times; t > 0; t /= 2) {
-        if (t % 2 == 1) ret = __dmul_rn(ret, tmp);
-        tmp = __dmul_rn(tmp, tmp);
-    }
-    return ret;
-}
-
-__device__ __forceinline__ double kernel_from_dot(const KernelParams &kp, double dot, double xsq_a, double xsq_b)
-{
-    switch (kp.type) {
-    case 0: return dot;
-    case 1: return powi_d(__dadd_rn(__dmul_rn(kp.gamma, dot), kp.coef0), kp.degree);
-    case 2: return exp(__dmul_rn(-kp.gamma, __dsub_rn(__dadd_rn(xsq_a, xsq_b), __dmul_rn(2.0, dot))));
-    case 3: return tanh(__dadd_rn(__dmul_rn(kp.gamma, dot), kp.coef0));
-    default: return 0.0;
-    }
-}
-
-// Q value exactly as the reference stores it: (Qfloat)(y_i*y_j*K)  (svm.cpp:1337)
-__device__ __forceinline__ float q_value(const KernelParams &kp, int yy, double dot, double xsq_a, double xsq_b)
-{
-    return __double2float_rn(__dmul_rn((double)yy, kernel_from_dot(kp, dot, xsq_a, xsq_b)));
 }
 
 // --------------------------------------------------------------------------
@@ -549,6 +521,15 @@ struct Shared {
     int nfill;
     int pick[kPrefetchMax];
     int npick;
+    // tensor-core block products (FORM_BF16X3, FORM_FP16X3): sources of the current pass
+    // (row id, position, alpha, norm, C, inverse scale, label, status), the
+    // pipeline's mbarriers (one per operand stage) and the TMEM base address
+    int tsrow[kTcMaxN], tspos[kTcMaxN];
+    double tsa[kTcMaxN], tsx[kTcMaxN], tsc[kTcMaxN], tsi[kTcMaxN];
+    signed char tsy[kTcMaxN];
+    unsigned char tss[kTcMaxN];
+    uint64_t tbar[kTcStages];
+    uint32_t tmem;
 };
 
 // The group's prefetch candidates (kPrefetchCand per block).  They live in
@@ -577,6 +558,8 @@ struct Ctx {
     int epoch;
     int phase;              // exchange counter: selects the record buffer and sequence number
     Partial *lrec;          // single-block groups keep their two records in shared memory
+    uint32_t tcbase;        // FORM_BF16X3: shared address of the operand stages (1024-aligned)
+    long long tc_g, tc_t;   // tensor-core steps and tiles issued so far (mbarrier phase parities)
 };
 
 __device__ __forceinline__ void set_chunks(Ctx &c)
@@ -794,6 +777,292 @@ __device__ void accumulate_rows(Ctx &c, Shared &sh, int src_end, int pick_free_o
     }
 }
 
+// --------------------------------------------------------------------------
+// tensor-core block products (FORM_BF16X3, FORM_FP16X3)
+// --------------------------------------------------------------------------
+// dot(x_t, x_s) for the targets t in [lo,hi) -- chunk-local indices into the
+// shared-memory chunk, or with `global_targets` positions of the global state
+// -- against the ns <= tc_n sources whose row ids are in sh.tsrow, with the
+// split of the form (x = hi + lo in bf16, or x 2^e = hi + lo in fp16;
+// hi.lo + lo.hi + hi.hi, 3 MMAs per K-step of 16).
+//
+// Each step is one 64-feature chunk of one 128-target tile; its 12 MMAs start
+// a fresh float32 accumulator in TMEM (two, alternating), and while the next
+// chunk's MMAs run, the threads add the finished chunk into float64 registers:
+// the tensor core's float32 accumulation then spans 64 features only, so its
+// rounding stays at the level of a float32 dot product of that length.  The
+// cross terms are issued before hi.hi so that they are added while the
+// accumulator is small.  When a tile's last chunk is absorbed, `epi(tile_lo,
+// acc)` runs on every thread: warp w holds TMEM lanes 32(w%4).. (targets) and,
+// if 16(w/4) < N, columns 16(w/4)..+15 (sources) of the tile in acc[16].
+//
+// Operand stages (kTcStages deep) are filled by cp.async with 16-byte pieces
+// of gathered rows into 128B-swizzled K-major tiles; thread 0 issues the
+// MMAs and commits each step to its stage's mbarrier.  Every commit is waited
+// for exactly once, in order, so the phase parities follow from the running
+// step counter c.tc_g.  A wait that times out sets the group's error flag and
+// the product returns false.
+template <class Epi>
+__device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool global_targets, Epi &&epi)
+{
+    const InstanceDesc &D = *c.D;
+    const int NK = D.x.nchunk;
+    const int ntiles = hi > lo ? (hi - lo + kTcM - 1) / kTcM : 0;
+    const int total = ntiles * NK;
+    if (total <= 0 || ns <= 0) return true;
+    const int N = (ns + 15) & ~15;                      // MMA N for M = 128: multiple of 16
+    const uint32_t idesc = tc::idesc_f16_f32(kTcM, N, D.form == FORM_BF16X3);
+    const uint32_t sbytes = (uint32_t)tc_stage_bytes(D.tc_n);
+    const uint32_t a_lo = kTcM * 128u;                  // target lo tile
+    const uint32_t b_hi = 2u * kTcM * 128u;             // source hi tile
+    const uint32_t b_lo = b_hi + (uint32_t)D.tc_n * 128u;
+    const long long rs = (long long)NK * 2 * kSplitChunk;
+    const uint16_t *Xs = D.x.Xs;
+    const int warp = threadIdx.x >> 5;
+    const int lg = warp & 3, cg = warp >> 2;
+    const bool reader = cg * 16 < N;
+    auto load = [&](int g) {
+        const int tile = g / NK, kc = g - tile * NK;
+        const uint32_t sa = c.tcbase + (uint32_t)((c.tc_g + g) % kTcStages) * sbytes;
+        const int tb = lo + tile * kTcM;
+        for (int i = threadIdx.x; i < kTcM * 16; i += blockDim.x) {
+            const int r = i >> 4, q = i & 15;
+            const int t = tb + r;
+            const bool ok = t < hi;
+            const int row = ok ? (global_targets ? D.pos_row[t] : c.sRow[t]) : 0;
+            tc::cp_async16(sa + (q >= 8 ? a_lo : 0u) + tc::sw128_offset(r, q & 7),
+                           Xs + (long long)row * rs + kc * 128 + q * 8, ok ? 16u : 0u);
+        }
+        for (int i = threadIdx.x; i < N * 16; i += blockDim.x) {
+            const int r = i >> 4, q = i & 15;
+            const bool ok = r < ns;
+            const int row = ok ? sh.tsrow[r] : 0;
+            tc::cp_async16(sa + (q >= 8 ? b_lo : b_hi) + tc::sw128_offset(r, q & 7),
+                           Xs + (long long)row * rs + kc * 128 + q * 8, ok ? 16u : 0u);
+        }
+    };
+    double acc[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) acc[k] = 0.0;
+    // add the finished chunk of global step Gs (its MMAs have completed) into acc
+    auto absorb = [&](long long Gs) {
+        tc::tc_fence_after();
+        if (reader) {
+            float v[16];
+            tc::tmem_ld16(sh.tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)((Gs & 1) * kTcMaxN + cg * 16), v);
+#pragma unroll
+            for (int k = 0; k < 16; k++) acc[k] = __dadd_rn(acc[k], (double)v[k]);
+        }
+    };
+    auto finish_tile = [&](int tile) {
+        epi(lo + tile * kTcM, acc);
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc[k] = 0.0;
+    };
+    for (int g = 0; g < kTcStages - 1; g++) {
+        if (g < total) load(g);
+        tc::cp_async_commit();
+    }
+    bool ok = true;
+    for (int g = 0; g < total; g++) {
+        const long long G = c.tc_g + g;
+        const int tile = g / NK, kc = g - tile * NK;
+        // the MMAs of step g-1 have read their stage and written their accumulator
+        bool w = true;
+        if (g >= 1) w = tc::mbar_wait(&sh.tbar[(G - 1) % kTcStages], (unsigned)(((G - 1) / kTcStages) & 1));
+        if (w && g + kTcStages - 1 < total) load(g + kTcStages - 1);
+        tc::cp_async_commit();
+        tc::cp_async_wait<kTcStages - 1>();             // step g has landed
+        tc::fence_async_smem();
+        ok = __syncthreads_and(w) != 0;
+        if (!ok) break;
+        if (threadIdx.x == 0) {
+            tc::tc_fence_after();
+            const uint32_t sa = c.tcbase + (uint32_t)(G % kTcStages) * sbytes;
+            const uint32_t dst = sh.tmem + (uint32_t)((G & 1) * kTcMaxN);
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                const uint64_t ah = tc::sw128_desc(sa + kk * 32), al = tc::sw128_desc(sa + a_lo + kk * 32);
+                const uint64_t bh = tc::sw128_desc(sa + b_hi + kk * 32), bl = tc::sw128_desc(sa + b_lo + kk * 32);
+                tc::mma_bf16(dst, ah, bl, idesc, kk > 0);
+                tc::mma_bf16(dst, al, bh, idesc, true);
+                tc::mma_bf16(dst, ah, bh, idesc, true);
+            }
+            tc::mma_commit(&sh.tbar[G % kTcStages]);
+        }
+        if (g >= 1) {
+            absorb(G - 1);
+            if (kc == 0) finish_tile(tile - 1);
+            tc::tc_fence_before();
+        }
+        __syncthreads();
+    }
+    if (ok) {
+        const long long G = c.tc_g + total - 1;
+        ok = __syncthreads_and(tc::mbar_wait(&sh.tbar[G % kTcStages], (unsigned)((G / kTcStages) & 1))) != 0;
+        if (ok) {
+            absorb(G);
+            finish_tile(ntiles - 1);
+            tc::tc_fence_before();
+        }
+    }
+    tc::cp_async_wait<0>();
+    c.tc_g += total;
+    c.tc_t += ntiles;
+    if (!ok && threadIdx.x == 0) atomicExch(&D.sync->error, 1);
+    __syncthreads();
+    return ok;
+}
+
+// tensor-core form of fill_rows: Q rows of ns (<= kPrefetchMax) sources into
+// cache slots, on my chunk of [0,A) (tail = 0) or of [A,l) (tail = 1)
+__device__ bool fill_rows_tc(Ctx &c, Shared &sh, int ns, const int *src_row, const int *src_y, const long long *slot,
+                             int tail)
+{
+    const InstanceDesc &D = *c.D;
+    if (ns == 0) return true;
+    if (threadIdx.x < ns) sh.tsrow[threadIdx.x] = src_row[threadIdx.x];
+    double xs[kPrefetchMax], is[kPrefetchMax];
+    float *dst[kPrefetchMax];
+    int sy[kPrefetchMax];
+#pragma unroll
+    for (int k = 0; k < kPrefetchMax; k++) {
+        const int kk = k < ns ? k : 0;
+        xs[k] = D.x.xsq[src_row[kk]];
+        is[k] = D.x.xinv ? D.x.xinv[src_row[kk]] : 1.0;
+        dst[k] = D.cache.data + slot[kk] * D.cache.stride;
+        sy[k] = src_y[kk];
+    }
+    __syncthreads();
+    const int lo = tail ? c.t0 : 0, hi = tail ? c.t1 : c.a1 - c.a0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    return tc_product(c, sh, ns, lo, hi, tail != 0, [&](int tlo, const double *acc) {
+        if (warp < 4) {
+            const int t = tlo + warp * 32 + lane;
+            if (t < hi) {
+                int r, yp, col;
+                if (tail) {
+                    r = D.pos_row[t];
+                    yp = D.y[t];
+                    col = D.pos_local[t];
+                } else {
+                    r = c.sRow[t];
+                    yp = c.sY[t];
+                    col = c.sCol[t];
+                }
+                const double xe = D.x.xsq[r];
+                const double ie = D.x.xinv ? D.x.xinv[r] : 1.0;
+#pragma unroll
+                for (int k = 0; k < kPrefetchMax; k++)
+                    if (k < ns) dst[k][col] = q_value(D.kp, sy[k] * yp, __dmul_rn(__dmul_rn(acc[k], ie), is[k]), xs[k], xe);
+            }
+        }
+    });
+}
+
+// tensor-core form of accumulate_rows: sources are taken kTcMaxN (tc_n) at a
+// time; per target the contributions of one pass are summed in source order
+// in four column groups, which are then added in a fixed order
+__device__ bool accumulate_rows_tc(Ctx &c, Shared &sh, int src_end, int pick_free_only, int with_bar, int lo, int hi)
+{
+    const InstanceDesc &D = *c.D;
+    const int cap = D.tc_n;
+    int scan = 0;
+    double *red = reinterpret_cast<double *>(c.tile);   // [2][4][kTcM] partial sums (aux area)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lg = warp & 3, cg = warp >> 2;
+    while (true) {
+        if (threadIdx.x == 0) sh.nsrc = 0;
+        __syncthreads();
+        while (scan < src_end) {
+            const int p = scan + threadIdx.x;
+            int sel = 0;
+            if (p < src_end) {
+                const unsigned char s = D.status[p];
+                sel = pick_free_only ? (s == ST_FREE) : (s != ST_LOWER);
+            }
+            int tot;
+            const int pre = block_excl_scan(sh.red, sel, &tot);
+            const int have = sh.nsrc;
+            const int room = cap - have;
+            if (sel && pre < room) sh.tspos[have + pre] = p;
+            const int take = tot < room ? tot : room;
+            if (take < tot && sel && pre == take) sh.stop_at = threadIdx.x;
+            __syncthreads();
+            const int consumed = take == tot ? (int)blockDim.x : sh.stop_at;
+            __syncthreads();
+            if (threadIdx.x == 0) sh.nsrc = have + take;
+            scan += consumed;
+            __syncthreads();
+            if (sh.nsrc == cap) break;
+        }
+        const int ns = sh.nsrc;
+        if (ns == 0) break;
+        if (threadIdx.x < ns) {
+            const int sp = sh.tspos[threadIdx.x];
+            const int r = D.pos_row[sp];
+            const int y = D.y[sp];
+            sh.tsrow[threadIdx.x] = r;
+            sh.tsa[threadIdx.x] = D.alpha[sp];
+            sh.tsx[threadIdx.x] = D.x.xsq[r];
+            sh.tsi[threadIdx.x] = D.x.xinv ? D.x.xinv[r] : 1.0;
+            sh.tsc[threadIdx.x] = get_C(D, y);
+            sh.tsy[threadIdx.x] = (signed char)y;
+            sh.tss[threadIdx.x] = D.status[sp];
+        }
+        __syncthreads();
+        const bool ok = tc_product(c, sh, ns, lo, hi, true, [&](int tlo, const double *acc) {
+            const int t = tlo + lg * 32 + lane;
+            double part = 0.0, partb = 0.0;
+            if (cg * 16 < ns && t < hi) {
+                const int r = D.pos_row[t];
+                const int ye = D.y[t];
+                const double xe = D.x.xsq[r];
+                const double ie = D.x.xinv ? D.x.xinv[r] : 1.0;
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const int s = cg * 16 + k;
+                    if (s < ns) {
+                        const double dot = __dmul_rn(__dmul_rn(acc[k], ie), sh.tsi[s]);
+                        const float q = q_value(D.kp, sh.tsy[s] * ye, dot, sh.tsx[s], xe);
+                        part = __dadd_rn(part, __dmul_rn(sh.tsa[s], (double)q));
+                        if (with_bar && sh.tss[s] == ST_UPPER) partb = __dadd_rn(partb, __dmul_rn(sh.tsc[s], (double)q));
+                    }
+                }
+            }
+            red[cg * kTcM + lg * 32 + lane] = part;
+            red[4 * kTcM + cg * kTcM + lg * 32 + lane] = partb;
+            __syncthreads();
+            if (cg == 0 && t < hi) {
+                double g = D.G[t];
+                for (int k = 0; k < 4; k++) g = __dadd_rn(g, red[k * kTcM + lg * 32 + lane]);
+                D.G[t] = g;
+                if (with_bar) {
+                    double gb = D.G_bar[t];
+                    for (int k = 0; k < 4; k++) gb = __dadd_rn(gb, red[4 * kTcM + k * kTcM + lg * 32 + lane]);
+                    D.G_bar[t] = gb;
+                }
+            }
+            __syncthreads();
+        });
+        if (!ok) return false;
+        if (ns < cap) break;
+    }
+    return true;
+}
+
+// the row-block product of the form: CUDA cores or tensor cores
+template <int FORM>
+__device__ bool accumulate(Ctx &c, Shared &sh, int src_end, int pick_free_only, int with_bar, int lo, int hi)
+{
+    if constexpr (is_tc_form(FORM)) {
+        return accumulate_rows_tc(c, sh, src_end, pick_free_only, with_bar, lo, hi);
+    } else {
+        accumulate_rows<FORM>(c, sh, src_end, pick_free_only, with_bar, lo, hi);
+        return true;
+    }
+}
+
 // gradient reconstruction (reference svm.cpp:473-513); group collective on the
 // global state (the caller has stored its chunk)
 template <int FORM>
@@ -801,9 +1070,16 @@ __device__ bool reconstruct(Ctx &c, Shared &sh)
 {
     const InstanceDesc &D = *c.D;
     if (c.A == D.l) return true;
+    if (D.lazy_gbar) {
+        // G = p + sum over every alpha > 0 (active or not) of alpha * Q, on the inactive positions
+        for (int e = c.t0 + threadIdx.x; e < c.t1; e += blockDim.x) D.G[e] = D.p[e];
+        __syncthreads();
+        if (!accumulate<FORM>(c, sh, D.l, 0, 0, c.t0, c.t1)) return false;
+        return exchange(c, sh);
+    }
     for (int e = c.t0 + threadIdx.x; e < c.t1; e += blockDim.x) D.G[e] = __dadd_rn(D.G_bar[e], D.p[e]);
     __syncthreads();
-    accumulate_rows<FORM>(c, sh, c.A, 1, 0, c.t0, c.t1);
+    if (!accumulate<FORM>(c, sh, c.A, 1, 0, c.t0, c.t1)) return false;
     return exchange(c, sh);
 }
 
@@ -1189,6 +1465,18 @@ __device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const 
     unstage_sources(D, c.stage, sh.ss);
 }
 
+// the fill pass of the form: CUDA cores or tensor cores
+template <int FORM>
+__device__ bool fill(Ctx &c, Shared &sh, int ns, const int *src_row, const int *src_y, const long long *slot, int tail)
+{
+    if constexpr (is_tc_form(FORM)) {
+        return fill_rows_tc(c, sh, ns, src_row, src_y, slot, tail);
+    } else {
+        fill_rows<FORM>(c, sh, ns, src_row, src_y, slot, tail);
+        return true;
+    }
+}
+
 // position of the phase-A winner of track k (excluded from prefetching)
 __device__ __forceinline__ int i0_prev_guard(const Shared &sh, int k) { return sh.bi[4 * k]; }
 
@@ -1207,10 +1495,19 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
     c.phase = 0;
     c.lrec = sh.lrec;
     {
-        // dynamic shared memory: [stage][tiles][G][alpha][QD][col][row][y][status]
-        size_t off = (size_t)D.stage_cap * D.stage_lds * sizeof(float);
+        // dynamic shared memory: [tensor-core stages][stage][tiles][G][alpha][QD][col][row][y][status]
+        size_t off = 0;
+        c.tcbase = 0;
+        c.tc_g = 0;
+        c.tc_t = 0;
+        if constexpr (is_tc_form(FORM)) {
+            const uint32_t raw = tc::smem_addr(dyn);
+            c.tcbase = (raw + 1023u) & ~1023u;
+            off = (size_t)tc_area_bytes(D.tc_n);
+        }
+        c.stage = reinterpret_cast<float *>(dyn + off);
+        off += (size_t)D.stage_cap * D.stage_lds * sizeof(float);
         off = (off + 15) & ~(size_t)15;
-        c.stage = reinterpret_cast<float *>(dyn);
         c.tile = reinterpret_cast<float *>(dyn + off);
         c.pt = reinterpret_cast<PrefetchTable *>(dyn + off);
         off += kAuxBytes;
@@ -1264,7 +1561,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
         for (int p = threadIdx.x; p < l; p += blockDim.x) any |= D.alpha[p] > 0 ? 1 : 0;
         any = __syncthreads_or(any);
         if (any) {
-            accumulate_rows<FORM>(c, sh, l, 0, 1, c.a0, c.a1);
+            if (!accumulate<FORM>(c, sh, l, 0, D.lazy_gbar ? 0 : 1, c.a0, c.a1)) goto fail;
             if (!exchange(c, sh)) goto fail;
         }
         chunk_load(c);
@@ -1413,7 +1710,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 const int ns = sh.nfill;
                 SVMB_PROF(kProfAReduce);
                 if (ns > 0) {
-                    fill_rows<FORM>(c, sh, ns, sh.frow, sh.fy, sh.fslot, 0);
+                    if (!fill<FORM>(c, sh, ns, sh.frow, sh.fy, sh.fslot, 0)) goto fail;
                     cnt_q += (long long)ns * c.A;
                     cnt_fill++;
                 }
@@ -1556,7 +1853,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 const int srow[1] = {row_j};
                 const int sy[1] = {yj};
                 const long long ss[1] = {slot_j};
-                fill_rows<FORM>(c, sh, 1, srow, sy, ss, 0);
+                if (!fill<FORM>(c, sh, 1, srow, sy, ss, 0)) goto fail;
                 cnt_q += c.A;
                 cnt_fill++;
             }
@@ -1602,8 +1899,8 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
             const double daj = __dsub_rn(aj, alpha_j);
             const unsigned char old_si = status_of(alpha_i, C_i), old_sj = status_of(alpha_j, C_j);
             const unsigned char new_si = status_of(ai, C_i), new_sj = status_of(aj, C_j);
-            const bool bar_i = (old_si == ST_UPPER) != (new_si == ST_UPPER);
-            const bool bar_j = (old_sj == ST_UPPER) != (new_sj == ST_UPPER);
+            const bool bar_i = !D.lazy_gbar && (old_si == ST_UPPER) != (new_si == ST_UPPER);
+            const bool bar_j = !D.lazy_gbar && (old_sj == ST_UPPER) != (new_sj == ST_UPPER);
             // complete rows for the G_bar update: fill the tail [A,l) where missing
             if ((bar_i || bar_j) && c.A < l) {
                 if (threadIdx.x == 0) {
@@ -1629,7 +1926,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 long long sslot[2] = {0, 0};
                 if (sh.bi[17]) { srow[ns] = row_i; sy[ns] = yi; sslot[ns] = slot_i; ns++; }
                 if (sh.bi[18]) { srow[ns] = row_j; sy[ns] = yj; sslot[ns] = slot_j; ns++; }
-                fill_rows<FORM>(c, sh, ns, srow, sy, sslot, 1);
+                if (!fill<FORM>(c, sh, ns, srow, sy, sslot, 1)) goto fail;
                 cnt_q += (long long)ns * (l - c.A);
             }
             SVMB_PROF(kProfBFill);
@@ -1801,7 +2098,26 @@ smo_persistent(const InstanceDesc *__restrict__ insts, const int *__restrict__ b
     const int inst = block_inst[blockIdx.x];
     const InstanceDesc &D = insts[inst];
     const int rank = blockIdx.x - D.block0;
+    if constexpr (is_tc_form(FORM)) {
+        // mbarriers of the tensor-core pipeline and the TMEM accumulator (one block per SM)
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < kTcStages; k++) tc::mbar_init(&sh.tbar[k], 1);
+            tc::mbar_init_fence();
+        }
+        if (threadIdx.x < 32) {
+            tc::tmem_alloc(&sh.tmem, 2 * kTcMaxN);
+            tc::tmem_relinquish();
+        }
+        tc::tc_fence_before();
+        __syncthreads();
+        tc::tc_fence_after();
+    }
     solve_instance<FORM>(D, rank, sh, dyn);
+    if constexpr (is_tc_form(FORM)) {
+        tc::tc_fence_before();
+        __syncthreads();
+        if (threadIdx.x < 32) tc::tmem_dealloc(sh.tmem, 2 * kTcMaxN);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1859,11 +2175,19 @@ cudaError_t launch_scatter_dense(const long long *rowptr, const int *col, const 
     return cudaGetLastError();
 }
 
+static const void *smo_fn(int form)
+{
+    if (form == FORM_EXACT) return (const void *)smo_persistent<FORM_EXACT>;
+    if (form == FORM_FP32) return (const void *)smo_persistent<FORM_FP32>;
+    if (form == FORM_BF16X3) return (const void *)smo_persistent<FORM_BF16X3>;
+    return (const void *)smo_persistent<FORM_FP16X3>;
+}
+
 cudaError_t launch_smo(int form, const InstanceDesc *d_insts, const int *d_block_inst, int nblocks,
                        size_t dyn_smem, bool cooperative, cudaStream_t s)
 {
     void *args[] = {(void *)&d_insts, (void *)&d_block_inst};
-    const void *fn = form == FORM_EXACT ? (const void *)smo_persistent<FORM_EXACT> : (const void *)smo_persistent<FORM_FP32>;
+    const void *fn = smo_fn(form);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
     if (e != cudaSuccess) return e;
     if (cooperative)
@@ -1873,7 +2197,7 @@ cudaError_t launch_smo(int form, const InstanceDesc *d_insts, const int *d_block
 
 cudaError_t smo_max_blocks(int form, size_t dyn_smem, int *blocks_per_sm)
 {
-    const void *fn = form == FORM_EXACT ? (const void *)smo_persistent<FORM_EXACT> : (const void *)smo_persistent<FORM_FP32>;
+    const void *fn = smo_fn(form);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, kThreads, dyn_smem);
@@ -1881,10 +2205,13 @@ cudaError_t smo_max_blocks(int form, size_t dyn_smem, int *blocks_per_sm)
 
 int smo_static_smem()
 {
-    cudaFuncAttributes a, b;
-    if (cudaFuncGetAttributes(&a, (const void *)smo_persistent<FORM_EXACT>) != cudaSuccess) return 16384;
-    if (cudaFuncGetAttributes(&b, (const void *)smo_persistent<FORM_FP32>) != cudaSuccess) return (int)a.sharedSizeBytes;
-    return (int)(a.sharedSizeBytes > b.sharedSizeBytes ? a.sharedSizeBytes : b.sharedSizeBytes);
+    int most = 0;
+    for (int f = 0; f < kNumForms; f++) {
+        cudaFuncAttributes a;
+        if (cudaFuncGetAttributes(&a, smo_fn(f)) != cudaSuccess) return 16384;
+        most = (int)a.sharedSizeBytes > most ? (int)a.sharedSizeBytes : most;
+    }
+    return most;
 }
 
 }  // namespace svmb

@@ -15,7 +15,7 @@ PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_DIR, "libsvm_b200.so")
 CLI_PATH = os.path.join(PKG_DIR, "svm-train")
 
-FORM_EXACT, FORM_FP32 = 0, 1
+FORM_EXACT, FORM_FP32, FORM_BF16X3, FORM_FP16X3 = 0, 1, 2, 3
 
 
 class EngineError(RuntimeError):
@@ -40,16 +40,18 @@ class SvmbParams(C.Structure):
     _fields_ = [("svm_type", C.c_int), ("kernel_type", C.c_int), ("degree", C.c_int), ("shrinking", C.c_int),
                 ("gamma", C.c_double), ("coef0", C.c_double), ("C_pos", C.c_double), ("C_neg", C.c_double),
                 ("nu", C.c_double), ("eps", C.c_double), ("cache_mb", C.c_double), ("form", C.c_int),
-                ("blocks", C.c_int), ("prefetch", C.c_int)]
+                ("blocks", C.c_int), ("prefetch", C.c_int), ("gbar_mode", C.c_int)]
 
 
 def make_params(svm_type=0, kernel_type=2, degree=3, gamma=0.0, coef0=0.0, C_pos=1.0, C_neg=None, nu=0.5,
-                eps=1e-3, cache_mb=100.0, shrinking=1, form=FORM_EXACT, blocks=0, prefetch=0) -> SvmbParams:
+                eps=1e-3, cache_mb=100.0, shrinking=1, form=FORM_EXACT, blocks=0, prefetch=0,
+                gbar_mode=0) -> SvmbParams:
     p = SvmbParams()
     p.svm_type, p.kernel_type, p.degree, p.shrinking = svm_type, kernel_type, degree, shrinking
     p.gamma, p.coef0, p.C_pos = gamma, coef0, C_pos
     p.C_neg = C_pos if C_neg is None else C_neg
     p.nu, p.eps, p.cache_mb, p.form, p.blocks, p.prefetch = nu, eps, cache_mb, form, blocks, prefetch
+    p.gbar_mode = gbar_mode
     return p
 
 
@@ -89,6 +91,8 @@ def _load(path: str) -> C.CDLL:
     lib.svmb_rows_solve_many.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, _P(SvmbParams),
                                          C.c_void_p, _P(SolveStats)]
     lib.svmb_rows_free.argtypes = [C.c_void_p]
+    lib.svmb_rows_kernel_block.argtypes = [C.c_void_p, _P(SvmbParams), C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                           C.c_void_p]
     return lib
 
 
@@ -249,6 +253,16 @@ class ResidentRows:
                                                prm, alpha.ctypes.data, st)
         self.eng._ok(rc, "svmb_rows_solve_many")
         return [alpha[ptr[k]:ptr[k + 1]] for k in range(len(params))], [s.as_dict() for s in st]
+
+    def kernel_block(self, ia, ib, params: SvmbParams) -> np.ndarray:
+        """K(x_ia[i], x_ib[j]) as a float64 [len(ia)][len(ib)] array (svmb_rows_kernel_block)."""
+        ia = np.ascontiguousarray(ia, dtype=np.int32)
+        ib = np.ascontiguousarray(ib, dtype=np.int32)
+        out = np.zeros((len(ia), len(ib)))
+        rc = self.eng.lib.svmb_rows_kernel_block(self.h, C.byref(params), len(ia), ia.ctypes.data, len(ib),
+                                                 ib.ctypes.data, out.ctypes.data)
+        self.eng._ok(rc, "svmb_rows_kernel_block")
+        return out
 
     def free(self):
         if self.h:
