@@ -117,8 +117,10 @@ int svmb_solve_binary_csr(int n, int d, const long long *rowptr, const int *col,
 /* Many independent binary solves over subsets of one row set, in ONE
  * persistent device launch (one-vs-one pairs, CV folds, grid points).
  * Instance k uses rows inst_rows[inst_ptr[k] .. inst_ptr[k+1]) with labels
- * inst_y[same range] and params[k]; kernel parameters and form must agree
- * across instances.  alpha_out is laid out like inst_rows. */
+ * inst_y[same range] and params[k] (each instance has its own kernel, C,
+ * eps, cache budget ...: a C x gamma grid of CV folds is one call); only the
+ * arithmetic form must agree across instances.  alpha_out is laid out like
+ * inst_rows. */
 int svmb_solve_many_csr(int n, int d, const long long *rowptr, const int *col, const float *val,
                         int ninst, const int *inst_ptr, const int *inst_rows, const double *inst_y,
                         const svmb_params *params, double *alpha_out, svmb_solve_stats *stats);
@@ -157,6 +159,38 @@ void svmb_rows_free(svmb_rows *rows);
  * tensor cores, the other forms on CUDA cores.  ia, ib, out are host arrays. */
 int svmb_rows_kernel_block(const svmb_rows *rows, const svmb_params *params, int ma, const int *ia, int nb,
                            const int *ib, double *out);
+
+/* ---- request loop (continuous batching of independent solves) ------------
+ * No counterpart in the reference, which trains one problem per call.  A
+ * scheduler thread admits requests in arrival order while their device memory
+ * (rows + solver state with the Q-row cache budget) fits the server's budget
+ * and the thread blocks they need fit the SMs that no running launch holds,
+ * and launches them together next to the launches already running (up to
+ * max_inflight at a time).  A request's result equals its solve alone. */
+typedef struct svmb_server svmb_server;
+typedef struct svmb_server_config {
+    long long mem_bytes;     /* device memory for admitted requests; 0 = 80% of the free memory */
+    int max_inflight;        /* concurrent launches; 0 = 4 */
+    int max_batch;           /* requests per launch; 0 = 64 */
+    int form;                /* SVMB_FORM_* of every request */
+} svmb_server_config;
+typedef struct svmb_server_stats {
+    long long completed, failed, waves, max_concurrent_waves, peak_mem_bytes, pending;
+    double p50_s, p99_s, max_s;   /* request latency: submit -> result ready */
+    double solves_per_s;          /* completed / (last completion - first submit) */
+} svmb_server_stats;
+
+int svmb_server_create(const svmb_server_config *cfg, svmb_server **out);
+/* One binary request from host CSR rows (copied; 0-based columns < d) and
+ * labels y[n] (y > 0 positive).  Returns a ticket >= 0, or -1. */
+long long svmb_server_submit(svmb_server *s, int n, int d, const long long *rowptr, const int *col, const float *val,
+                             const double *y, const svmb_params *params);
+int svmb_server_poll(svmb_server *s, long long ticket);       /* 1 finished, 0 running or queued, -1 unknown */
+/* Wait for a ticket (collected once): alpha_out[n] receives the signed
+ * coefficients as in svmb_solve_binary_csr; stats and latency_s may be NULL. */
+int svmb_server_wait(svmb_server *s, long long ticket, double *alpha_out, svmb_solve_stats *stats, double *latency_s);
+int svmb_server_get_stats(svmb_server *s, svmb_server_stats *out);
+void svmb_server_destroy(svmb_server *s);      /* finishes the admitted and queued requests first */
 
 #ifdef __cplusplus
 }

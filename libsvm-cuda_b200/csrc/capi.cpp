@@ -12,6 +12,7 @@
 #include "engine.hpp"
 #include "predict.hpp"
 #include "svm_b200.h"
+#include "capi_internal.hpp"
 
 namespace svmb {
 int api_set_option(const char *name, long long value);
@@ -22,7 +23,8 @@ struct svmb_rows {
     svmb::DeviceRows dev;
 };
 
-namespace {
+namespace svmb {
+namespace capi {
 
 int check_params(const svmb_params *p)
 {
@@ -41,121 +43,132 @@ int check_params(const svmb_params *p)
     return 0;
 }
 
-int solve_many(const svmb::DeviceRows &rows, int ninst, const int *inst_ptr, const int *inst_rows, const double *inst_y,
+SolveParams to_solve_params(const svmb_params &p)
+{
+    SolveParams prm;
+    prm.kp.type = p.kernel_type;
+    prm.kp.degree = p.degree;
+    prm.kp.gamma = p.gamma;
+    prm.kp.coef0 = p.coef0;
+    prm.eps = p.eps;
+    prm.shrinking = p.shrinking;
+    prm.cache_mb = p.cache_mb;
+    prm.form = p.form;
+    prm.blocks_override = p.blocks;
+    prm.prefetch = p.prefetch;
+    prm.lazy_gbar = p.gbar_mode == SVMB_GBAR_INCREMENTAL ? 0 : p.gbar_mode == SVMB_GBAR_RECOMPUTE ? 1 : -1;
+    return prm;
+}
+
+// one binary subproblem in the formulation of solve_c_svc / solve_nu_svc
+// (reference svm.cpp:1500-1588): labels, initial alpha, linear term, bounds
+int make_subproblem(const svmb_params &p, int l, const int *rows, const double *y, int nrows, SubProblem &sp)
+{
+    if (l < 0) { set_error("inst_ptr must be non-decreasing"); return -1; }
+    sp.rows.assign(rows, rows + l);
+    for (int r : sp.rows)
+        if (r < 0 || r >= nrows) { set_error("row id out of range"); return -1; }
+    sp.y.resize(l);
+    for (int i = 0; i < l; i++) sp.y[i] = y[i] > 0 ? +1 : -1;
+    sp.alpha0.assign(l, 0.0);
+    sp.p.assign(l, 0.0);
+    if (p.svm_type == NU_SVC) {
+        // solve_nu_svc initial point (reference svm.cpp:1546-1564)
+        int npos = 0, nneg = 0;
+        for (int i = 0; i < l; i++) (sp.y[i] > 0 ? npos : nneg)++;
+        if (p.nu * l / 2 > std::min(npos, nneg)) { set_error("specified nu is infeasible"); return -1; }
+        double sum_pos = p.nu * l / 2, sum_neg = p.nu * l / 2;
+        for (int i = 0; i < l; i++) {
+            if (sp.y[i] == +1) { sp.alpha0[i] = std::min(1.0, sum_pos); sum_pos -= sp.alpha0[i]; }
+            else { sp.alpha0[i] = std::min(1.0, sum_neg); sum_neg -= sp.alpha0[i]; }
+        }
+        sp.nu = 1;
+        sp.Cp = sp.Cn = 1.0;
+    } else {
+        for (int i = 0; i < l; i++) sp.p[i] = -1;
+        sp.Cp = p.C_pos;
+        sp.Cn = p.C_neg;
+    }
+    return 0;
+}
+
+// signed coefficients y_i alpha_i (nu-SVC: / r) and the statistics of one solve
+void finish_instance(const SubProblem &sp, const SolveResult &R, double *alpha_out, svmb_solve_stats *stats)
+{
+    const int l = (int)sp.rows.size();
+    double rho = R.out.rho, obj = R.out.obj, up = sp.Cp, un = sp.Cn;
+    for (int i = 0; i < l; i++) {
+        double v = R.alpha[i];
+        if (sp.nu) v *= sp.y[i] / R.out.r;
+        else v *= sp.y[i];
+        alpha_out[i] = v;
+    }
+    if (sp.nu) {
+        rho /= R.out.r;
+        obj /= (R.out.r * R.out.r);
+        up = un = 1 / R.out.r;
+    }
+    if (!stats) return;
+    svmb_solve_stats &st = *stats;
+    memset(&st, 0, sizeof st);
+    st.iters = R.out.iters;
+    st.obj = obj;
+    st.rho = rho;
+    st.r = R.out.r;
+    st.l = l;
+    st.status = R.out.status;
+    st.active_size = R.out.active_size;
+    st.seconds = R.seconds;
+    st.sum_active = R.out.sum_active;
+    st.q_evals = R.out.q_evals;
+    st.lookups = R.out.lookups;
+    st.hits = R.out.hits;
+    st.fills = R.out.fills;
+    st.prefetched = R.out.prefetched;
+    st.prefetch_used = R.out.prefetch_used;
+    for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
+    for (int i = 0; i < l; i++) {
+        const double v = alpha_out[i];
+        if (v != 0) {
+            st.nr_sv++;
+            if (fabs(v) >= (sp.y[i] > 0 ? up : un)) st.nr_bsv++;
+        }
+    }
+}
+
+int solve_many(const DeviceRows &rows, int ninst, const int *inst_ptr, const int *inst_rows, const double *inst_y,
                const svmb_params *params, double *alpha_out, svmb_solve_stats *stats)
 {
     if (ninst <= 0) return 0;
     for (int k = 0; k < ninst; k++) {
         if (check_params(&params[k])) return -1;
-        if (params[k].kernel_type != params[0].kernel_type || params[k].gamma != params[0].gamma ||
-            params[k].coef0 != params[0].coef0 || params[k].degree != params[0].degree || params[k].form != params[0].form ||
-            params[k].gbar_mode != params[0].gbar_mode) {
-            svmb::set_error("instances of one launch must share kernel parameters and form");
+        if (params[k].form != params[0].form) {
+            set_error("instances of one launch must share the arithmetic form");
             return -1;
         }
     }
-    std::vector<svmb::SubProblem> subs(ninst);
+    // every instance carries its own parameters (kernel, C, eps, cache, ...);
+    // only the arithmetic form is common to a launch
+    std::vector<SolveParams> own(ninst);
+    std::vector<SubProblem> subs(ninst);
     for (int k = 0; k < ninst; k++) {
         const int a = inst_ptr[k], b = inst_ptr[k + 1];
-        const int l = b - a;
-        if (l < 0) { svmb::set_error("inst_ptr must be non-decreasing"); return -1; }
-        svmb::SubProblem &sp = subs[k];
-        sp.rows.assign(inst_rows + a, inst_rows + b);
-        for (int r : sp.rows)
-            if (r < 0 || r >= rows.n) { svmb::set_error("row id out of range"); return -1; }
-        sp.y.resize(l);
-        for (int i = 0; i < l; i++) sp.y[i] = inst_y[a + i] > 0 ? +1 : -1;
-        sp.alpha0.assign(l, 0.0);
-        sp.p.assign(l, 0.0);
-        const svmb_params &p = params[k];
-        if (p.svm_type == NU_SVC) {
-            // solve_nu_svc initial point (reference svm.cpp:1546-1564)
-            int npos = 0, nneg = 0;
-            for (int i = 0; i < l; i++) (sp.y[i] > 0 ? npos : nneg)++;
-            if (p.nu * l / 2 > std::min(npos, nneg)) { svmb::set_error("specified nu is infeasible"); return -1; }
-            double sum_pos = p.nu * l / 2, sum_neg = p.nu * l / 2;
-            for (int i = 0; i < l; i++) {
-                if (sp.y[i] == +1) { sp.alpha0[i] = std::min(1.0, sum_pos); sum_pos -= sp.alpha0[i]; }
-                else { sp.alpha0[i] = std::min(1.0, sum_neg); sum_neg -= sp.alpha0[i]; }
-            }
-            sp.nu = 1;
-            sp.Cp = sp.Cn = 1.0;
-        } else {
-            for (int i = 0; i < l; i++) sp.p[i] = -1;
-            sp.Cp = p.C_pos;
-            sp.Cn = p.C_neg;
-        }
+        if (make_subproblem(params[k], b - a, inst_rows + a, inst_y + a, rows.n, subs[k]) != 0) return -1;
+        own[k] = to_solve_params(params[k]);
+        subs[k].own = &own[k];
     }
-    svmb::SolveParams prm;
-    prm.kp.type = params[0].kernel_type;
-    prm.kp.degree = params[0].degree;
-    prm.kp.gamma = params[0].gamma;
-    prm.kp.coef0 = params[0].coef0;
-    prm.eps = params[0].eps;
-    prm.shrinking = params[0].shrinking;
-    prm.cache_mb = params[0].cache_mb;
-    prm.form = params[0].form;
-    prm.blocks_override = params[0].blocks;
-    prm.prefetch = params[0].prefetch;
-    prm.lazy_gbar = params[0].gbar_mode == SVMB_GBAR_INCREMENTAL ? 0 : params[0].gbar_mode == SVMB_GBAR_RECOMPUTE ? 1 : -1;
-    for (int k = 1; k < ninst; k++)
-        if (params[k].eps != prm.eps || params[k].shrinking != prm.shrinking || params[k].cache_mb != prm.cache_mb) {
-            svmb::set_error("instances of one launch must share eps, shrinking and cache_mb");
-            return -1;
-        }
-    std::vector<svmb::SolveResult> res;
-    const auto t0 = std::chrono::steady_clock::now();
-    if (svmb::solve_batch(rows, subs, prm, res, 0) != 0) return -1;
-    const auto t1 = std::chrono::steady_clock::now();
-    for (int k = 0; k < ninst; k++) {
-        const svmb::SubProblem &sp = subs[k];
-        const svmb::SolveResult &R = res[k];
-        const int a = inst_ptr[k], l = (int)sp.rows.size();
-        double rho = R.out.rho, obj = R.out.obj, up = sp.Cp, un = sp.Cn;
-        for (int i = 0; i < l; i++) {
-            double v = R.alpha[i];
-            if (sp.nu) v *= sp.y[i] / R.out.r;
-            else v *= sp.y[i];
-            alpha_out[a + i] = v;
-        }
-        if (sp.nu) {
-            rho /= R.out.r;
-            obj /= (R.out.r * R.out.r);
-            up = un = 1 / R.out.r;
-        }
-        if (stats) {
-            svmb_solve_stats &st = stats[k];
-            memset(&st, 0, sizeof st);
-            st.iters = R.out.iters;
-            st.obj = obj;
-            st.rho = rho;
-            st.r = R.out.r;
-            st.l = l;
-            st.status = R.out.status;
-            st.active_size = R.out.active_size;
-            st.seconds = R.seconds;
-            st.sum_active = R.out.sum_active;
-            st.q_evals = R.out.q_evals;
-            st.lookups = R.out.lookups;
-            st.hits = R.out.hits;
-            st.fills = R.out.fills;
-            st.prefetched = R.out.prefetched;
-            st.prefetch_used = R.out.prefetch_used;
-            for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
-            (void)t0; (void)t1;
-            for (int i = 0; i < l; i++) {
-                const double v = alpha_out[a + i];
-                if (v != 0) {
-                    st.nr_sv++;
-                    if (fabs(v) >= (sp.y[i] > 0 ? up : un)) st.nr_bsv++;
-                }
-            }
-        }
-    }
+    std::vector<SolveResult> res;
+    if (solve_batch(rows, subs, own[0], res, 0) != 0) return -1;
+    for (int k = 0; k < ninst; k++)
+        finish_instance(subs[k], res[k], alpha_out + inst_ptr[k], stats ? &stats[k] : nullptr);
     return 0;
 }
 
-}  // namespace
+}  // namespace capi
+}  // namespace svmb
+
+using svmb::capi::check_params;
+using svmb::capi::solve_many;
 
 extern "C" {
 

@@ -127,14 +127,20 @@ int device_sm_count()
 
 DeviceRows::~DeviceRows()
 {
-    cudaFree(X);
-    cudaFree(rowptr);
-    cudaFree(col);
-    cudaFree(val);
-    cudaFree(xsq[0]);
-    cudaFree(xsq[1]);
+    if (block && !block_async) cudaFree(block);
     cudaFree(Xs);
     cudaFree(xinv);
+}
+
+void DeviceRows::release_async(cudaStream_t s)
+{
+    if (block) {
+        if (block_async) cudaFreeAsync(block, s);
+        else cudaFree(block);
+    }
+    block = nullptr;
+    X = nullptr; rowptr = nullptr; col = nullptr; val = nullptr;
+    xsq[0] = xsq[1] = nullptr;
 }
 
 int DeviceRows::prepare_form(int form, cudaStream_t s)
@@ -189,7 +195,7 @@ DevX DeviceRows::view(int form) const
 }
 
 int upload_csr(const long long *rowptr, const int *col, const float *val, int n, int d, DeviceRows &out,
-               int force, cudaStream_t s)
+               int force, cudaStream_t s, bool async_alloc)
 {
     out.n = n;
     out.d = d > 0 ? d : 1;
@@ -203,11 +209,28 @@ int upload_csr(const long long *rowptr, const int *col, const float *val, int n,
     bool dense = force == 1 || (force < 0 && dense_bytes <= 1.2 * csr_bytes);
     if (dense && dense_bytes > 60e9) dense = false;
     out.dense = dense;
-    // the CSR arrays always travel; dense rows are scattered on the device
+    // the CSR arrays always travel; dense rows are scattered on the device.
+    // One device block holds [rowptr][col][val][dense rows][norms x 2].
     out.nnz = nnz;
-    CK(cudaMalloc(&out.rowptr, (size_t)(n + 1) * sizeof(long long)));
-    CK(cudaMalloc(&out.col, (size_t)std::max<long long>(nnz, 1) * sizeof(int)));
-    CK(cudaMalloc(&out.val, (size_t)std::max<long long>(nnz, 1) * sizeof(float)));
+    auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
+    const size_t b_rp = 0;
+    const size_t b_col = al(b_rp + (size_t)(n + 1) * sizeof(long long));
+    const size_t b_val = al(b_col + (size_t)std::max<long long>(nnz, 1) * sizeof(int));
+    const size_t b_X = al(b_val + (size_t)std::max<long long>(nnz, 1) * sizeof(float));
+    const size_t b_sq = al(b_X + (dense ? std::max<size_t>((size_t)n * out.ld, 4) * sizeof(float) : 0));
+    const size_t b_end = b_sq + 2 * al((size_t)std::max(n, 1) * sizeof(double));
+    char *blk = nullptr;
+    if (async_alloc) CK(cudaMallocAsync((void **)&blk, b_end, s));
+    else CK(cudaMalloc((void **)&blk, b_end));
+    out.block = blk;
+    out.block_async = async_alloc;
+    out.block_bytes = b_end;
+    out.rowptr = (long long *)(blk + b_rp);
+    out.col = (int *)(blk + b_col);
+    out.val = (float *)(blk + b_val);
+    out.X = dense ? (float *)(blk + b_X) : nullptr;
+    out.xsq[0] = (double *)(blk + b_sq);
+    out.xsq[1] = (double *)(blk + b_sq + al((size_t)std::max(n, 1) * sizeof(double)));
     CK(xfer_async(out.rowptr, rowptr, (size_t)(n + 1) * sizeof(long long), cudaMemcpyHostToDevice, s));
     if (nnz) {
         CK(xfer_async(out.col, col, (size_t)nnz * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -216,7 +239,6 @@ int upload_csr(const long long *rowptr, const int *col, const float *val, int n,
     out.h2d_bytes = (size_t)(n + 1) * 8 + (size_t)nnz * 8;
     if (dense) {
         const size_t elems = std::max<size_t>((size_t)n * out.ld, 4);
-        CK(cudaMalloc(&out.X, elems * sizeof(float)));
         CK(cudaMemsetAsync(out.X, 0, elems * sizeof(float), s));
         if (n) {
             CK(launch_scatter_dense(out.rowptr, out.col, out.val, n, out.ld, out.X, s));
@@ -227,13 +249,12 @@ int upload_csr(const long long *rowptr, const int *col, const float *val, int n,
         out.bytes = (size_t)(n + 1) * 8 + (size_t)nnz * 8;
     }
     for (int f = 0; f < 2; f++) {
-        CK(cudaMalloc(&out.xsq[f], (size_t)std::max(n, 1) * sizeof(double)));
         if (n) {
             CK(launch_xsq(out.view(f), n, out.xsq[f], f, s));
             count_launch();
         }
     }
-    CK(cudaStreamSynchronize(s));
+    if (!async_alloc) CK(cudaStreamSynchronize(s));
     return 0;
 }
 
@@ -300,10 +321,7 @@ struct Bump {
 };
 
 // Byte layout of one instance's device state (all offsets 256-aligned).
-struct InstanceLayout {
-    size_t G, Gb, A, P, QD, Al, Y, S, PL, PR, Sc, Out, Sync, Part, Tag, Ep, St, Data, bytes;
-    int sets, ways;
-};
+using InstanceLayout = Wave::Layout;
 
 InstanceLayout instance_layout(int l, int nb, double cache_mb)
 {
@@ -325,6 +343,12 @@ InstanceLayout instance_layout(int l, int nb, double cache_mb)
     L.bytes = (b.off + 255) & ~size_t(255);
     return L;
 }
+
+}  // namespace
+
+size_t instance_bytes(int l, double cache_mb) { return instance_layout(l, 1, cache_mb).bytes; }
+
+namespace {
 
 // Grow-only device arena for solver state: one buffer reused by every launch
 // (allocating and freeing gigabytes of Q-row caches per call costs more than
@@ -363,14 +387,341 @@ void release_arena()
     g_arena_bytes = 0;
 }
 
+// ---------------------------------------------------------------------------
+// waves: the instances of one persistent launch
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kChunkBytes = 3 * 8 + 2 * 4 + 2;     // per position: G, alpha, QD, col, row, y, status
+
+// dynamic shared memory a solver block can use beside its static part
+long long smem_budget()
+{
+    int smem_total = 0, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    if (cudaDeviceGetAttribute(&smem_total, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return -1;
+    return (long long)smem_total - smo_static_smem() - 1024;
+}
+
+// shared-memory staging of one instance's rows: source rows staged in
+// float32 (CUDA-core forms) or the tensor-core operand stages
+struct StagePlan {
+    int stage_cap = 0, stage_lds = 0, tc_n = 0;
+    long long bytes = 0;        // staging + aux area
+    long long chunk_max = 0;    // positions of state one block can hold
+};
+
+StagePlan stage_plan(const DeviceRows &rows, int form, long long budget)
+{
+    StagePlan p;
+    if (is_tc_form(form)) {
+        p.tc_n = kTcMaxN;
+        while (p.tc_n > 16 && (budget - tc_area_bytes(p.tc_n) - kAuxBytes) / kChunkBytes < 1024) p.tc_n /= 2;
+        p.bytes = tc_area_bytes(p.tc_n);
+    } else {
+        if (rows.dense) {
+            p.stage_lds = rows.ld;
+            p.stage_cap = (int)std::min<long long>(kSrcBatch, (48LL << 10) / ((long long)std::max(rows.ld, 4) * 4));
+        } else {
+            p.stage_lds = rows.d;
+            p.stage_cap = (int)std::min<long long>(kSrcBatch, (budget / 2) / ((long long)std::max(rows.d, 1) * 4));
+        }
+        if (p.stage_cap < 2) p.stage_cap = 0;
+        p.bytes = (((long long)p.stage_cap * p.stage_lds * 4) + 15) & ~15LL;
+    }
+    p.bytes += kAuxBytes;   // transpose tiles / prefetch candidates / block-product partial sums
+    p.chunk_max = (budget - p.bytes) / kChunkBytes;
+    return p;
+}
+
+const SolveParams &params_of(const SubProblem &sp, const SolveParams &prm) { return sp.own ? *sp.own : prm; }
+const DeviceRows &rows_of(const SubProblem &sp, const DeviceRows &rows) { return sp.rows_dev ? *sp.rows_dev : rows; }
+
+}  // namespace
+
+int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, int first,
+              int capacity, Wave &w)
+{
+    const int ninst = (int)subs.size();
+    w = Wave();
+    w.first = first;
+    w.form = prm.form;
+    const long long budget = smem_budget();
+    if (budget <= 0) {
+        set_error("cannot query the device's shared memory");
+        return -1;
+    }
+    const int sms = device_sm_count();
+    std::vector<StagePlan> sp_all;
+    std::vector<long long> nmin;
+    long long need = 0;
+    int last = first;
+    while (last < ninst) {
+        const SubProblem &sp = subs[last];
+        const SolveParams &p = params_of(sp, prm);
+        if (p.form != prm.form) {
+            set_error("instances of one launch must share the arithmetic form");
+            return -1;
+        }
+        const StagePlan st = stage_plan(rows_of(sp, rows), prm.form, budget);
+        if (st.chunk_max < 64) {
+            set_error("not enough shared memory for the solver state");
+            return -1;
+        }
+        const long long l = (long long)sp.rows.size();
+        const long long nm = std::max<long long>(1, (l + st.chunk_max - 1) / st.chunk_max);
+        if (nm > capacity) {
+            if (last == first) {
+                set_error("problem too large: more positions than the device's blocks can hold in shared memory");
+                return -1;
+            }
+            break;
+        }
+        if (need + nm > capacity) break;
+        need += nm;
+        sp_all.push_back(st);
+        nmin.push_back(nm);
+        last++;
+    }
+    const int count = last - first;
+    w.count = count;
+    w.nb.assign(count, 1);
+    // blocks per instance: enough to hold the state in shared memory, more for
+    // large problems; instances that run together share the device by l^2
+    // (the expected work: rows evaluated x row length), so that the largest
+    // instances, which bound the launch, get the most blocks
+    double total_w = 0;
+    for (int k = 0; k < count; k++) {
+        const double l = (double)subs[first + k].rows.size();
+        total_w += l * l;
+    }
+    for (int k = 0; k < count; k++) {
+        const SubProblem &sp = subs[first + k];
+        const long long l = (long long)sp.rows.size();
+        const int bo = params_of(sp, prm).blocks_override;
+        int want;
+        if (bo > 0) want = bo;
+        else want = (int)std::max<long long>(1, std::min<long long>(sms, (l + 499) / 500));
+        if (count > 1) {
+            const long long share = (long long)std::floor((double)capacity * (double)l * (double)l / std::max(total_w, 1.0));
+            want = (int)std::min<long long>(want, std::max<long long>(1, share));
+        }
+        want = (int)std::min<long long>(want, std::max<long long>(1, l));
+        want = std::min(want, std::min(kThreads, kMaxGroupBlocks));
+        w.nb[k] = std::max<int>(want, (int)nmin[k]);
+    }
+    int used = 0;
+    for (int v : w.nb) used += v;
+    while (used > capacity) {
+        // trim the instance with the most blocks above its minimum
+        int big = -1;
+        long long slack = 0;
+        for (int k = 0; k < count; k++)
+            if (w.nb[k] - nmin[k] > slack) { slack = w.nb[k] - nmin[k]; big = k; }
+        if (big < 0) break;
+        w.nb[big]--;
+        used--;
+    }
+    w.used = used;
+    w.stage.resize(count);
+    long long dyn = 0;
+    for (int k = 0; k < count; k++) {
+        const long long l = (long long)subs[first + k].rows.size();
+        const long long cap = (l + w.nb[k] - 1) / w.nb[k];
+        w.stage[k][0] = sp_all[k].stage_cap;
+        w.stage[k][1] = sp_all[k].stage_lds;
+        w.stage[k][2] = sp_all[k].tc_n;
+        w.stage[k][3] = (int)cap;
+        dyn = std::max(dyn, sp_all[k].bytes + cap * kChunkBytes);
+    }
+    w.dyn_smem = (size_t)dyn;
+
+    // One device block per wave, laid out so that the host touches it with
+    // one upload, three fills and two downloads:
+    //   upload   [descriptors][block map][alpha][p][row ids][labels]
+    //   download [outputs][alpha by local index]
+    //   zero     [group syncs][exchange records][cache epochs][cache stamps]
+    //   0xff     [cache tags]
+    //   per instance: G, G_bar, QD, status, position->local, shrink lists, Q rows
+    auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
+    w.loff.assign(count + 1, 0);
+    w.poff.assign(count + 1, 0);
+    w.coff.assign(count + 1, 0);
+    w.lay.resize(count);
+    for (int k = 0; k < count; k++) {
+        const SubProblem &sp = subs[first + k];
+        const int l = (int)sp.rows.size();
+        w.lay[k] = instance_layout(l, w.nb[k], params_of(sp, prm).cache_mb);
+        w.loff[k + 1] = w.loff[k] + (size_t)l;
+        w.poff[k + 1] = w.poff[k] + 2 * (size_t)w.nb[k];
+        w.coff[k + 1] = w.coff[k] + (size_t)w.lay[k].sets * w.lay[k].ways;
+    }
+    const size_t L = w.loff[count], P = w.poff[count], S = w.coff[count];
+    size_t off = 0;
+    w.o_desc = off; off = al(off + sizeof(InstanceDesc) * count);
+    w.o_bmap = off; off = al(off + sizeof(int) * used);
+    w.o_alpha = off; off = al(off + 8 * L);
+    w.o_p = off; off = al(off + 8 * L);
+    w.o_row = off; off = al(off + 4 * L);
+    w.o_y = off; off = al(off + L);
+    w.up_bytes = off;
+    w.o_out = off; off = al(off + sizeof(SolveOut) * count);
+    w.o_alocal = off; off = al(off + 8 * L);
+    w.down_bytes = off - w.o_out;
+    w.o_zero = off;
+    w.o_sync = off; off = al(off + sizeof(GroupSync) * count);
+    w.o_part = off; off = al(off + sizeof(Partial) * P);
+    w.o_ep = off; off = al(off + 4 * S);
+    w.o_st = off; off = al(off + 8 * S);
+    w.zero_bytes = off - w.o_zero;
+    w.o_tag = off; off = al(off + 4 * S);
+    w.tag_bytes = 4 * S;
+    w.inst_off.resize(count);
+    for (int k = 0; k < count; k++) {
+        w.inst_off[k] = off;
+        off += w.lay[k].bytes;
+    }
+    w.dev_bytes = off;
+    return 0;
+}
+
+int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, Wave &w,
+               char *dev, char *host, cudaStream_t s)
+{
+    const int count = w.count, first = w.first;
+    w.dev = dev;
+    w.host = host;
+    w.stream = s;
+    InstanceDesc *h_desc = (InstanceDesc *)(host + w.o_desc);
+    int *h_bmap = (int *)(host + w.o_bmap);
+    double *h_alpha = (double *)(host + w.o_alpha);
+    double *h_p = (double *)(host + w.o_p);
+    int *h_row = (int *)(host + w.o_row);
+    signed char *h_y = (signed char *)(host + w.o_y);
+    InstanceDesc *d_desc = (InstanceDesc *)(dev + w.o_desc);
+    int *d_block_inst = (int *)(dev + w.o_bmap);
+    int b0 = 0;
+    for (int k = 0; k < count; k++) {
+        const SubProblem &sp = subs[first + k];
+        const SolveParams &p = params_of(sp, prm);
+        const DeviceRows &r = rows_of(sp, rows);
+        const int l = (int)sp.rows.size();
+        InstanceDesc &D = h_desc[k];
+        memset(&D, 0, sizeof(D));
+        D.l = l;
+        D.nu = sp.nu;
+        D.shrinking = p.shrinking;
+        D.form = prm.form;
+        D.Cp = sp.Cp;
+        D.Cn = sp.Cn;
+        D.eps = p.eps;
+        D.max_iter = std::max<long long>(10000000LL, l > INT_MAX / 100 ? (long long)INT_MAX : 100LL * l);
+        D.kp = p.kp;
+        D.x = r.view(prm.form);
+        D.block0 = b0;
+        D.nblocks = w.nb[k];
+        D.stage_cap = w.stage[k][0];
+        D.stage_lds = w.stage[k][1];
+        D.tc_n = w.stage[k][2];
+        D.chunk_cap = w.stage[k][3];
+        {
+            const int limit = D.stage_cap > 0 ? std::min(kPrefetchMax, D.stage_cap) : kPrefetchMax;
+            D.prefetch = p.prefetch > 0 ? std::min(p.prefetch, limit) : limit;
+            D.lazy_gbar = p.lazy_gbar < 0 ? (is_tc_form(prm.form) ? 1 : 0) : p.lazy_gbar;
+        }
+        for (int b = 0; b < w.nb[k]; b++) h_bmap[b0 + b] = k;
+        b0 += w.nb[k];
+        const InstanceLayout &Lk = w.lay[k];
+        char *base = dev + w.inst_off[k];
+        D.G = (double *)(base + Lk.G);
+        D.G_bar = (double *)(base + Lk.Gb);
+        D.QD = (double *)(base + Lk.QD);
+        D.status = (unsigned char *)(base + Lk.S);
+        D.pos_local = (int *)(base + Lk.PL);
+        D.scratch = (int *)(base + Lk.Sc);
+        D.cache.data = (float *)(base + Lk.Data);
+        // initial state lives in the shared regions (positions start as local indices)
+        D.alpha = (double *)(dev + w.o_alpha) + w.loff[k];
+        D.p = (double *)(dev + w.o_p) + w.loff[k];
+        D.pos_row = (int *)(dev + w.o_row) + w.loff[k];
+        D.y = (signed char *)(dev + w.o_y) + w.loff[k];
+        D.out = (SolveOut *)(dev + w.o_out) + k;
+        D.alpha_local = (double *)(dev + w.o_alocal) + w.loff[k];
+        D.sync = (GroupSync *)(dev + w.o_sync) + k;
+        D.partials = (Partial *)(dev + w.o_part) + w.poff[k];
+        D.cache.tag = (int *)(dev + w.o_tag) + w.coff[k];
+        D.cache.epoch = (int *)(dev + w.o_ep) + w.coff[k];
+        D.cache.stamp = (unsigned long long *)(dev + w.o_st) + w.coff[k];
+        D.cache.nsets = Lk.sets;
+        D.cache.nways = Lk.ways;
+        D.cache.stride = l;
+        memcpy(h_alpha + w.loff[k], sp.alpha0.data(), sizeof(double) * l);
+        memcpy(h_p + w.loff[k], sp.p.data(), sizeof(double) * l);
+        memcpy(h_row + w.loff[k], sp.rows.data(), sizeof(int) * l);
+        memcpy(h_y + w.loff[k], sp.y.data(), (size_t)l);
+    }
+    CK(xfer_async(dev, host, w.up_bytes, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(dev + w.o_zero, 0, w.zero_bytes, s));
+    CK(cudaMemsetAsync(dev + w.o_tag, 0xff, w.tag_bytes, s));
+    CK(cudaEventCreate(&w.ev0));
+    CK(cudaEventCreate(&w.ev1));
+    CK(cudaEventRecord(w.ev0, s));
+    cudaError_t le = launch_smo(w.form, d_desc, d_block_inst, w.used, w.dyn_smem, w.cooperative, s);
+    if (le == cudaSuccess) count_launch();
+    cudaEventRecord(w.ev1, s);
+    if (le == cudaSuccess) le = xfer_async(host + w.up_bytes, dev + w.o_out, w.down_bytes, cudaMemcpyDeviceToHost, s);
+    if (le != cudaSuccess) {
+        set_error(std::string("solver launch failed: ") + cudaGetErrorString(le));
+        return -1;
+    }
+    CK(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming));
+    CK(cudaEventRecord(w.done, s));
+    return 0;
+}
+
+bool wave_ready(const Wave &w) { return w.done && cudaEventQuery(w.done) != cudaErrorNotReady; }
+
+int wave_finish(Wave &w, std::vector<SolveResult> &res)
+{
+    cudaError_t se = w.done ? cudaEventSynchronize(w.done) : cudaErrorInvalidResourceHandle;
+    float ms = 0;
+    if (se == cudaSuccess) se = cudaEventElapsedTime(&ms, w.ev0, w.ev1);
+    if (w.ev0) cudaEventDestroy(w.ev0);
+    if (w.ev1) cudaEventDestroy(w.ev1);
+    if (w.done) cudaEventDestroy(w.done);
+    w.ev0 = w.ev1 = w.done = nullptr;
+    if (se != cudaSuccess) {
+        set_error(std::string("solver launch failed: ") + cudaGetErrorString(se));
+        return -1;
+    }
+    w.ms = ms;
+    const SolveOut *h_out = (const SolveOut *)(w.host + w.up_bytes);
+    const double *h_alocal = (const double *)(w.host + w.up_bytes + (w.o_alocal - w.o_out));
+    int rc = 0;
+    for (int k = 0; k < w.count; k++) {
+        SolveResult &R = res[w.first + k];
+        const size_t l = w.loff[k + 1] - w.loff[k];
+        R.alpha.assign(h_alocal + w.loff[k], h_alocal + w.loff[k] + l);
+        R.out = h_out[k];
+        R.seconds = ms * 1e-3;
+        if (R.out.status < 0) {
+            set_error("solver group barrier timed out");
+            rc = -1;
+        }
+    }
+    return rc;
+}
+
 int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm,
                 std::vector<SolveResult> &res, cudaStream_t s)
 {
     const int ninst = (int)subs.size();
     res.assign(ninst, SolveResult());
     if (ninst == 0) return 0;
-    // the split bf16 copy of the rows is a derived cache of the rows, built on first use
+    // the split copy of the rows is a derived cache of the rows, built on first use
     if (const_cast<DeviceRows &>(rows).prepare_form(prm.form, s) != 0) return -1;
+    for (const SubProblem &sp : subs)
+        if (sp.rows_dev && const_cast<DeviceRows *>(sp.rows_dev)->prepare_form(prm.form, s) != 0) return -1;
     std::lock_guard<std::mutex> arena_lock(g_arena_mu);
     StageClock clk;
     const int sms = device_sm_count();
@@ -378,284 +729,38 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         set_error("no CUDA device");
         return -1;
     }
-    // Shared memory of a block: [source staging][chunk state, kChunkBytes per position].
-    constexpr int kChunkBytes = 3 * 8 + 2 * 4 + 2;     // G, alpha, QD, col, row, y, status
-    int smem_total = 0, dev = 0;
-    CK(cudaGetDevice(&dev));
-    CK(cudaDeviceGetAttribute(&smem_total, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const long long budget = (long long)smem_total - smo_static_smem() - 1024;
-    int stage_cap, stage_lds;
-    if (rows.dense) {
-        stage_lds = rows.ld;
-        stage_cap = (int)std::min<long long>(kSrcBatch, (48LL << 10) / ((long long)rows.ld * 4));
-    } else {
-        stage_lds = rows.d;
-        stage_cap = (int)std::min<long long>(kSrcBatch, (budget / 2) / ((long long)std::max(rows.d, 1) * 4));
-    }
-    if (stage_cap < 2) stage_cap = 0;
-    int tc_n = 0;
-    long long stage_bytes;
-    if (is_tc_form(prm.form)) {
-        // tensor form: the operand stages of the tensor-core pipeline replace the
-        // source staging; as many sources per block-product pass as leave room for
-        // a useful chunk of state
-        stage_cap = 0;
-        tc_n = kTcMaxN;
-        while (tc_n > 16 && (budget - tc_area_bytes(tc_n) - kAuxBytes) / kChunkBytes < 1024) tc_n /= 2;
-        stage_bytes = tc_area_bytes(tc_n);
-    } else {
-        stage_bytes = (((long long)stage_cap * stage_lds * 4) + 15) & ~15LL;
-    }
-    stage_bytes += kAuxBytes;   // transpose tiles / prefetch candidates
-    const long long chunk_max = (budget - stage_bytes) / kChunkBytes;
-    if (chunk_max < 64) {
-        set_error("not enough shared memory for the solver state");
-        return -1;
-    }
-    const size_t max_dyn = (size_t)(stage_bytes + chunk_max * kChunkBytes);
+    // co-resident capacity of the persistent kernel at the largest shared memory it may use
+    const long long budget = smem_budget();
     int per_sm = 0;
-    CK(smo_max_blocks(prm.form, max_dyn, &per_sm));
+    CK(smo_max_blocks(prm.form, (size_t)std::max<long long>(budget, 0), &per_sm));
     if (per_sm < 1) {
         set_error("solver kernel does not fit on an SM");
         return -1;
     }
     const int capacity = per_sm * sms;
     clk.mark("setup");
-    for (const SubProblem &sp : subs)
-        if ((long long)sp.rows.size() > chunk_max * capacity) {
-            set_error("problem too large: more positions than the device's blocks can hold in shared memory");
-            return -1;
-        }
-
-    // process instances in waves that fit the co-resident capacity
     int first = 0;
     while (first < ninst) {
-        // blocks per instance: enough to hold the state in shared memory, more
-        // for large problems, shared proportionally when instances run together
-        std::vector<int> nb;
-        long long total_l = 0, need = 0;
-        int last = first;
-        while (last < ninst) {
-            const long long l = (long long)subs[last].rows.size();
-            const long long nmin = std::max<long long>(1, (l + chunk_max - 1) / chunk_max);
-            if (need + nmin > capacity) break;
-            need += nmin;
-            total_l += l;
-            last++;
-        }
-        const int count = last - first;
-        nb.assign(count, 1);
-        // expected work of an instance grows like l^2 (rows evaluated x row length):
-        // share the device by l^2 so that the largest instances, which bound the
-        // launch, get the most blocks
-        double total_w = 0;
-        for (int k = 0; k < count; k++) {
-            const double l = (double)subs[first + k].rows.size();
-            total_w += l * l;
-        }
-        for (int k = 0; k < count; k++) {
-            const long long l = (long long)subs[first + k].rows.size();
-            const int nmin = (int)std::max<long long>(1, (l + chunk_max - 1) / chunk_max);
-            int want;
-            if (prm.blocks_override > 0) want = prm.blocks_override;
-            else want = (int)std::max<long long>(1, std::min<long long>(sms, (l + 499) / 500));
-            if (count > 1) {
-                const long long share = (long long)std::floor((double)capacity * (double)l * (double)l / std::max(total_w, 1.0));
-                want = (int)std::min<long long>(want, std::max<long long>(1, share));
-            }
-            want = (int)std::min<long long>(want, std::max<long long>(1, l));
-            want = std::min(want, kThreads);
-            nb[k] = std::max(want, nmin);
-        }
-        (void)total_l;
-        int used = 0;
-        for (int v : nb) used += v;
-        while (used > capacity) {
-            // trim the instance with the most blocks above its minimum
-            int big = -1;
-            long long slack = 0;
-            for (int k = 0; k < count; k++) {
-                const long long l = (long long)subs[first + k].rows.size();
-                const long long nmin = std::max<long long>(1, (l + chunk_max - 1) / chunk_max);
-                if (nb[k] - nmin > slack) { slack = nb[k] - nmin; big = k; }
-            }
-            if (big < 0) break;
-            nb[big]--;
-            used--;
-        }
-        long long chunk_cap = 1;
-        for (int k = 0; k < count; k++) {
-            const long long l = (long long)subs[first + k].rows.size();
-            chunk_cap = std::max<long long>(chunk_cap, (l + nb[k] - 1) / nb[k]);
-        }
-        const size_t dyn_smem = (size_t)(stage_bytes + chunk_cap * kChunkBytes);
-
-        // One arena block per wave, laid out so that the host touches it with
-        // one upload, three fills and two downloads:
-        //   upload   [descriptors][block map][alpha][p][row ids][labels]
-        //   download [outputs][alpha by local index]
-        //   zero     [group syncs][exchange records][cache epochs][cache stamps]
-        //   0xff     [cache tags]
-        //   per instance: G, G_bar, QD, status, position->local, shrink lists, Q rows
-        auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
-        std::vector<size_t> loff(count + 1, 0), poff(count + 1, 0), coff(count + 1, 0);
-        std::vector<InstanceLayout> lay(count);
-        for (int k = 0; k < count; k++) {
-            const int l = (int)subs[first + k].rows.size();
-            lay[k] = instance_layout(l, nb[k], prm.cache_mb);
-            loff[k + 1] = loff[k] + (size_t)l;
-            poff[k + 1] = poff[k] + 2 * (size_t)nb[k];
-            coff[k + 1] = coff[k] + (size_t)lay[k].sets * lay[k].ways;
-        }
-        const size_t L = loff[count], P = poff[count], S = coff[count];
-        size_t off = 0;
-        const size_t o_desc = off; off = al(off + sizeof(InstanceDesc) * count);
-        const size_t o_bmap = off; off = al(off + sizeof(int) * used);
-        const size_t o_alpha = off; off = al(off + 8 * L);
-        const size_t o_p = off; off = al(off + 8 * L);
-        const size_t o_row = off; off = al(off + 4 * L);
-        const size_t o_y = off; off = al(off + L);
-        const size_t up_bytes = off;
-        const size_t o_out = off; off = al(off + sizeof(SolveOut) * count);
-        const size_t o_alocal = off; off = al(off + 8 * L);
-        const size_t down_bytes = off - o_out;
-        const size_t o_zero = off;
-        const size_t o_sync = off; off = al(off + sizeof(GroupSync) * count);
-        const size_t o_part = off; off = al(off + sizeof(Partial) * P);
-        const size_t o_ep = off; off = al(off + 4 * S);
-        const size_t o_st = off; off = al(off + 8 * S);
-        const size_t zero_bytes = off - o_zero;
-        const size_t o_tag = off; off = al(off + 4 * S);
-        std::vector<size_t> inst_off(count);
-        for (int k = 0; k < count; k++) {
-            inst_off[k] = off;
-            off += lay[k].bytes;
-        }
+        Wave w;
+        if (wave_plan(rows, subs, prm, first, capacity, w) != 0) return -1;
         clk.mark("plan");
-        char *arena = arena_reserve(off);
-        clk.mark("arena");
+        char *arena = arena_reserve(w.dev_bytes);
         if (!arena) {
-            set_error("device allocation for solver state failed (" + std::to_string(off >> 20) + " MiB)");
+            set_error("device allocation for solver state failed (" + std::to_string(w.dev_bytes >> 20) + " MiB)");
             return -1;
         }
-        // host side of the upload region, in page-locked memory
-        char *host = nullptr;
+        char *host = (char *)pinned_staging_slot(1, w.up_bytes + w.down_bytes);
         std::vector<char> host_fallback;
-        {
-            host = (char *)pinned_staging_slot(1, up_bytes + down_bytes);
-            if (!host) {
-                host_fallback.resize(up_bytes + down_bytes);
-                host = host_fallback.data();
-            }
+        if (!host) {
+            host_fallback.resize(w.up_bytes + w.down_bytes);
+            host = host_fallback.data();
         }
-        InstanceDesc *h_desc = (InstanceDesc *)(host + o_desc);
-        int *h_bmap = (int *)(host + o_bmap);
-        double *h_alpha = (double *)(host + o_alpha);
-        double *h_p = (double *)(host + o_p);
-        int *h_row = (int *)(host + o_row);
-        signed char *h_y = (signed char *)(host + o_y);
-        InstanceDesc *d_desc = (InstanceDesc *)(arena + o_desc);
-        int *d_block_inst = (int *)(arena + o_bmap);
-        std::vector<InstanceDesc> desc(count);
-        int b0 = 0;
-        for (int k = 0; k < count; k++) {
-            const SubProblem &sp = subs[first + k];
-            const int l = (int)sp.rows.size();
-            InstanceDesc &D = desc[k];
-            memset(&D, 0, sizeof(D));
-            D.l = l;
-            D.nu = sp.nu;
-            D.shrinking = prm.shrinking;
-            D.form = prm.form;
-            D.Cp = sp.Cp;
-            D.Cn = sp.Cn;
-            D.eps = prm.eps;
-            D.max_iter = std::max<long long>(10000000LL, l > INT_MAX / 100 ? (long long)INT_MAX : 100LL * l);
-            D.kp = prm.kp;
-            D.x = rows.view(prm.form);
-            D.block0 = b0;
-            D.nblocks = nb[k];
-            D.stage_cap = stage_cap;
-            D.stage_lds = stage_lds;
-            D.chunk_cap = (int)chunk_cap;
-            {
-                const int limit = stage_cap > 0 ? std::min(kPrefetchMax, stage_cap) : kPrefetchMax;
-                D.prefetch = prm.prefetch > 0 ? std::min(prm.prefetch, limit) : limit;
-                D.lazy_gbar = prm.lazy_gbar < 0 ? (is_tc_form(prm.form) ? 1 : 0) : prm.lazy_gbar;
-                D.tc_n = tc_n;
-            }
-            for (int b = 0; b < nb[k]; b++) h_bmap[b0 + b] = k;
-            b0 += nb[k];
-            const InstanceLayout &Lk = lay[k];
-            char *base = arena + inst_off[k];
-            D.G = (double *)(base + Lk.G);
-            D.G_bar = (double *)(base + Lk.Gb);
-            D.QD = (double *)(base + Lk.QD);
-            D.status = (unsigned char *)(base + Lk.S);
-            D.pos_local = (int *)(base + Lk.PL);
-            D.scratch = (int *)(base + Lk.Sc);
-            D.cache.data = (float *)(base + Lk.Data);
-            // initial state lives in the shared regions (positions start as local indices)
-            D.alpha = (double *)(arena + o_alpha) + loff[k];
-            D.p = (double *)(arena + o_p) + loff[k];
-            D.pos_row = (int *)(arena + o_row) + loff[k];
-            D.y = (signed char *)(arena + o_y) + loff[k];
-            D.out = (SolveOut *)(arena + o_out) + k;
-            D.alpha_local = (double *)(arena + o_alocal) + loff[k];
-            D.sync = (GroupSync *)(arena + o_sync) + k;
-            D.partials = (Partial *)(arena + o_part) + poff[k];
-            D.cache.tag = (int *)(arena + o_tag) + coff[k];
-            D.cache.epoch = (int *)(arena + o_ep) + coff[k];
-            D.cache.stamp = (unsigned long long *)(arena + o_st) + coff[k];
-            D.cache.nsets = Lk.sets;
-            D.cache.nways = Lk.ways;
-            D.cache.stride = l;
-            memcpy(h_alpha + loff[k], sp.alpha0.data(), sizeof(double) * l);
-            memcpy(h_p + loff[k], sp.p.data(), sizeof(double) * l);
-            memcpy(h_row + loff[k], sp.rows.data(), sizeof(int) * l);
-            memcpy(h_y + loff[k], sp.y.data(), (size_t)l);
-        }
-        memcpy(h_desc, desc.data(), sizeof(InstanceDesc) * count);
-        clk.mark("pack");
-        CK(xfer_async(arena, host, up_bytes, cudaMemcpyHostToDevice, s));
-        CK(cudaMemsetAsync(arena + o_zero, 0, zero_bytes, s));
-        CK(cudaMemsetAsync(arena + o_tag, 0xff, 4 * S, s));
-        cudaEvent_t ev0, ev1;
-        CK(cudaEventCreate(&ev0));
-        CK(cudaEventCreate(&ev1));
-        CK(cudaEventRecord(ev0, s));
-        cudaError_t le = launch_smo(prm.form, d_desc, d_block_inst, used, dyn_smem, true, s);
-        if (le == cudaSuccess) count_launch();
-        cudaEventRecord(ev1, s);
-        if (le == cudaSuccess) le = xfer_async(host + up_bytes, arena + o_out, down_bytes, cudaMemcpyDeviceToHost, s);
+        clk.mark("arena");
+        if (wave_start(rows, subs, prm, w, arena, host, s) != 0) return -1;
         clk.mark("launch");
-        cudaError_t se = le == cudaSuccess ? cudaStreamSynchronize(s) : le;
-        clk.mark("wait");
-        float ms = 0;
-        if (se == cudaSuccess) cudaEventElapsedTime(&ms, ev0, ev1);
-        cudaEventDestroy(ev0);
-        cudaEventDestroy(ev1);
-        int rc = 0;
-        if (se != cudaSuccess) {
-            set_error(std::string("solver launch failed: ") + cudaGetErrorString(se));
-            rc = -1;
-        }
-        const SolveOut *h_out = (const SolveOut *)(host + up_bytes);
-        const double *h_alocal = (const double *)(host + up_bytes + (o_alocal - o_out));
-        for (int k = 0; k < count && rc == 0; k++) {
-            SolveResult &R = res[first + k];
-            const int l = desc[k].l;
-            R.alpha.assign(h_alocal + loff[k], h_alocal + loff[k] + l);
-            R.out = h_out[k];
-            R.seconds = ms * 1e-3;
-            if (R.out.status < 0) {
-                set_error("solver group barrier timed out");
-                rc = -1;
-            }
-        }
-        clk.mark("unpack");
-        if (rc) return rc;
-        first = last;
+        if (wave_finish(w, res) != 0) return -1;
+        clk.mark("finish");
+        first += w.count;
     }
     return 0;
 }

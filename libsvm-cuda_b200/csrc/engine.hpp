@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <string>
 #include <vector>
 
@@ -33,7 +34,11 @@ struct DeviceRows {
     int nchunk = 0;
     size_t bytes = 0;          // device bytes of the layout the solver reads
     size_t h2d_bytes = 0;      // bytes copied from the host by the upload
+    char *block = nullptr;     // one device block holding the rows and norms
+    bool block_async = false;  // allocated stream-ordered (freed with release_async)
+    size_t block_bytes = 0;
     ~DeviceRows();
+    void release_async(cudaStream_t s);
     DevX view(int form) const;
     // build Xs if the form needs it; -1 (error set) when the rows cannot take the form
     int prepare_form(int form, cudaStream_t s);
@@ -43,8 +48,14 @@ struct DeviceRows {
 // force: -1 auto, 0 CSR, 1 dense.
 int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cudaStream_t s);
 // Upload rows given as host CSR arrays (0-based columns).
+// With async_alloc the device block comes from the stream-ordered allocator
+// and the call does not wait for the upload (later work on s is ordered after it).
 int upload_csr(const long long *rowptr, const int *col, const float *val, int n, int d, DeviceRows &out,
-               int force, cudaStream_t s);
+               int force, cudaStream_t s, bool async_alloc = false);
+// device bytes of one instance's solver state (gradient, status, shrink lists, Q-row cache)
+size_t instance_bytes(int l, double cache_mb);
+
+struct SolveParams;
 
 struct SubProblem {
     std::vector<int> rows;          // row id in DeviceRows per local variable
@@ -53,6 +64,8 @@ struct SubProblem {
     std::vector<double> p;          // linear term
     double Cp = 1, Cn = 1;
     int nu = 0;                     // Solver_NU
+    const DeviceRows *rows_dev = nullptr;   // the instance's own rows (nullptr: the launch's rows)
+    const SolveParams *own = nullptr;       // the instance's own parameters (nullptr: the launch's)
 };
 
 struct SolveParams {
@@ -71,6 +84,38 @@ struct SolveResult {
     SolveOut out{};
     double seconds = 0;
 };
+
+// The instances of one persistent launch ("wave"): block counts, shared
+// memory, and the layout of the launch's device block and host staging.
+struct Wave {
+    int first = 0, count = 0, used = 0, form = 0;
+    std::vector<int> nb;                      // blocks per instance
+    std::vector<std::array<int, 4>> stage;    // stage_cap, stage_lds, tc_n, chunk_cap per instance
+    size_t dyn_smem = 0;
+    struct Layout { size_t G, Gb, A, P, QD, Al, Y, S, PL, PR, Sc, Out, Sync, Part, Tag, Ep, St, Data, bytes; int sets, ways; };
+    std::vector<Layout> lay;
+    std::vector<size_t> loff, poff, coff, inst_off;
+    size_t o_desc = 0, o_bmap = 0, o_alpha = 0, o_p = 0, o_row = 0, o_y = 0, o_out = 0, o_alocal = 0;
+    size_t o_zero = 0, o_sync = 0, o_part = 0, o_ep = 0, o_st = 0, o_tag = 0;
+    size_t up_bytes = 0, down_bytes = 0, zero_bytes = 0, tag_bytes = 0, dev_bytes = 0;
+    char *dev = nullptr, *host = nullptr;
+    cudaStream_t stream = nullptr;
+    bool cooperative = true;   // false: plain launch (the caller guarantees the blocks are co-resident)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
+    float ms = 0;
+};
+
+// Plan the wave that starts at instance `first` within `capacity` co-resident
+// blocks (as many instances as fit).  Needs w.dev_bytes of device memory and
+// w.up_bytes + w.down_bytes of (preferably page-locked) host staging.
+int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, int first,
+              int capacity, Wave &w);
+// Upload, launch and queue the result download on stream s (asynchronous).
+int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, Wave &w,
+               char *dev, char *host, cudaStream_t s);
+bool wave_ready(const Wave &w);
+// Wait for the wave and unpack results[first .. first+count).
+int wave_finish(Wave &w, std::vector<SolveResult> &res);
 
 // Solve every subproblem in one persistent launch (instances get disjoint
 // groups of blocks).  Returns 0 on success.

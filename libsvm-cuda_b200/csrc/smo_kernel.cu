@@ -2175,6 +2175,17 @@ cudaError_t launch_scatter_dense(const long long *rowptr, const int *col, const 
     return cudaGetLastError();
 }
 
+static cudaError_t set_max_dyn_smem(const void *fn)
+{
+    int dev = 0, optin = 0;
+    cudaFuncAttributes a;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, fn);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes);
+    return e;
+}
+
 static const void *smo_fn(int form)
 {
     if (form == FORM_EXACT) return (const void *)smo_persistent<FORM_EXACT>;
@@ -2188,8 +2199,11 @@ cudaError_t launch_smo(int form, const InstanceDesc *d_insts, const int *d_block
 {
     void *args[] = {(void *)&d_insts, (void *)&d_block_inst};
     const void *fn = smo_fn(form);
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
+    // the attribute is set to the largest size any launch may use (the same
+    // value from every thread), never lowered to one launch's need
+    cudaError_t e = set_max_dyn_smem(fn);
     if (e != cudaSuccess) return e;
+    (void)dyn_smem;
     if (cooperative)
         return cudaLaunchCooperativeKernel(fn, dim3(nblocks), dim3(kThreads), args, dyn_smem, s);
     return cudaLaunchKernel(fn, dim3(nblocks), dim3(kThreads), args, dyn_smem, s);
@@ -2198,7 +2212,7 @@ cudaError_t launch_smo(int form, const InstanceDesc *d_insts, const int *d_block
 cudaError_t smo_max_blocks(int form, size_t dyn_smem, int *blocks_per_sm)
 {
     const void *fn = smo_fn(form);
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
+    cudaError_t e = set_max_dyn_smem(fn);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, kThreads, dyn_smem);
 }

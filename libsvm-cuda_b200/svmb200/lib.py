@@ -43,6 +43,19 @@ class SvmbParams(C.Structure):
                 ("blocks", C.c_int), ("prefetch", C.c_int), ("gbar_mode", C.c_int)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("mem_bytes", C.c_longlong), ("max_inflight", C.c_int), ("max_batch", C.c_int), ("form", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_longlong), ("failed", C.c_longlong), ("waves", C.c_longlong),
+                ("max_concurrent_waves", C.c_longlong), ("peak_mem_bytes", C.c_longlong), ("pending", C.c_longlong),
+                ("p50_s", C.c_double), ("p99_s", C.c_double), ("max_s", C.c_double), ("solves_per_s", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def make_params(svm_type=0, kernel_type=2, degree=3, gamma=0.0, coef0=0.0, C_pos=1.0, C_neg=None, nu=0.5,
                 eps=1e-3, cache_mb=100.0, shrinking=1, form=FORM_EXACT, blocks=0, prefetch=0,
                 gbar_mode=0) -> SvmbParams:
@@ -93,6 +106,14 @@ def _load(path: str) -> C.CDLL:
     lib.svmb_rows_free.argtypes = [C.c_void_p]
     lib.svmb_rows_kernel_block.argtypes = [C.c_void_p, _P(SvmbParams), C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                            C.c_void_p]
+    lib.svmb_server_create.argtypes = [_P(ServerConfig), _P(C.c_void_p)]
+    lib.svmb_server_submit.restype = C.c_longlong
+    lib.svmb_server_submit.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       _P(SvmbParams)]
+    lib.svmb_server_poll.argtypes = [C.c_void_p, C.c_longlong]
+    lib.svmb_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, _P(SolveStats), _P(C.c_double)]
+    lib.svmb_server_get_stats.argtypes = [C.c_void_p, _P(ServerStats)]
+    lib.svmb_server_destroy.argtypes = [C.c_void_p]
     return lib
 
 
@@ -272,5 +293,57 @@ class ResidentRows:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request loop (svmb_server_*): submitted binary solves are batched
+    continuously onto the GPU; wait(ticket) returns (signed alpha, stats, latency)."""
+
+    def __init__(self, eng: Engine, mem_bytes: int = 0, max_inflight: int = 0, max_batch: int = 0, form: int = 0):
+        self.eng = eng
+        self.h = None
+        cfg = ServerConfig(mem_bytes, max_inflight, max_batch, form)
+        h = C.c_void_p()
+        eng._ok(eng.lib.svmb_server_create(C.byref(cfg), C.byref(h)), "svmb_server_create")
+        self.h = h
+        self._n = {}
+
+    def submit(self, p: CSR, params: SvmbParams, y: Optional[np.ndarray] = None) -> int:
+        rp, col, val = csr_arrays(p)
+        yy = np.ascontiguousarray(p.y if y is None else y, dtype=np.float64)
+        t = self.eng.lib.svmb_server_submit(self.h, p.n, p.d, rp.ctypes.data, col.ctypes.data, val.ctypes.data,
+                                            yy.ctypes.data, C.byref(params))
+        if t < 0:
+            raise EngineError(f"svmb_server_submit: {self.eng.error()}")
+        self._n[t] = p.n
+        return t
+
+    def done(self, ticket: int) -> bool:
+        return self.eng.lib.svmb_server_poll(self.h, ticket) == 1
+
+    def wait(self, ticket: int):
+        n = self._n.pop(ticket)
+        alpha = np.zeros(n)
+        st = SolveStats()
+        lat = C.c_double()
+        self.eng._ok(self.eng.lib.svmb_server_wait(self.h, ticket, alpha.ctypes.data, C.byref(st), C.byref(lat)),
+                     "svmb_server_wait")
+        return alpha, st.as_dict(), lat.value
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        self.eng._ok(self.eng.lib.svmb_server_get_stats(self.h, C.byref(s)), "svmb_server_get_stats")
+        return s.as_dict()
+
+    def close(self):
+        if self.h:
+            self.eng.lib.svmb_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
