@@ -92,12 +92,24 @@ int svmb_device_available(void);                /* 1 if a CUDA device can be use
  *   "form"   SVMB_FORM_EXACT (default) or SVMB_FORM_FP32
  *   "blocks" thread blocks per solve (0 = automatic)
  *   "layout" -1 automatic, 0 CSR, 1 dense device layout of the rows
- *   "prefetch" kernel rows per cache-miss pass (1 = none, 0 = automatic) */
+ *   "prefetch" kernel rows per cache-miss pass (1 = none, 0 = automatic)
+ *   "predict_form" SVMB_FORM_EXACT (default: the reference's kernel values bit
+ *            for bit) or a tensor-core form: svm_predict* and svmb_predict_batch
+ *            then evaluate K(test rows, SVs) as block products on the tensor cores */
 int svmb_set_option(const char *name, long long value);
 
 /* Per-subproblem statistics of the last svm_train / svm_cross_validation
  * call on this process; returns the number of records (copies at most cap). */
 int svmb_last_train_stats(svmb_solve_stats *out, int cap);
+
+/* svm_cross_validation (reference svm.cpp:2407-2525) over a grid of npoints
+ * (C[p], gamma[p]) values in one call: the folds are drawn once with rand(),
+ * exactly as svm_cross_validation draws them, and the one-vs-one subproblems
+ * of every point and fold are solved in batched launches over rows uploaded
+ * once.  target[p*l + i] receives the prediction for row i of the model of
+ * point p trained without i's fold (NaN where that training failed). */
+int svmb_cross_validation_grid(const struct svm_problem *prob, const struct svm_parameter *param, int nr_fold,
+                               int npoints, const double *C, const double *gamma, double *target);
 
 /* Decision values of n rows in one device pass (the batched form of
  * svm_predict_values, reference svm.cpp:2569-2643).  labels[n];
@@ -162,18 +174,23 @@ int svmb_rows_kernel_block(const svmb_rows *rows, const svmb_params *params, int
 
 /* ---- request loop (continuous batching of independent solves) ------------
  * No counterpart in the reference, which trains one problem per call.  A
- * scheduler thread admits requests in arrival order while their device memory
- * (rows + solver state with the Q-row cache budget) fits the server's budget
- * and the thread blocks they need fit the SMs that no running launch holds,
- * and launches them together next to the launches already running (up to
- * max_inflight at a time).  A request's result equals its solve alone. */
+ * scheduler thread picks a leading request (the policy), adds pending
+ * requests of a similar size while their device memory (rows + solver state
+ * with the Q-row cache budget) fits the server's budget and the thread blocks
+ * they need fit the SMs that no running launch holds, and launches them
+ * together next to the launches already running (up to max_inflight at a
+ * time).  A request's result equals its solve alone. */
 typedef struct svmb_server svmb_server;
 typedef struct svmb_server_config {
     long long mem_bytes;     /* device memory for admitted requests; 0 = 80% of the free memory */
-    int max_inflight;        /* concurrent launches; 0 = 4 */
-    int max_batch;           /* requests per launch; 0 = 64 */
+    int max_inflight;        /* concurrent launches; 0 = 8 */
+    int max_batch;           /* requests per launch; 0 = 32 */
     int form;                /* SVMB_FORM_* of every request */
+    int policy;              /* SVMB_SERVE_*: which pending request leads the next launch */
+    int rows_per_block;      /* thread blocks per request = rows / rows_per_block (at least 1); 0 = 2000 */
 } svmb_server_config;
+#define SVMB_SERVE_SMALLEST_FIRST 0  /* the smallest pending request, unless one has waited over 2 s */
+#define SVMB_SERVE_ARRIVAL_ORDER  1  /* the oldest pending request */
 typedef struct svmb_server_stats {
     long long completed, failed, waves, max_concurrent_waves, peak_mem_bytes, pending;
     double p50_s, p99_s, max_s;   /* request latency: submit -> result ready */

@@ -624,6 +624,7 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
         D.stage_lds = w.stage[k][1];
         D.tc_n = w.stage[k][2];
         D.chunk_cap = w.stage[k][3];
+        D.done_flag = w.done_flags ? w.done_flags + k : nullptr;
         {
             const int limit = D.stage_cap > 0 ? std::min(kPrefetchMax, D.stage_cap) : kPrefetchMax;
             D.prefetch = p.prefetch > 0 ? std::min(p.prefetch, limit) : limit;
@@ -680,6 +681,21 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
 }
 
 bool wave_ready(const Wave &w) { return w.done && cudaEventQuery(w.done) != cudaErrorNotReady; }
+
+int wave_fetch(const Wave &w, int k, SolveResult &r, cudaStream_t s)
+{
+    const size_t l = w.loff[k + 1] - w.loff[k];
+    r.alpha.resize(l);
+    CK(xfer_async(&r.out, w.dev + w.o_out + sizeof(SolveOut) * k, sizeof(SolveOut), cudaMemcpyDeviceToHost, s));
+    if (l) CK(xfer_async(r.alpha.data(), w.dev + w.o_alocal + 8 * w.loff[k], 8 * l, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    r.seconds = 0;
+    if (r.out.status < 0) {
+        set_error("solver group barrier timed out");
+        return -1;
+    }
+    return 0;
+}
 
 int wave_finish(Wave &w, std::vector<SolveResult> &res)
 {
@@ -739,10 +755,29 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
     }
     const int capacity = per_sm * sms;
     clk.mark("setup");
+    // More instances than one launch holds: launch them largest first, so that
+    // each launch holds instances of similar size (a launch lasts as long as
+    // its longest solve, and its other SMs idle meanwhile).  Results do not
+    // depend on which instances share a launch.
+    std::vector<SubProblem> sorted_subs;
+    std::vector<int> order;
+    const std::vector<SubProblem> *plan = &subs;
+    if (ninst > capacity) {
+        order.resize(ninst);
+        for (int k = 0; k < ninst; k++) order[k] = k;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return subs[a].rows.size() > subs[b].rows.size(); });
+        sorted_subs.reserve(ninst);
+        for (int k : order) sorted_subs.push_back(subs[k]);
+        plan = &sorted_subs;
+    }
+    std::vector<SolveResult> sorted_res;
+    std::vector<SolveResult> &out = order.empty() ? res : sorted_res;
+    if (!order.empty()) sorted_res.assign(ninst, SolveResult());
     int first = 0;
     while (first < ninst) {
         Wave w;
-        if (wave_plan(rows, subs, prm, first, capacity, w) != 0) return -1;
+        if (wave_plan(rows, *plan, prm, first, capacity, w) != 0) return -1;
         clk.mark("plan");
         char *arena = arena_reserve(w.dev_bytes);
         if (!arena) {
@@ -756,12 +791,13 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
             host = host_fallback.data();
         }
         clk.mark("arena");
-        if (wave_start(rows, subs, prm, w, arena, host, s) != 0) return -1;
+        if (wave_start(rows, *plan, prm, w, arena, host, s) != 0) return -1;
         clk.mark("launch");
-        if (wave_finish(w, res) != 0) return -1;
+        if (wave_finish(w, out) != 0) return -1;
         clk.mark("finish");
         first += w.count;
     }
+    for (size_t i = 0; i < order.size(); i++) res[order[i]] = std::move(sorted_res[i]);
     return 0;
 }
 

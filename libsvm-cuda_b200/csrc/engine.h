@@ -91,7 +91,8 @@ struct GroupSync {
     unsigned int count;
     unsigned int gen;
     int error;                  // nonzero: a wait timed out somewhere in the group
-    int pad[29];
+    unsigned int finished;      // blocks of the group that have written their results
+    int pad[28];
 };
 
 // Cross-block reduction record (one per block per phase).  Besides the
@@ -172,6 +173,7 @@ struct InstanceDesc {
     //    inactive positions as one block product (no full-length rows during the loop)
     int lazy_gbar;
     int tc_n;                   // FORM_BF16X3: sources per tensor-core pass (16, 32 or 64); 0 otherwise
+    int *done_flag;             // host-mapped word set to 1 once the whole instance has written its results, or nullptr
 };
 
 }  // namespace svmb

@@ -101,6 +101,7 @@ struct Wave {
     char *dev = nullptr, *host = nullptr;
     cudaStream_t stream = nullptr;
     bool cooperative = true;   // false: plain launch (the caller guarantees the blocks are co-resident)
+    int *done_flags = nullptr; // device view of host-mapped words, one per instance (nullptr: none)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
     float ms = 0;
 };
@@ -114,6 +115,8 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
 int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, Wave &w,
                char *dev, char *host, cudaStream_t s);
 bool wave_ready(const Wave &w);
+// Copy instance k's results (once its done flag is set) with a copy on stream s.
+int wave_fetch(const Wave &w, int k, SolveResult &r, cudaStream_t s);
 // Wait for the wave and unpack results[first .. first+count).
 int wave_finish(Wave &w, std::vector<SolveResult> &res);
 

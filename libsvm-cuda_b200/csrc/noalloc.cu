@@ -203,6 +203,7 @@ extern "C" int svmb_solve_dense_noalloc(int n, int ld, const float *X, const dou
     if (params->prefetch > 0) D.prefetch = std::min(D.prefetch, params->prefetch);
     D.lazy_gbar = 0;
     D.tc_n = 0;
+    D.done_flag = nullptr;
     int block_inst[kNoAllocMaxBlocks];
     for (int b = 0; b < nb; b++) block_inst[b] = 0;
 

@@ -192,6 +192,7 @@ struct Session {
 
 std::mutex g_mu;
 std::map<const svm_model *, std::unique_ptr<Session>> g_sessions;
+int g_predict_form = FORM_EXACT;
 
 #define PK(call)                                                                  \
     do {                                                                          \
@@ -289,7 +290,65 @@ Session *get_session(const svm_model *m)
     return raw;
 }
 
+// Tensor-core kernel values: the SVs and the test rows of a chunk go into one
+// row set (column = feature index), whose split copy feeds the block product
+// K(test, SV) on the tensor cores; RBF uses the float64 norms of both.
+int kvalue_tensor(const svm_model *m, const svm_node *const *rows, int tn, int form, double *kv)
+{
+    const int l = m->l;
+    const int n = l + tn;
+    std::vector<long long> rp((size_t)n + 1, 0);
+    std::vector<int> col;
+    std::vector<float> val;
+    int maxi = 0;
+    for (int r = 0; r < n; r++) {
+        const svm_node *x = r < l ? m->SV[r] : rows[r - l];
+        for (const svm_node *p = x; p->index != -1; ++p) {
+            col.push_back(p->index);
+            val.push_back((float)p->value);
+            maxi = std::max(maxi, p->index);
+        }
+        rp[r + 1] = (long long)col.size();
+    }
+    if (col.empty()) { col.push_back(0); val.push_back(0.0f); }
+    DeviceRows dr;
+    if (upload_csr(rp.data(), col.data(), val.data(), n, maxi + 1, dr, -1, 0) != 0) return -1;
+    if (dr.prepare_form(form, 0) != 0) return -1;
+    std::vector<int> ia(tn), ib(l);
+    for (int t = 0; t < tn; t++) ia[t] = l + t;
+    for (int s = 0; s < l; s++) ib[s] = s;
+    int *d_ia = nullptr, *d_ib = nullptr, *d_err = nullptr;
+    PK(cudaMalloc(&d_ia, sizeof(int) * (size_t)tn));
+    PK(cudaMalloc(&d_ib, sizeof(int) * (size_t)l));
+    PK(cudaMalloc(&d_err, sizeof(int)));
+    PK(xfer(d_ia, ia.data(), sizeof(int) * (size_t)tn, cudaMemcpyHostToDevice));
+    PK(xfer(d_ib, ib.data(), sizeof(int) * (size_t)l, cudaMemcpyHostToDevice));
+    PK(cudaMemset(d_err, 0, sizeof(int)));
+    KernelParams kp{m->param.kernel_type, m->param.degree, m->param.gamma, m->param.coef0};
+    cudaError_t e = launch_kernel_block(dr, kp, form, d_ia, tn, d_ib, l, kv, l, d_err, 0);
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = xfer(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d_ia);
+    cudaFree(d_ib);
+    cudaFree(d_err);
+    if (e != cudaSuccess || herr) {
+        set_error(e != cudaSuccess ? std::string("tensor-core kernel values: ") + cudaGetErrorString(e)
+                                   : std::string("tensor-core kernel values: a wait timed out"));
+        return -1;
+    }
+    return 0;
+}
+
 }  // namespace
+
+int predict_set_form(int form)
+{
+    if (form != FORM_EXACT && !is_tc_form(form)) return -1;
+    std::lock_guard<std::mutex> g(g_mu);
+    g_predict_form = form;
+    return 0;
+}
 
 void predict_forget(const svm_model *model)
 {
@@ -334,7 +393,9 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
             for (int r = 0; r < tn; r++)
                 for (const svm_node *p = rows[t0 + r]; p->index != -1; ++p) maxi = std::max(maxi, p->index);
             const bool wider = maxi + 1 > s->d;
-            if (s->sv.dense && !wider) {
+            if (is_tc_form(g_predict_form)) {
+                if (kvalue_tensor(m, rows + t0, tn, g_predict_form, kv) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
+            } else if (s->sv.dense && !wider) {
                 if (upload_nodes(rows + t0, tn, s->d, s->base, true, T) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
                 dim3 grid((m->l + 255) / 256, (tn + kTT - 1) / kTT);
                 const size_t smem = (size_t)kTT * s->sv.ld * sizeof(float);

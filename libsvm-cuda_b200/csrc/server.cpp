@@ -5,17 +5,25 @@
 // svm-train/svm-train.c:92-133); there is no serving layer to mirror.  Here a
 // scheduler thread keeps up to `max_inflight` persistent launches ("waves")
 // running on their own streams.  Whenever a wave finishes or a request
-// arrives, pending requests are admitted in arrival order while
+// arrives, a leading request -- the smallest pending one (the oldest once it
+// has waited 2 s), or the oldest, by policy -- and the pending ones of a
+// similar size (within a factor of 4 in rows) are admitted while
 //   - the device memory of the admitted work (rows + solver state with its
 //     Q-row cache budget) stays within the server's budget, and
 //   - the thread blocks their state needs fit in the SMs that no running wave
 //     holds,
 // then uploaded (stream-ordered allocations, no device-wide synchronisation)
 // and launched together as one new wave next to the waves already running.
+// Requests get fewer blocks than a solve alone (rows / rows_per_block): a
+// solve's iterations are latency-bound, so more requests side by side give
+// more throughput than more blocks per request.
 // A wave's blocks are planned within the free SMs, so all of them are
 // resident at once; launches are therefore plain (not cooperative) and
-// several run concurrently.  Each request keeps its rows and state on the
-// device until its wave ends.  Results equal a solve of the same request
+// several run concurrently.  When every block of one request has finished,
+// the kernel sets that request's word in host-mapped memory; the scheduler
+// then copies its result out and hands its SMs to the next wave while the
+// rest of the launch runs on.  Rows and solver state stay on the device
+// until the launch ends.  Results equal a solve of the same request
 // alone: the solver's arithmetic does not depend on the number of blocks or
 // on the other instances of a launch.
 #include <cuda_runtime.h>
@@ -40,6 +48,7 @@ namespace svmb {
 namespace {
 
 using Clock = std::chrono::steady_clock;
+constexpr double kMaxWait = 2.0;    // seconds a request may wait before it leads regardless of its size
 
 struct Job {
     long long ticket = 0;
@@ -64,6 +73,9 @@ struct Slot {
     bool busy = false;
     cudaStream_t stream = nullptr;
     Wave w;
+    int *flags_host = nullptr;      // host-mapped completion words, one per instance of the wave
+    int *flags_dev = nullptr;
+    std::vector<char> delivered;    // instance results already handed out
     std::vector<Job *> jobs;
     std::vector<SubProblem> subs;
     char *dev = nullptr;
@@ -112,43 +124,81 @@ struct Server {
     Clock::time_point t_first, t_last;
     bool any_submit = false;
 
+    cudaStream_t copy_stream = nullptr;
+
     void loop();
     void admit(Slot &slot, std::unique_lock<std::mutex> &lk);
+    void collect(Slot &slot);
     void reap(Slot &slot);
+    void complete_locked(Job *j, bool ok, const std::string &err);
 };
+
+// a request's final state (called with the lock held)
+void Server::complete_locked(Job *j, bool ok, const std::string &err)
+{
+    j->t_done = Clock::now();
+    j->state = ok ? 2 : -1;             // waiters read a request only once its state is final
+    if (ok) {
+        completed++;
+        latencies.push_back(std::chrono::duration<double>(j->t_done - j->t_submit).count());
+    } else {
+        j->error = err;
+        failed++;
+    }
+    t_last = j->t_done;
+    cv_done.notify_all();
+}
+
+// Hand out the instances of a running wave whose blocks have all finished
+// (their completion word is set) and give their SMs to new waves at once
+// (called without the lock).
+void Server::collect(Slot &slot)
+{
+    for (int k = 0; k < slot.w.count; k++) {
+        if (slot.delivered[k] || *(volatile int *)(slot.flags_host + k) == 0) continue;
+        Job *j = slot.jobs[k];
+        SolveResult r;
+        const int rc = wave_fetch(slot.w, k, r, copy_stream);
+        if (rc == 0) {
+            j->alpha.assign(j->n, 0.0);
+            capi::finish_instance(j->sub, r, j->alpha.data(), &j->stats);
+        }
+        const std::string err = rc ? std::string(last_error()) : std::string();
+        slot.delivered[k] = 1;
+        j->rows->release_async(slot.stream);    // ordered after the launch on its stream
+        j->rows.reset();
+        slot.jobs[k] = nullptr;                 // a waiter may free the request once it is complete
+        std::lock_guard<std::mutex> g(mu);
+        complete_locked(j, rc == 0, err);
+        blocks_used -= slot.w.nb[k];
+        slot.blocks -= slot.w.nb[k];
+    }
+}
 
 // Collect a finished wave (called without the lock).
 void Server::reap(Slot &slot)
 {
+    collect(slot);
     std::vector<SolveResult> res(slot.subs.size());
     const int rc = wave_finish(slot.w, res);
     const std::string err = rc ? std::string(last_error()) : std::string();
-    const auto now = Clock::now();
     cudaFreeAsync(slot.dev, slot.stream);
     slot.dev = nullptr;
     for (size_t k = 0; k < slot.jobs.size(); k++) {
         Job *j = slot.jobs[k];
+        if (slot.delivered[k]) continue;
         j->rows->release_async(slot.stream);
         if (rc == 0) {
             j->alpha.assign(j->n, 0.0);
             capi::finish_instance(j->sub, res[k], j->alpha.data(), &j->stats);
-        } else {
-            j->error = err;
         }
-        j->t_done = now;
     }
     std::lock_guard<std::mutex> g(mu);
-    for (Job *j : slot.jobs) {
-        j->state = rc == 0 ? 2 : -1;        // waiters read a request only once its state is final
-        if (j->state == 2) {
-            completed++;
-            latencies.push_back(std::chrono::duration<double>(j->t_done - j->t_submit).count());
-        } else {
-            failed++;
-        }
-        j->rows.reset();
+    for (size_t k = 0; k < slot.jobs.size(); k++) {
+        if (slot.delivered[k]) continue;
+        slot.jobs[k]->rows.reset();
+        complete_locked(slot.jobs[k], rc == 0, err);
     }
-    t_last = now;
     mem_used -= slot.mem;
     blocks_used -= slot.blocks;
     slot.jobs.clear();
@@ -165,8 +215,25 @@ void Server::admit(Slot &slot, std::unique_lock<std::mutex> &lk)
     if (free_blocks <= 0 || pending.empty()) return;
     std::vector<Job *> take;
     size_t mem = 0;
+    // A leading request, then pending requests whose size is within a factor
+    // of 4 of the leader's: a launch keeps its device memory until its
+    // longest solve ends, so similar sizes free it sooner.
+    // the leader: the oldest request, or (smallest-first policy) the smallest
+    // one unless the oldest has waited longer than kMaxWait
+    if (cfg.policy == SVMB_SERVE_SMALLEST_FIRST &&
+        std::chrono::duration<double>(Clock::now() - pending.front()->t_submit).count() < kMaxWait) {
+        auto best = std::min_element(pending.begin(), pending.end(), [](const Job *a, const Job *b) { return a->n < b->n; });
+        Job *lead = *best;
+        pending.erase(best);
+        pending.push_front(lead);
+    }
+    double lead_rows = 0;
     for (auto it = pending.begin(); it != pending.end() && (int)take.size() < std::min(cfg.max_batch, free_blocks);) {
         Job *j = *it;
+        if (!take.empty() && ((double)j->n > 4.0 * lead_rows || 4.0 * (double)j->n < lead_rows)) {
+            ++it;
+            continue;
+        }
         if (mem_used + mem + j->mem > (size_t)cfg.mem_bytes) {
             // nothing running and nothing taken: this request can never fit
             if (take.empty() && blocks_used == 0 && j->mem > (size_t)cfg.mem_bytes) {
@@ -178,8 +245,11 @@ void Server::admit(Slot &slot, std::unique_lock<std::mutex> &lk)
                 cv_done.notify_all();
                 continue;
             }
-            break;      // arrival order: later requests wait behind the first that does not fit
+            if (take.empty()) break;    // the leader waits for memory; nothing overtakes it
+            ++it;
+            continue;
         }
+        if (take.empty()) lead_rows = (double)j->n;
         take.push_back(j);
         mem += j->mem;
         it = pending.erase(it);
@@ -244,6 +314,9 @@ void Server::admit(Slot &slot, std::unique_lock<std::mutex> &lk)
     }
     if (ok) {
         slot.w.cooperative = false;
+        memset(slot.flags_host, 0, sizeof(int) * (size_t)cfg.max_batch);
+        slot.w.done_flags = slot.flags_dev;
+        slot.delivered.assign(slot.w.count, 0);
         if (wave_start(empty_rows(), slot.subs, take[0]->prm, slot.w, slot.dev, slot.host, slot.stream) != 0) {
             ok = false;
             err = last_error();
@@ -291,13 +364,11 @@ void Server::loop()
         bool any_busy = false;
         for (Slot &s : slots) {
             if (!s.busy) continue;
-            if (wave_ready(s.w)) {
-                lk.unlock();
-                reap(s);
-                lk.lock();
-            } else {
-                any_busy = true;
-            }
+            lk.unlock();
+            if (wave_ready(s.w)) reap(s);
+            else collect(s);
+            lk.lock();
+            if (s.busy) any_busy = true;
         }
         for (Slot &s : slots) {
             if (pending.empty()) break;
@@ -334,16 +405,29 @@ int svmb_server_create(const svmb_server_config *cfg, svmb_server **out)
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     if (S.cfg.mem_bytes <= 0) S.cfg.mem_bytes = (long long)(free_b * 0.8);
-    if (S.cfg.max_inflight <= 0) S.cfg.max_inflight = 4;
-    if (S.cfg.max_batch <= 0) S.cfg.max_batch = 64;
+    if (S.cfg.max_inflight <= 0) S.cfg.max_inflight = 8;
+    if (S.cfg.max_batch <= 0) S.cfg.max_batch = 32;
+    if (S.cfg.rows_per_block <= 0) S.cfg.rows_per_block = 2000;
+    if (S.cfg.policy != SVMB_SERVE_ARRIVAL_ORDER) S.cfg.policy = SVMB_SERVE_SMALLEST_FIRST;
     S.capacity = svmb::device_sm_count();     // one solver block per SM at its largest shared memory
     if (S.capacity <= 0) { svmb::set_error("no CUDA device"); return -1; }
     S.slots.resize(S.cfg.max_inflight);
-    for (auto &sl : S.slots)
+    if (cudaStreamCreateWithFlags(&S.copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        svmb::set_error("stream creation failed");
+        return -1;
+    }
+    for (auto &sl : S.slots) {
         if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess) {
             svmb::set_error("stream creation failed");
             return -1;
         }
+        // completion words the kernel sets in host memory, one per instance
+        if (cudaHostAlloc((void **)&sl.flags_host, sizeof(int) * (size_t)S.cfg.max_batch, cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostGetDevicePointer((void **)&sl.flags_dev, sl.flags_host, 0) != cudaSuccess) {
+            svmb::set_error("mapped host allocation failed");
+            return -1;
+        }
+    }
     S.worker = std::thread([&S] { S.loop(); });
     *out = h.release();
     return 0;
@@ -367,6 +451,8 @@ long long svmb_server_submit(svmb_server *h, int n, int d, const long long *rowp
     j->val.assign(val, val + rowptr[n]);
     j->params = *params;
     j->prm = svmb::capi::to_solve_params(*params);
+    if (j->prm.blocks_override <= 0)
+        j->prm.blocks_override = std::max(1, std::min(svmb::device_sm_count(), n / h->s.cfg.rows_per_block));
     std::vector<int> idx(n);
     for (int i = 0; i < n; i++) idx[i] = i;
     if (svmb::capi::make_subproblem(*params, n, idx.data(), y, n, j->sub) != 0) return -1;
@@ -455,7 +541,9 @@ void svmb_server_destroy(svmb_server *h)
             cudaStreamDestroy(sl.stream);
         }
         if (sl.host) cudaFreeHost(sl.host);
+        if (sl.flags_host) cudaFreeHost(sl.flags_host);
     }
+    if (h->s.copy_stream) cudaStreamDestroy(h->s.copy_stream);
     delete h;
 }
 

@@ -2089,6 +2089,22 @@ fail:
 #undef SVMB_PROF
 }
 
+// Tell the host, through a word of mapped host memory, that every block of the
+// instance has written its results (a request loop collects the instance and
+// reuses its SMs while the rest of the launch runs on).
+__device__ void signal_done(const InstanceDesc &D)
+{
+    if (!D.done_flag) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence_system();
+        if (atomicAdd(&D.sync->finished, 1u) == (unsigned)D.nblocks - 1u) {
+            __threadfence_system();
+            *(volatile int *)D.done_flag = 1;
+        }
+    }
+}
+
 template <int FORM>
 __global__ void __launch_bounds__(kThreads, 1)
 smo_persistent(const InstanceDesc *__restrict__ insts, const int *__restrict__ block_inst)
@@ -2113,6 +2129,7 @@ smo_persistent(const InstanceDesc *__restrict__ insts, const int *__restrict__ b
         tc::tc_fence_after();
     }
     solve_instance<FORM>(D, rank, sh, dyn);
+    signal_done(D);
     if constexpr (is_tc_form(FORM)) {
         tc::tc_fence_before();
         __syncthreads();

@@ -32,6 +32,10 @@ extern "C" {
 int libsvm_version = LIBSVM_VERSION;
 }
 
+namespace svmb {
+int api_force_layout();
+}
+
 namespace {
 
 void print_string_stdout(const char *s)
@@ -225,103 +229,80 @@ DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResul
 
 bool svm_type_supported(int t) { return t == C_SVC || t == NU_SVC; }
 
-}  // namespace
-
-namespace svmb {
-int api_set_option(const char *name, long long value)
+bool train_supported(const svm_parameter *param)
 {
-    if (!strcmp(name, "form")) {
-        if (value != FORM_EXACT && value != FORM_FP32 && value != FORM_BF16X3 && value != FORM_FP16X3) return -1;
-        g_opt.form = (int)value;
-    } else if (!strcmp(name, "blocks")) {
-        g_opt.blocks = (int)value;
-    } else if (!strcmp(name, "layout")) {
-        g_opt.force_layout = (int)value;
-    } else if (!strcmp(name, "prefetch")) {
-        if (value < 0 || value > kPrefetchMax) return -1;
-        g_opt.prefetch = (int)value;
-    } else {
-        return -1;
-    }
-    return 0;
-}
-int api_last_stats(svmb_solve_stats *out, int cap)
-{
-    std::lock_guard<std::mutex> g(g_stats_mu);
-    const int n = (int)g_last_stats.size();
-    for (int k = 0; k < n && k < cap; k++) out[k] = g_last_stats[k];
-    return n;
-}
-void api_print(const char *s) { (*svm_print_string)(s); }
-int api_force_layout() { return g_opt.force_layout; }
-}  // namespace svmb
-
-extern "C" {
-
-struct svm_model *svm_train(const struct svm_problem *prob, const struct svm_parameter *param)
-{
-    {
-        std::lock_guard<std::mutex> g(g_stats_mu);
-        g_last_stats.clear();
-    }
     if (!svm_type_supported(param->svm_type) || param->kernel_type == PRECOMPUTED) {
         svmb::set_error("only C_SVC and NU_SVC with linear/poly/rbf/sigmoid kernels are trained on the GPU");
         info("ERROR: %s\n", svmb::last_error());
-        return NULL;
+        return false;
     }
-    const int l = prob->l;
-    int nr_class;
+    return true;
+}
+
+// One svm_train call (reference svm.cpp:2159-2404) split into its one-vs-one
+// subproblems -- which address the rows of an uploaded row set by id -- and
+// the model assembly from their solutions, so that the subproblems of many
+// trainings (CV folds, grid points) can share one batched solve.
+struct TrainJob {
+    const svm_problem *prob = nullptr;
+    svm_parameter param{};
+    int l = 0, nr_class = 0;
     std::vector<int> label, start, count, perm;
-    group_classes(prob, &nr_class, label, start, count, perm);
+    std::vector<svm_node *> x;                 // rows in grouped order
+    std::vector<svmb::SubProblem> subs;
+    std::vector<std::vector<double>> subys;
+    svmb::SolveParams own;                     // solve parameters of this training
+};
+
+// row_id[i]: id of prob row i in the uploaded row set (nullptr: rows uploaded in grouped order)
+void setup_train(const svm_problem *prob, const svm_parameter *param, const int *row_id, TrainJob &tj)
+{
+    tj.prob = prob;
+    tj.param = *param;
+    tj.l = prob->l;
+    group_classes(prob, &tj.nr_class, tj.label, tj.start, tj.count, tj.perm);
+    const int nr_class = tj.nr_class;
     if (nr_class == 1) info("WARNING: training data in only one class. See README for details.\n");
-
-    std::vector<svm_node *> x(l);
-    for (int i = 0; i < l; i++) x[i] = prob->x[perm[i]];
-
+    tj.x.resize(tj.l);
+    for (int i = 0; i < tj.l; i++) tj.x[i] = prob->x[tj.perm[i]];
     std::vector<double> weighted_C(nr_class, param->C);
     for (int i = 0; i < param->nr_weight; i++) {
         int j;
         for (j = 0; j < nr_class; j++)
-            if (param->weight_label[i] == label[j]) break;
+            if (param->weight_label[i] == tj.label[j]) break;
         if (j == nr_class)
             fprintf(stderr, "WARNING: class label %d specified in weight is not found\n", param->weight_label[i]);
         else
             weighted_C[j] *= param->weight[i];
     }
-
-    // rows are uploaded once, in grouped order; every pair addresses them by id
-    svmb::DeviceRows rows;
-    if (l > 0 && svmb::upload_rows(x.data(), l, rows, svmb::api_force_layout(), 0) != 0) {
-        info("ERROR: %s\n", svmb::last_error());
-        return NULL;
-    }
-    std::vector<svmb::SubProblem> subs;
-    std::vector<std::vector<double>> subys;
+    auto id = [&](int g) { return row_id ? row_id[tj.perm[g]] : g; };   // grouped index -> uploaded row id
     for (int i = 0; i < nr_class; i++)
         for (int j = i + 1; j < nr_class; j++) {
             std::vector<int> r;
             std::vector<signed char> y;
             std::vector<double> yv;
-            for (int k = 0; k < count[i]; k++) { r.push_back(start[i] + k); y.push_back(+1); yv.push_back(+1); }
-            for (int k = 0; k < count[j]; k++) { r.push_back(start[j] + k); y.push_back(-1); yv.push_back(-1); }
-            subs.push_back(make_sub(r, y, param, weighted_C[i], weighted_C[j]));
-            subys.push_back(yv);
+            for (int k = 0; k < tj.count[i]; k++) { r.push_back(id(tj.start[i] + k)); y.push_back(+1); yv.push_back(+1); }
+            for (int k = 0; k < tj.count[j]; k++) { r.push_back(id(tj.start[j] + k)); y.push_back(-1); yv.push_back(-1); }
+            tj.subs.push_back(make_sub(r, y, param, weighted_C[i], weighted_C[j]));
+            tj.subys.push_back(yv);
         }
-    std::vector<svmb::SolveResult> res;
-    if (!subs.empty() && svmb::solve_batch(rows, subs, make_solve_params(param), res, 0) != 0) {
-        info("ERROR: %s\n", svmb::last_error());
-        return NULL;
-    }
-    std::vector<DecisionFunction> f(subs.size());
-    for (size_t p = 0; p < subs.size(); p++) f[p] = finish_solve(subs[p], res[p], param, subys[p].data());
+    tj.own = make_solve_params(param);
+}
 
-    // model assembly (svm.cpp:2297-2386)
+// model assembly (reference svm.cpp:2297-2386) from the solutions res[first ..]
+svm_model *assemble_model(const TrainJob &tj, const std::vector<svmb::SolveResult> &res, size_t first)
+{
+    const svm_parameter *param = &tj.param;
+    const int l = tj.l, nr_class = tj.nr_class;
+    const std::vector<int> &start = tj.start, &count = tj.count;
+    std::vector<DecisionFunction> f(tj.subs.size());
+    for (size_t p = 0; p < tj.subs.size(); p++) f[p] = finish_solve(tj.subs[p], res[first + p], param, tj.subys[p].data());
     svm_model *model = (svm_model *)malloc(sizeof(svm_model));
     model->param = *param;
     model->free_sv = 0;
     model->nr_class = nr_class;
     model->label = (int *)malloc(sizeof(int) * std::max(nr_class, 1));
-    for (int i = 0; i < nr_class; i++) model->label[i] = label[i];
+    for (int i = 0; i < nr_class; i++) model->label[i] = tj.label[i];
     const int npair = nr_class * (nr_class - 1) / 2;
     model->rho = (double *)malloc(sizeof(double) * std::max(npair, 1));
     for (int i = 0; i < npair; i++) model->rho[i] = f[i].rho;
@@ -357,8 +338,8 @@ struct svm_model *svm_train(const struct svm_problem *prob, const struct svm_par
         int p = 0;
         for (int i = 0; i < l; i++)
             if (nonzero[i]) {
-                model->SV[p] = x[i];
-                model->sv_indices[p++] = perm[i] + 1;
+                model->SV[p] = tj.x[i];
+                model->sv_indices[p++] = tj.perm[i] + 1;
             }
     }
     std::vector<int> nz_start(nr_class, 0);
@@ -381,8 +362,18 @@ struct svm_model *svm_train(const struct svm_problem *prob, const struct svm_par
     return model;
 }
 
-void svm_cross_validation(const struct svm_problem *prob, const struct svm_parameter *param, int nr_fold, double *target)
+// Stratified k-fold cross-validation (reference svm.cpp:2407-2525) over a grid
+// of (C, gamma) points: one fold assignment with the C library rand(), as the
+// reference draws it, then every point's and fold's one-vs-one subproblems are
+// solved in batched launches over the rows uploaded once.  target[p*l + i] is
+// the prediction of row i by the model of point p trained without i's fold.
+int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, int nr_fold, int npoints,
+                          const double *Cs, const double *gammas, double *target)
 {
+    {
+        std::lock_guard<std::mutex> g(g_stats_mu);
+        g_last_stats.clear();
+    }
     const int l = prob->l;
     std::vector<int> perm(l);
     if (nr_fold > l) {
@@ -423,39 +414,147 @@ void svm_cross_validation(const struct svm_problem *prob, const struct svm_param
         }
         for (int i = 0; i <= nr_fold; i++) fold_start[i] = i * l / nr_fold;
     }
-    std::vector<svmb_solve_stats> all_stats;
+    for (long long k = 0; k < (long long)npoints * l; k++) target[k] = NAN;
+    if (!train_supported(param)) return -1;
+    // all rows once, in the problem's order (row id = index in prob)
+    svmb::DeviceRows rows;
+    if (l > 0 && svmb::upload_rows(prob->x, l, rows, svmb::api_force_layout(), 0) != 0) {
+        info("ERROR: %s\n", svmb::last_error());
+        return -1;
+    }
+    // the training set of every fold, its row ids, and one training per (point, fold)
+    std::vector<svm_problem> fold_prob(nr_fold);
+    std::vector<std::vector<svm_node *>> fold_x(nr_fold);
+    std::vector<std::vector<double>> fold_y(nr_fold);
+    std::vector<std::vector<int>> fold_id(nr_fold);
     for (int i = 0; i < nr_fold; i++) {
         const int begin = fold_start[i], end = fold_start[i + 1];
-        svm_problem sub;
-        sub.l = l - (end - begin);
-        std::vector<svm_node *> sx(std::max(sub.l, 1));
-        std::vector<double> sy(std::max(sub.l, 1));
-        int k = 0;
-        for (int j = 0; j < begin; j++) { sx[k] = prob->x[perm[j]]; sy[k] = prob->y[perm[j]]; ++k; }
-        for (int j = end; j < l; j++) { sx[k] = prob->x[perm[j]]; sy[k] = prob->y[perm[j]]; ++k; }
-        sub.x = sx.data();
-        sub.y = sy.data();
-        svm_model *m = svm_train(&sub, param);
-        {
-            std::lock_guard<std::mutex> g(g_stats_mu);
-            all_stats.insert(all_stats.end(), g_last_stats.begin(), g_last_stats.end());
+        for (int j = 0; j < l; j++) {
+            if (j >= begin && j < end) continue;
+            fold_x[i].push_back(prob->x[perm[j]]);
+            fold_y[i].push_back(prob->y[perm[j]]);
+            fold_id[i].push_back(perm[j]);
         }
-        if (!m) {
-            for (int j = begin; j < end; j++) target[perm[j]] = NAN;
-            continue;
-        }
-        std::vector<const svm_node *> held;
-        for (int j = begin; j < end; j++) held.push_back(prob->x[perm[j]]);
-        std::vector<double> lab(held.size());
-        if (!held.empty() && svmb::predict_batch(m, held.data(), (int)held.size(), lab.data(), nullptr) != 0) {
-            for (int j = begin; j < end; j++) target[perm[j]] = NAN;
-        } else {
-            for (int j = begin; j < end; j++) target[perm[j]] = lab[j - begin];
-        }
-        svm_free_and_destroy_model(&m);
+        fold_prob[i].l = (int)fold_x[i].size();
+        fold_prob[i].x = fold_x[i].data();
+        fold_prob[i].y = fold_y[i].data();
     }
+    std::vector<svm_parameter> pparam(npoints, *param);
+    std::vector<TrainJob> jobs((size_t)npoints * nr_fold);
+    std::vector<svmb::SubProblem> all;
+    std::vector<size_t> first(jobs.size());
+    for (int q = 0; q < npoints; q++) {
+        pparam[q].C = Cs[q];
+        pparam[q].gamma = gammas[q];
+        for (int i = 0; i < nr_fold; i++) {
+            TrainJob &tj = jobs[(size_t)q * nr_fold + i];
+            setup_train(&fold_prob[i], &pparam[q], fold_id[i].data(), tj);
+        }
+    }
+    for (size_t k = 0; k < jobs.size(); k++) {
+        first[k] = all.size();
+        for (svmb::SubProblem &sp : jobs[k].subs) {
+            sp.own = &jobs[k].own;
+            all.push_back(sp);
+        }
+    }
+    std::vector<svmb::SolveResult> res;
+    {
+        std::lock_guard<std::mutex> g(g_stats_mu);
+        g_last_stats.clear();
+    }
+    if (!all.empty() && svmb::solve_batch(rows, all, jobs[0].own, res, 0) != 0) {
+        info("ERROR: %s\n", svmb::last_error());
+        return -1;
+    }
+    for (int q = 0; q < npoints; q++)
+        for (int i = 0; i < nr_fold; i++) {
+            const size_t k = (size_t)q * nr_fold + i;
+            svm_model *m = assemble_model(jobs[k], res, first[k]);
+            const int begin = fold_start[i], end = fold_start[i + 1];
+            std::vector<const svm_node *> held;
+            for (int j = begin; j < end; j++) held.push_back(prob->x[perm[j]]);
+            std::vector<double> lab(held.size());
+            if (held.empty() || svmb::predict_batch(m, held.data(), (int)held.size(), lab.data(), nullptr) == 0)
+                for (int j = begin; j < end; j++) target[(size_t)q * l + perm[j]] = lab[j - begin];
+            svm_free_and_destroy_model(&m);
+        }
+    return 0;
+}
+
+
+}  // namespace
+
+namespace svmb {
+int api_set_option(const char *name, long long value)
+{
+    if (!strcmp(name, "form")) {
+        if (value != FORM_EXACT && value != FORM_FP32 && value != FORM_BF16X3 && value != FORM_FP16X3) return -1;
+        g_opt.form = (int)value;
+    } else if (!strcmp(name, "blocks")) {
+        g_opt.blocks = (int)value;
+    } else if (!strcmp(name, "layout")) {
+        g_opt.force_layout = (int)value;
+    } else if (!strcmp(name, "predict_form")) {
+        if (predict_set_form((int)value) != 0) return -1;
+    } else if (!strcmp(name, "prefetch")) {
+        if (value < 0 || value > kPrefetchMax) return -1;
+        g_opt.prefetch = (int)value;
+    } else {
+        return -1;
+    }
+    return 0;
+}
+int api_last_stats(svmb_solve_stats *out, int cap)
+{
     std::lock_guard<std::mutex> g(g_stats_mu);
-    g_last_stats = all_stats;
+    const int n = (int)g_last_stats.size();
+    for (int k = 0; k < n && k < cap; k++) out[k] = g_last_stats[k];
+    return n;
+}
+void api_print(const char *s) { (*svm_print_string)(s); }
+int api_force_layout() { return g_opt.force_layout; }
+}  // namespace svmb
+
+extern "C" {
+
+struct svm_model *svm_train(const struct svm_problem *prob, const struct svm_parameter *param)
+{
+    {
+        std::lock_guard<std::mutex> g(g_stats_mu);
+        g_last_stats.clear();
+    }
+    if (!train_supported(param)) return NULL;
+    TrainJob tj;
+    setup_train(prob, param, nullptr, tj);
+    // rows are uploaded once, in grouped order; every pair addresses them by id
+    svmb::DeviceRows rows;
+    if (tj.l > 0 && svmb::upload_rows(tj.x.data(), tj.l, rows, svmb::api_force_layout(), 0) != 0) {
+        info("ERROR: %s\n", svmb::last_error());
+        return NULL;
+    }
+    std::vector<svmb::SolveResult> res;
+    if (!tj.subs.empty() && svmb::solve_batch(rows, tj.subs, make_solve_params(param), res, 0) != 0) {
+        info("ERROR: %s\n", svmb::last_error());
+        return NULL;
+    }
+    return assemble_model(tj, res, 0);
+}
+
+void svm_cross_validation(const struct svm_problem *prob, const struct svm_parameter *param, int nr_fold, double *target)
+{
+    const double C1[1] = {param->C}, G1[1] = {param->gamma};
+    cross_validation_grid(prob, param, nr_fold, 1, C1, G1, target);
+}
+
+int svmb_cross_validation_grid(const struct svm_problem *prob, const struct svm_parameter *param, int nr_fold,
+                               int npoints, const double *C, const double *gamma, double *target)
+{
+    if (!prob || !param || !C || !gamma || !target || npoints <= 0 || nr_fold < 2) {
+        svmb::set_error("invalid arguments");
+        return -1;
+    }
+    return cross_validation_grid(prob, param, nr_fold, npoints, C, gamma, target);
 }
 
 int svm_get_svm_type(const svm_model *model) { return model->param.svm_type; }

@@ -44,7 +44,8 @@ class SvmbParams(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("mem_bytes", C.c_longlong), ("max_inflight", C.c_int), ("max_batch", C.c_int), ("form", C.c_int)]
+    _fields_ = [("mem_bytes", C.c_longlong), ("max_inflight", C.c_int), ("max_batch", C.c_int), ("form", C.c_int),
+                ("policy", C.c_int), ("rows_per_block", C.c_int)]
 
 
 class ServerStats(C.Structure):
@@ -106,6 +107,8 @@ def _load(path: str) -> C.CDLL:
     lib.svmb_rows_free.argtypes = [C.c_void_p]
     lib.svmb_rows_kernel_block.argtypes = [C.c_void_p, _P(SvmbParams), C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                            C.c_void_p]
+    lib.svmb_cross_validation_grid.argtypes = [_P(svm_problem), _P(svm_parameter), C.c_int, C.c_int, C.c_void_p,
+                                               C.c_void_p, C.c_void_p]
     lib.svmb_server_create.argtypes = [_P(ServerConfig), _P(C.c_void_p)]
     lib.svmb_server_submit.restype = C.c_longlong
     lib.svmb_server_submit.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -197,6 +200,17 @@ class Engine:
         out = np.zeros(max(p.n, 1))
         self.lib.svm_cross_validation(C.byref(rows.prob), C.byref(param), nfold, out.ctypes.data_as(_P(C.c_double)))
         return out[:p.n]
+
+    def cross_validation_grid(self, p: CSR, param: svm_parameter, nfold: int, Cs, gammas) -> np.ndarray:
+        """svmb_cross_validation_grid: predictions [npoints][n] of every (C, gamma) point."""
+        rows = NodeRows(p)
+        Cs = np.ascontiguousarray(Cs, dtype=np.float64)
+        gs = np.ascontiguousarray(gammas, dtype=np.float64)
+        out = np.zeros((len(Cs), max(p.n, 1)))
+        rc = self.lib.svmb_cross_validation_grid(C.byref(rows.prob), C.byref(param), nfold, len(Cs), Cs.ctypes.data,
+                                                 gs.ctypes.data, out.ctypes.data)
+        self._ok(rc, "svmb_cross_validation_grid")
+        return out[:, :p.n]
 
     def predict(self, model: Model, p: CSR) -> Tuple[np.ndarray, np.ndarray]:
         rows = NodeRows(p)
@@ -301,10 +315,11 @@ class Server:
     """Request loop (svmb_server_*): submitted binary solves are batched
     continuously onto the GPU; wait(ticket) returns (signed alpha, stats, latency)."""
 
-    def __init__(self, eng: Engine, mem_bytes: int = 0, max_inflight: int = 0, max_batch: int = 0, form: int = 0):
+    def __init__(self, eng: Engine, mem_bytes: int = 0, max_inflight: int = 0, max_batch: int = 0, form: int = 0,
+                 policy: int = 0, rows_per_block: int = 0):
         self.eng = eng
         self.h = None
-        cfg = ServerConfig(mem_bytes, max_inflight, max_batch, form)
+        cfg = ServerConfig(mem_bytes, max_inflight, max_batch, form, policy, rows_per_block)
         h = C.c_void_p()
         eng._ok(eng.lib.svmb_server_create(C.byref(cfg), C.byref(h)), "svmb_server_create")
         self.h = h
