@@ -19,12 +19,12 @@
 // multiple of 64.  RBF distances use the float64 row norms.
 // The kernel value itself is always formed in float64 from the dot product.
 //
-// Tensor-core tiling: one CTA computes a 128 x 128 tile of dots; K runs in
+// Tensor-core tiling: one CTA computes a 128 x 64 tile of dots; K runs in
 // chunks of 64 features (the split rows store, per chunk, 64 hi then 64 lo
-// bf16 = 256 contiguous bytes), staged by cp.async into 128B-swizzled
+// 16-bit values = 256 contiguous bytes), staged by cp.async into 128B-swizzled
 // K-major shared-memory tiles, three stages deep; thread 0 issues the 12 MMAs
-// of a chunk (4 K-steps x 3 products, M=128 N=128 K=16) and commits them to
-// the stage's mbarrier, which releases the stage for the next chunk's loads.
+// of a chunk (4 K-steps x 3 products, M=128 N=64 K=16) and commits them to
+// the stage's mbarrier, which releases the stage and the chunk's accumulator.
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -39,17 +39,19 @@ namespace svmb {
 
 namespace {
 
-constexpr int kGM = 128;
-constexpr int kGN = 128;
+constexpr int kGM = 128;                                // rows of a tile (TMEM lanes)
+constexpr int kGN = 64;                                 // columns of a tile
+constexpr int kGThreads = 256;                          // 8 warps: 4 lane quarters x 2 column halves
 constexpr int kGStages = 3;
-constexpr int kGTile = 128 * 128;                       // bytes of one 128-row x 64-bf16 operand tile
-constexpr int kGStageBytes = 4 * kGTile;                // A hi, A lo, B hi, B lo
+constexpr int kGTileA = kGM * 128;                      // bytes of a 128-row x 64-bf16 operand tile
+constexpr int kGTileB = kGN * 128;                      // bytes of a 64-row x 64-bf16 operand tile
+constexpr int kGStageBytes = 2 * kGTileA + 2 * kGTileB; // A hi, A lo, B hi, B lo
 constexpr int kGSmem = kGStages * kGStageBytes + 1024;  // + alignment slack
 
 struct GramArgs {
     const uint16_t *xs;         // split rows [n][nchunk][128]
     const double *xinv;         // per-row inverse scales (fp16 split) or nullptr
-    long long rs;               // row stride in bf16 elements (nchunk * 128)
+    long long rs;               // row stride in 16-bit elements (nchunk * 128)
     int nchunk;
     const int *ia;              // row ids of the tile rows (nullptr: identity)
     int ma;
@@ -62,30 +64,39 @@ struct GramArgs {
     int *err;
 };
 
+// One CTA: a 128 x 64 tile of dots.  Each 64-feature chunk's 12 MMAs (4
+// K-steps x hi.lo, lo.hi, hi.hi) start a fresh float32 accumulator in TMEM
+// (two, alternating); while the next chunk's MMAs run, the 8 warps add the
+// finished chunk into float64 registers (warp w: lanes 32(w%4).., columns
+// 32(w/4)..+31), so the tensor core's float32 accumulation spans 64 features.
 template <bool BF16>
-__global__ void __launch_bounds__(128, 1) gram_split_kernel(GramArgs a)
+__global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
 {
     extern __shared__ uint8_t g_smem_raw[];
-    __shared__ uint64_t bars[kGStages + 1];
+    __shared__ uint64_t bars[kGStages];
     __shared__ uint32_t tmem_base;
     __shared__ long long offA[kGM], offB[kGN];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int lq = warp & 3, ch = warp >> 2;
     const int m0 = blockIdx.y * kGM, n0 = blockIdx.x * kGN;
     const uint32_t raw = tc::smem_addr(g_smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
 
-    {
-        const int r = m0 + tid, c = n0 + tid;
+    if (tid < kGM) {
+        const int r = m0 + tid;
         offA[tid] = r < a.ma ? (long long)(a.ia ? a.ia[r] : r) * a.rs : -1;
+    }
+    if (tid < kGN) {
+        const int c = n0 + tid;
         offB[tid] = c < a.nb ? (long long)(a.ib ? a.ib[c] : c) * a.rs : -1;
     }
     if (tid == 0) {
-        for (int s = 0; s <= kGStages; s++) tc::mbar_init(&bars[s], 1);
+        for (int s = 0; s < kGStages; s++) tc::mbar_init(&bars[s], 1);
         tc::mbar_init_fence();
     }
     if (warp == 0) {
-        tc::tmem_alloc(&tmem_base, kGN);
+        tc::tmem_alloc(&tmem_base, 2 * kGN);
         tc::tmem_relinquish();
     }
     tc::tc_fence_before();
@@ -93,21 +104,39 @@ __global__ void __launch_bounds__(128, 1) gram_split_kernel(GramArgs a)
     tc::tc_fence_after();
     const uint32_t tmem = tmem_base;
 
-    // stage s <- chunk kc of the 128 A rows and 128 B rows (16 pieces of 16 B per row)
+    // stage s <- chunk kc of the 128 A rows and 64 B rows (16 pieces of 16 B per row)
     auto load = [&](int s, int kc) {
         const uint32_t sa = base + s * kGStageBytes;
-#pragma unroll 4
-        for (int i = 0; i < 16; i++) {
-            const int idx = tid + 128 * i, r = idx >> 4, q = idx & 15;
-            const uint32_t so = (q >= 8 ? kGTile : 0) + tc::sw128_offset(r, q & 7);
-            const long long oa = offA[r], ob = offB[r];
-            tc::cp_async16(sa + so, a.xs + (oa < 0 ? 0 : oa) + kc * 128 + q * 8, oa < 0 ? 0u : 16u);
-            tc::cp_async16(sa + 2 * kGTile + so, a.xs + (ob < 0 ? 0 : ob) + kc * 128 + q * 8, ob < 0 ? 0u : 16u);
+        for (int idx = tid; idx < (kGM + kGN) * 16; idx += kGThreads) {
+            const int r = idx >> 4, q = idx & 15;
+            if (r < kGM) {
+                const long long o = offA[r];
+                tc::cp_async16(sa + (q >= 8 ? kGTileA : 0) + tc::sw128_offset(r, q & 7),
+                               a.xs + (o < 0 ? 0 : o) + kc * 128 + q * 8, o < 0 ? 0u : 16u);
+            } else {
+                const int rb = r - kGM;
+                const long long o = offB[rb];
+                tc::cp_async16(sa + 2 * kGTileA + (q >= 8 ? kGTileB : 0) + tc::sw128_offset(rb, q & 7),
+                               a.xs + (o < 0 ? 0 : o) + kc * 128 + q * 8, o < 0 ? 0u : 16u);
+            }
         }
     };
 
     const uint32_t idesc = tc::idesc_f16_f32(kGM, kGN, BF16);
     const int nk = a.nchunk;
+    double acc[32];
+#pragma unroll
+    for (int k = 0; k < 32; k++) acc[k] = 0.0;
+    auto absorb = [&](int kc) {
+        tc::tc_fence_after();
+        float v[16];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            tc::tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)((kc & 1) * kGN + ch * 32 + h * 16), v);
+#pragma unroll
+            for (int k = 0; k < 16; k++) acc[h * 16 + k] = __dadd_rn(acc[h * 16 + k], (double)v[k]);
+        }
+    };
     bool ok = true;
     for (int s = 0; s < kGStages - 1; s++) {
         if (s < nk) load(s, s);
@@ -115,62 +144,63 @@ __global__ void __launch_bounds__(128, 1) gram_split_kernel(GramArgs a)
     }
     for (int kc = 0; kc < nk; kc++) {
         const int s = kc % kGStages;
-        tc::cp_async_wait<kGStages - 2>();
+        // the MMAs of chunk kc-1 have read their stage and written their accumulator
+        bool w = true;
+        if (kc >= 1) w = tc::mbar_wait(&bars[(kc - 1) % kGStages], ((kc - 1) / kGStages) & 1);
+        if (w && kc + kGStages - 1 < nk) load((kc + kGStages - 1) % kGStages, kc + kGStages - 1);
+        tc::cp_async_commit();
+        tc::cp_async_wait<kGStages - 1>();
         tc::fence_async_smem();
-        __syncthreads();
+        ok = __syncthreads_and(w) != 0;
+        if (!ok) break;
         if (tid == 0) {
             tc::tc_fence_after();
             const uint32_t sa = base + s * kGStageBytes;
+            const uint32_t dst = tmem + (uint32_t)((kc & 1) * kGN);
 #pragma unroll
             for (int kk = 0; kk < 4; kk++) {
-                const uint64_t ahi = tc::sw128_desc(sa + kk * 32), alo = tc::sw128_desc(sa + kGTile + kk * 32);
-                const uint64_t bhi = tc::sw128_desc(sa + 2 * kGTile + kk * 32);
-                const uint64_t blo = tc::sw128_desc(sa + 3 * kGTile + kk * 32);
-                tc::mma_bf16(tmem, ahi, bhi, idesc, kc > 0 || kk > 0);
-                tc::mma_bf16(tmem, ahi, blo, idesc, true);
-                tc::mma_bf16(tmem, alo, bhi, idesc, true);
+                const uint64_t ahi = tc::sw128_desc(sa + kk * 32), alo = tc::sw128_desc(sa + kGTileA + kk * 32);
+                const uint64_t bhi = tc::sw128_desc(sa + 2 * kGTileA + kk * 32);
+                const uint64_t blo = tc::sw128_desc(sa + 2 * kGTileA + kGTileB + kk * 32);
+                tc::mma_bf16(dst, ahi, blo, idesc, kk > 0);
+                tc::mma_bf16(dst, alo, bhi, idesc, true);
+                tc::mma_bf16(dst, ahi, bhi, idesc, true);
             }
             tc::mma_commit(&bars[s]);
-            if (kc == nk - 1) tc::mma_commit(&bars[kGStages]);
         }
-        const int nxt = kc + kGStages - 1;
-        if (nxt < nk) {
-            // the stage of chunk nxt was last read by the MMAs of chunk kc-1
-            if (kc >= 1 && ok && !tc::mbar_wait(&bars[(kc - 1) % kGStages], ((kc - 1) / kGStages) & 1)) ok = false;
-            if (ok) load(nxt % kGStages, nxt);
+        if (kc >= 1) {
+            absorb(kc - 1);
+            tc::tc_fence_before();
         }
-        tc::cp_async_commit();
+        __syncthreads();
+    }
+    if (ok && nk > 0) {
+        ok = __syncthreads_and(tc::mbar_wait(&bars[(nk - 1) % kGStages], ((nk - 1) / kGStages) & 1)) != 0;
+        if (ok) absorb(nk - 1);
     }
     tc::cp_async_wait<0>();
-    if (nk > 0 && ok && !tc::mbar_wait(&bars[kGStages], 0)) ok = false;
-    if (!ok) atomicExch(a.err, 1);
-    tc::tc_fence_after();
+    if (!ok && tid == 0) atomicExch(a.err, 1);
 
-    // epilogue: warp w holds tile rows 32w..32w+31 (TMEM lanes), 16 columns per load
-    const int row = m0 + warp * 32 + lane;
-    const bool rok = ok && nk > 0 && row < a.ma;
-    const int ra = rok ? (a.ia ? a.ia[row] : row) : 0;
-    const double xa = rok ? a.xsq[ra] : 0.0;
-    const double sa_inv = (rok && a.xinv) ? a.xinv[ra] : 1.0;
-    for (int c0 = 0; c0 < kGN; c0 += 16) {
-        float v[16];
-        tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
-        if (rok) {
-            double *dst = a.out + (long long)row * a.ldo;
-#pragma unroll
-            for (int k = 0; k < 16; k++) {
-                const int col = n0 + c0 + k;
-                if (col < a.nb) {
-                    const int rb = a.ib ? a.ib[col] : col;
-                    const double sb_inv = a.xinv ? a.xinv[rb] : 1.0;
-                    dst[col] = kernel_from_dot(a.kp, __dmul_rn(__dmul_rn((double)v[k], sa_inv), sb_inv), xa, a.xsq[rb]);
-                }
+    // epilogue: this thread's row and 32 columns
+    const int row = m0 + lq * 32 + lane;
+    if (ok && nk > 0 && row < a.ma) {
+        const int ra = a.ia ? a.ia[row] : row;
+        const double xa = a.xsq[ra];
+        const double sa_inv = a.xinv ? a.xinv[ra] : 1.0;
+        double *dst = a.out + (long long)row * a.ldo;
+#pragma unroll 4
+        for (int k = 0; k < 32; k++) {
+            const int col = n0 + ch * 32 + k;
+            if (col < a.nb) {
+                const int rb = a.ib ? a.ib[col] : col;
+                const double sb_inv = a.xinv ? a.xinv[rb] : 1.0;
+                dst[col] = kernel_from_dot(a.kp, __dmul_rn(__dmul_rn(acc[k], sa_inv), sb_inv), xa, a.xsq[rb]);
             }
         }
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, kGN);
+    if (warp == 0) tc::tmem_dealloc(tmem, 2 * kGN);
 }
 
 // CUDA-core kernel block: one thread per output, 16 x 16 threads per CTA
@@ -334,8 +364,8 @@ cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, 
         a.out = d_out; a.ldo = ldo;
         a.err = d_err;
         dim3 grid((nb + kGN - 1) / kGN, (ma + kGM - 1) / kGM);
-        if (bf16) gram_split_kernel<true><<<grid, 128, kGSmem, s>>>(a);
-        else gram_split_kernel<false><<<grid, 128, kGSmem, s>>>(a);
+        if (bf16) gram_split_kernel<true><<<grid, kGThreads, kGSmem, s>>>(a);
+        else gram_split_kernel<false><<<grid, kGThreads, kGSmem, s>>>(a);
     } else {
         dim3 grid((nb + 15) / 16, (ma + 15) / 16), block(16, 16);
         if (form == FORM_EXACT)

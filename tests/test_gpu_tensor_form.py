@@ -117,3 +117,24 @@ def test_tensor_form_nu_and_batched(engine):
         a1, s1 = rows.solve_many([inst_rows[k]], [inst_y[k]], [prm[k]])
         assert np.array_equal(a1[0], al[k])
         assert s1[0]["iters"] == st[k]["iters"]
+
+
+@pytest.mark.parametrize("name", ["rbf_pixels", "multiclass_rbf", "poly_dense"])
+def test_tensor_form_prediction(engine, name):
+    """Decision values with K(test, SV) as tensor-core block products
+    (predict_form = SVMB_FORM_FP16X3) against the exact prediction path:
+    within 1e-6 of the largest decision value's magnitude, same labels."""
+    build, opts, _ = cases.CASES[name]
+    tr, te = build()
+    prm = param_from_opts(opts, max_index(tr))
+    model = engine.train(tr, prm)
+    lab0, dec0 = engine.predict(model, te)
+    engine.set_option("predict_form", FORM_FP16X3)
+    try:
+        lab1, dec1 = engine.predict(model, te)
+    finally:
+        engine.set_option("predict_form", 0)
+    scale = 1.0 + np.abs(dec0).max()
+    assert np.abs(dec1 - dec0).max() <= 1e-6 * scale
+    assert np.mean(lab1 == lab0) >= 0.99
+    model.free()
