@@ -384,7 +384,8 @@ def main():
         e1.record()
         barrier()
         step_ms.append(e0.elapsed_time(e1))
-        kern_s.append(stats[0]["seconds"])
+        # device time of the step's launches (instances of one launch share its time)
+        kern_s.append(sum({s["launch"]: s["seconds"] for s in stats}.values()))
         # algorithmic bytes of the launch: per iteration 46 B per active position
         # (WSS 22 B + update 24 B), per kernel value evaluated one stored row + 4 B
         row_bytes = res.bytes / max(res.n, 1)
@@ -450,6 +451,7 @@ def main():
     for _ in range(3):
         _, st = res.solve_many([rows[big]], [ys[big]], [params[big]])
         alone.append(st[0]["seconds"])
+    launches_per_step = len({s["launch"] for s in stats_all[-1]})
 
     if rank == 0:
         peak, peak_kind = load_peaks()
@@ -485,7 +487,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": int(launches),
-            "iters_total": int(sum(iters)), "iters_max": int(max(iters)),
+            "iters_total": int(sum(iters)), "iters_max": int(max(iters)), "solver_launches_per_step": launches_per_step,
             "largest_alone_ms": min(alone) * 1e3, "batched_over_largest": kavg / min(alone),
         }
         line.update(extras)

@@ -34,7 +34,7 @@ typedef struct svmb_solve_stats {
     int nr_bsv;
     int status;          /* 0 converged, 1 max_iter reached */
     int active_size;     /* active set size at exit (shrinking) */
-    int pad;
+    int launch;          /* index, within the call, of the persistent launch that solved it */
     double seconds;      /* device time (CUDA events) of the launch that solved it */
     /* work counters of the solve: sum over iterations of the active-set size,
      * kernel values evaluated, Q-row cache lookups and hits */

@@ -119,6 +119,7 @@ void finish_instance(const SubProblem &sp, const SolveResult &R, double *alpha_o
     st.status = R.out.status;
     st.active_size = R.out.active_size;
     st.seconds = R.seconds;
+    st.launch = R.wave;
     st.sum_active = R.out.sum_active;
     st.q_evals = R.out.q_evals;
     st.lookups = R.out.lookups;

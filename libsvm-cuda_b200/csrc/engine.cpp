@@ -17,6 +17,7 @@
 #include <atomic>
 #include <cstdlib>
 #include <mutex>
+#include <queue>
 
 #include "svm.h"
 
@@ -95,6 +96,8 @@ static bool trace_on()
     return on == 1;
 }
 struct StageClock {
+    explicit StageClock(const char *name = "solve_batch") : what(name) {}
+    const char *what;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now(), last = t0;
     std::string log;
     void mark(const char *what)
@@ -108,7 +111,7 @@ struct StageClock {
     }
     ~StageClock()
     {
-        if (trace_on() && !log.empty()) fprintf(stderr, "[svmb] solve_batch%s\n", log.c_str());
+        if (trace_on() && !log.empty()) fprintf(stderr, "[svmb] %s%s\n", what, log.c_str());
     }
 };
 
@@ -125,9 +128,44 @@ int device_sm_count()
     return sms;
 }
 
+// One grow-only device block reused by the row uploads of svm_train and
+// svm_cross_validation (allocating and freeing 100+ MB per call costs tens of
+// milliseconds); a second concurrent user gets a plain allocation.
+static std::mutex g_rowpool_mu;
+static char *g_rowpool = nullptr;
+static size_t g_rowpool_bytes = 0;
+static bool g_rowpool_busy = false;
+
+static char *rowpool_take(size_t bytes)
+{
+    std::lock_guard<std::mutex> g(g_rowpool_mu);
+    if (g_rowpool_busy) return nullptr;
+    if (bytes > g_rowpool_bytes) {
+        if (g_rowpool) cudaFree(g_rowpool);
+        g_rowpool = nullptr;
+        g_rowpool_bytes = 0;
+        const size_t want = bytes + bytes / 4;
+        if (cudaMalloc((void **)&g_rowpool, want) != cudaSuccess) {
+            cudaGetLastError();
+            g_rowpool = nullptr;
+            return nullptr;
+        }
+        g_rowpool_bytes = want;
+    }
+    g_rowpool_busy = true;
+    return g_rowpool;
+}
+
+static void rowpool_give(char *p)
+{
+    std::lock_guard<std::mutex> g(g_rowpool_mu);
+    if (p == g_rowpool) g_rowpool_busy = false;
+}
+
 DeviceRows::~DeviceRows()
 {
-    if (block && !block_async) cudaFree(block);
+    if (block && block_pooled) rowpool_give(block);
+    else if (block && !block_async) cudaFree(block);
     cudaFree(Xs);
     cudaFree(xinv);
 }
@@ -135,7 +173,8 @@ DeviceRows::~DeviceRows()
 void DeviceRows::release_async(cudaStream_t s)
 {
     if (block) {
-        if (block_async) cudaFreeAsync(block, s);
+        if (block_pooled) rowpool_give(block);
+        else if (block_async) cudaFreeAsync(block, s);
         else cudaFree(block);
     }
     block = nullptr;
@@ -195,8 +234,9 @@ DevX DeviceRows::view(int form) const
 }
 
 int upload_csr(const long long *rowptr, const int *col, const float *val, int n, int d, DeviceRows &out,
-               int force, cudaStream_t s, bool async_alloc)
+               int force, cudaStream_t s, int alloc)
 {
+    const bool async_alloc = alloc == kAllocAsync;
     out.n = n;
     out.d = d > 0 ? d : 1;
     const long long nnz = rowptr[n];
@@ -220,8 +260,12 @@ int upload_csr(const long long *rowptr, const int *col, const float *val, int n,
     const size_t b_sq = al(b_X + (dense ? std::max<size_t>((size_t)n * out.ld, 4) * sizeof(float) : 0));
     const size_t b_end = b_sq + 2 * al((size_t)std::max(n, 1) * sizeof(double));
     char *blk = nullptr;
-    if (async_alloc) CK(cudaMallocAsync((void **)&blk, b_end, s));
-    else CK(cudaMalloc((void **)&blk, b_end));
+    if (alloc == kAllocPooled) blk = rowpool_take(b_end);
+    out.block_pooled = blk != nullptr;
+    if (!blk) {
+        if (async_alloc) CK(cudaMallocAsync((void **)&blk, b_end, s));
+        else CK(cudaMalloc((void **)&blk, b_end));
+    }
     out.block = blk;
     out.block_async = async_alloc;
     out.block_bytes = b_end;
@@ -258,10 +302,11 @@ int upload_csr(const long long *rowptr, const int *col, const float *val, int n,
     return 0;
 }
 
-int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cudaStream_t s)
+int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cudaStream_t s, int alloc)
 {
     // CSR with 0-based columns; libsvm indices start at 1 (index 0 is kept as a
     // column when present).  Rows are converted in parallel on the host.
+    StageClock clk("upload_rows");
     std::vector<long long> cnt((size_t)n + 1, 0);
     int min_index = INT_MAX, max_index = 0;
 #pragma omp parallel for schedule(static) reduction(min : min_index) reduction(max : max_index)
@@ -303,7 +348,10 @@ int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cud
         }
     }
     const int d = nnz ? max_index - base + 1 : 1;
-    return upload_csr(rp, col, val, n, d, out, force, s);
+    clk.mark("convert");
+    const int rc = upload_csr(rp, col, val, n, d, out, force, s, alloc);
+    clk.mark("upload");
+    return rc;
 }
 
 namespace {
@@ -406,17 +454,18 @@ long long smem_budget()
 // shared-memory staging of one instance's rows: source rows staged in
 // float32 (CUDA-core forms) or the tensor-core operand stages
 struct StagePlan {
-    int stage_cap = 0, stage_lds = 0, tc_n = 0;
+    int stage_cap = 0, stage_lds = 0, tc_n = 0, tile_bufs = 2;
     long long bytes = 0;        // staging + aux area
     long long chunk_max = 0;    // positions of state one block can hold
 };
 
-StagePlan stage_plan(const DeviceRows &rows, int form, long long budget)
+StagePlan stage_plan(const DeviceRows &rows, int form, long long budget, int tile_bufs)
 {
     StagePlan p;
+    p.tile_bufs = tile_bufs;
     if (is_tc_form(form)) {
         p.tc_n = kTcMaxN;
-        while (p.tc_n > 16 && (budget - tc_area_bytes(p.tc_n) - kAuxBytes) / kChunkBytes < 1024) p.tc_n /= 2;
+        while (p.tc_n > 16 && (budget - tc_area_bytes(p.tc_n) - kAuxBytesTc) / kChunkBytes < 1024) p.tc_n /= 2;
         p.bytes = tc_area_bytes(p.tc_n);
     } else {
         if (rows.dense) {
@@ -429,7 +478,7 @@ StagePlan stage_plan(const DeviceRows &rows, int form, long long budget)
         if (p.stage_cap < 2) p.stage_cap = 0;
         p.bytes = (((long long)p.stage_cap * p.stage_lds * 4) + 15) & ~15LL;
     }
-    p.bytes += kAuxBytes;   // transpose tiles / prefetch candidates / block-product partial sums
+    p.bytes += aux_bytes(form, tile_bufs);   // transpose tiles / prefetch candidates / block-product partial sums
     p.chunk_max = (budget - p.bytes) / kChunkBytes;
     return p;
 }
@@ -454,76 +503,97 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
     const int sms = device_sm_count();
     std::vector<StagePlan> sp_all;
     std::vector<long long> nmin;
-    long long need = 0;
     int last = first;
-    while (last < ninst) {
-        const SubProblem &sp = subs[last];
-        const SolveParams &p = params_of(sp, prm);
-        if (p.form != prm.form) {
-            set_error("instances of one launch must share the arithmetic form");
-            return -1;
-        }
-        const StagePlan st = stage_plan(rows_of(sp, rows), prm.form, budget);
-        if (st.chunk_max < 64) {
-            set_error("not enough shared memory for the solver state");
-            return -1;
-        }
-        const long long l = (long long)sp.rows.size();
-        const long long nm = std::max<long long>(1, (l + st.chunk_max - 1) / st.chunk_max);
-        if (nm > capacity) {
-            if (last == first) {
-                set_error("problem too large: more positions than the device's blocks can hold in shared memory");
+    // the instances from `first` that one launch holds, with 2 or 1 transpose
+    // tiles per warp (two keep the next column slice in flight; one leaves
+    // more shared memory for state, so that more instances fit one launch)
+    auto fit = [&](int bufs, std::vector<StagePlan> &sps, std::vector<long long> &nms, int &end) -> int {
+        sps.clear();
+        nms.clear();
+        long long need = 0;
+        end = first;
+        while (end < ninst) {
+            const SubProblem &sp = subs[end];
+            const SolveParams &p = params_of(sp, prm);
+            if (p.form != prm.form) {
+                set_error("instances of one launch must share the arithmetic form");
                 return -1;
             }
-            break;
+            const StagePlan st = stage_plan(rows_of(sp, rows), prm.form, budget, bufs);
+            if (st.chunk_max < 64) {
+                set_error("not enough shared memory for the solver state");
+                return -1;
+            }
+            const long long l = (long long)sp.rows.size();
+            const long long nm = std::max<long long>(1, (l + st.chunk_max - 1) / st.chunk_max);
+            if (nm > capacity) {
+                if (end == first) {
+                    set_error("problem too large: more positions than the device's blocks can hold in shared memory");
+                    return -1;
+                }
+                break;
+            }
+            if (need + nm > capacity) break;
+            need += nm;
+            sps.push_back(st);
+            nms.push_back(nm);
+            end++;
         }
-        if (need + nm > capacity) break;
-        need += nm;
-        sp_all.push_back(st);
-        nmin.push_back(nm);
-        last++;
+        return 0;
+    };
+    if (fit(2, sp_all, nmin, last) != 0) return -1;
+    if (last < ninst && !is_tc_form(prm.form)) {
+        std::vector<StagePlan> sp1;
+        std::vector<long long> nm1;
+        int last1 = first;
+        if (fit(1, sp1, nm1, last1) != 0) return -1;
+        if (last1 > last) {
+            sp_all.swap(sp1);
+            nmin.swap(nm1);
+            last = last1;
+        }
     }
     const int count = last - first;
     w.count = count;
     w.nb.assign(count, 1);
-    // blocks per instance: enough to hold the state in shared memory, more for
-    // large problems; instances that run together share the device by l^2
-    // (the expected work: rows evaluated x row length), so that the largest
-    // instances, which bound the launch, get the most blocks
-    double total_w = 0;
-    for (int k = 0; k < count; k++) {
-        const double l = (double)subs[first + k].rows.size();
-        total_w += l * l;
-    }
+    // Blocks per instance: every instance starts with the blocks its state
+    // needs in shared memory; the remaining blocks go one at a time to the
+    // instance with the most positions per block, each up to min(SMs, l/500)
+    // (or its override).  The instances of a launch iterate about equally
+    // often, and an iteration's row evaluations take time in proportion to
+    // the positions per block, so equal chunks make the instances finish
+    // together; the l/500 cap keeps the cross-block exchanges of a small
+    // instance cheap.
+    std::vector<int> cap(count);
+    int used = 0;
     for (int k = 0; k < count; k++) {
         const SubProblem &sp = subs[first + k];
         const long long l = (long long)sp.rows.size();
         const int bo = params_of(sp, prm).blocks_override;
-        int want;
-        if (bo > 0) want = bo;
-        else want = (int)std::max<long long>(1, std::min<long long>(sms, (l + 499) / 500));
-        if (count > 1) {
-            const long long share = (long long)std::floor((double)capacity * (double)l * (double)l / std::max(total_w, 1.0));
-            want = (int)std::min<long long>(want, std::max<long long>(1, share));
-        }
-        want = (int)std::min<long long>(want, std::max<long long>(1, l));
-        want = std::min(want, std::min(kThreads, kMaxGroupBlocks));
-        w.nb[k] = std::max<int>(want, (int)nmin[k]);
+        long long want = bo > 0 ? bo : std::max<long long>(1, std::min<long long>(sms, (l + 499) / 500));
+        want = std::min<long long>(want, std::max<long long>(1, l));
+        want = std::min<long long>(want, std::min(kThreads, kMaxGroupBlocks));
+        w.nb[k] = (int)nmin[k];
+        cap[k] = (int)std::max<long long>(nmin[k], want);
+        used += w.nb[k];
     }
-    int used = 0;
-    for (int v : w.nb) used += v;
-    while (used > capacity) {
-        // trim the instance with the most blocks above its minimum
-        int big = -1;
-        long long slack = 0;
+    {
+        auto per_block = [&](int k) { return (double)subs[first + k].rows.size() / (double)w.nb[k]; };
+        auto cmp = [&](int a, int b) { return per_block(a) < per_block(b) || (per_block(a) == per_block(b) && a > b); };
+        std::priority_queue<int, std::vector<int>, decltype(cmp)> q(cmp);
         for (int k = 0; k < count; k++)
-            if (w.nb[k] - nmin[k] > slack) { slack = w.nb[k] - nmin[k]; big = k; }
-        if (big < 0) break;
-        w.nb[big]--;
-        used--;
+            if (w.nb[k] < cap[k]) q.push(k);
+        while (used < capacity && !q.empty()) {
+            const int k = q.top();
+            q.pop();
+            w.nb[k]++;
+            used++;
+            if (w.nb[k] < cap[k]) q.push(k);
+        }
     }
     w.used = used;
     w.stage.resize(count);
+    w.tile_bufs = count > 0 ? sp_all[0].tile_bufs : 2;
     long long dyn = 0;
     for (int k = 0; k < count; k++) {
         const long long l = (long long)subs[first + k].rows.size();
@@ -625,6 +695,7 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
         D.tc_n = w.stage[k][2];
         D.chunk_cap = w.stage[k][3];
         D.done_flag = w.done_flags ? w.done_flags + k : nullptr;
+        D.tile_bufs = w.tile_bufs;
         {
             const int limit = D.stage_cap > 0 ? std::min(kPrefetchMax, D.stage_cap) : kPrefetchMax;
             D.prefetch = p.prefetch > 0 ? std::min(p.prefetch, limit) : limit;
@@ -774,7 +845,7 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
     std::vector<SolveResult> sorted_res;
     std::vector<SolveResult> &out = order.empty() ? res : sorted_res;
     if (!order.empty()) sorted_res.assign(ninst, SolveResult());
-    int first = 0;
+    int first = 0, nwave = 0;
     while (first < ninst) {
         Wave w;
         if (wave_plan(rows, *plan, prm, first, capacity, w) != 0) return -1;
@@ -795,6 +866,8 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         clk.mark("launch");
         if (wave_finish(w, out) != 0) return -1;
         clk.mark("finish");
+        for (int k = 0; k < w.count; k++) out[first + k].wave = nwave;
+        nwave++;
         first += w.count;
     }
     for (size_t i = 0; i < order.size(); i++) res[order[i]] = std::move(sorted_res[i]);

@@ -28,10 +28,16 @@ constexpr int kPrefetchMax = 8;         // rows evaluated per fill pass (the mis
 constexpr int kNoTag = -1;
 constexpr int kMaxGroupBlocks = 160;     // blocks per instance (one per SM)
 constexpr int kTileStride = 20;         // floats per row of a warp's 32x16 transpose tile
-// shared memory shared by the transpose tiles and the prefetch candidate table
-constexpr int kTileBytes = kWarps * 32 * kTileStride * 4;
+// shared memory shared by the transpose tiles (two per warp: the next column
+// slice loads while the current one is used) and the prefetch candidate table
+constexpr int kTileBytes = kWarps * 32 * kTileStride * 4;      // one tile per warp
 constexpr int kCandBytes = kMaxGroupBlocks * kPrefetchCand * (8 + 4 * 4);
-constexpr int kAuxBytes = ((kTileBytes > kCandBytes ? kTileBytes : kCandBytes) + 15) / 16 * 16;
+constexpr int kAuxBytes = ((2 * kTileBytes > kCandBytes ? 2 * kTileBytes : kCandBytes) + 15) / 16 * 16;
+constexpr int kAuxBytes1 = ((kTileBytes > kCandBytes ? kTileBytes : kCandBytes) + 15) / 16 * 16;
+// tensor forms: no transpose tiles; candidates or the block-product partial sums
+constexpr int kRedBytes = 8 * 128 * 8;
+constexpr int kAuxBytesTc = ((kCandBytes > kRedBytes ? kCandBytes : kRedBytes) + 15) / 16 * 16;
+SVMB_HD constexpr int aux_bytes(int form, int tile_bufs) { return (form == 2 || form == 3) ? kAuxBytesTc : tile_bufs == 1 ? kAuxBytes1 : kAuxBytes; }
 
 // tensor-core (FORM_BF16X3) block products inside the solver
 constexpr int kTcM = 128;               // targets per tile (MMA M); rows are TMEM lanes
@@ -174,6 +180,7 @@ struct InstanceDesc {
     int lazy_gbar;
     int tc_n;                   // FORM_BF16X3: sources per tensor-core pass (16, 32 or 64); 0 otherwise
     int *done_flag;             // host-mapped word set to 1 once the whole instance has written its results, or nullptr
+    int tile_bufs;              // transpose tiles per warp in the CUDA-core fills (1 or 2; same in every instance of a launch)
 };
 
 }  // namespace svmb

@@ -36,6 +36,7 @@ struct DeviceRows {
     size_t h2d_bytes = 0;      // bytes copied from the host by the upload
     char *block = nullptr;     // one device block holding the rows and norms
     bool block_async = false;  // allocated stream-ordered (freed with release_async)
+    bool block_pooled = false; // the process's reusable row block (returned, not freed)
     size_t block_bytes = 0;
     ~DeviceRows();
     void release_async(cudaStream_t s);
@@ -46,12 +47,14 @@ struct DeviceRows {
 
 // Upload rows given as libsvm svm_node lists (index >= 1, terminated by -1).
 // force: -1 auto, 0 CSR, 1 dense.
-int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cudaStream_t s);
+int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cudaStream_t s, int alloc = 0);
 // Upload rows given as host CSR arrays (0-based columns).
-// With async_alloc the device block comes from the stream-ordered allocator
-// and the call does not wait for the upload (later work on s is ordered after it).
+// Where the device block of an upload comes from: cudaMalloc; the stream-ordered
+// allocator (the call then does not wait for the upload: later work on s is
+// ordered after it); or the process's reusable row block when it is free.
+enum { kAllocPlain = 0, kAllocAsync = 1, kAllocPooled = 2 };
 int upload_csr(const long long *rowptr, const int *col, const float *val, int n, int d, DeviceRows &out,
-               int force, cudaStream_t s, bool async_alloc = false);
+               int force, cudaStream_t s, int alloc = kAllocPlain);
 // device bytes of one instance's solver state (gradient, status, shrink lists, Q-row cache)
 size_t instance_bytes(int l, double cache_mb);
 
@@ -83,6 +86,7 @@ struct SolveResult {
     std::vector<double> alpha;      // by local index (unsigned)
     SolveOut out{};
     double seconds = 0;
+    int wave = 0;                   // index of the launch (within the call) that solved it
 };
 
 // The instances of one persistent launch ("wave"): block counts, shared
@@ -101,6 +105,7 @@ struct Wave {
     char *dev = nullptr, *host = nullptr;
     cudaStream_t stream = nullptr;
     bool cooperative = true;   // false: plain launch (the caller guarantees the blocks are co-resident)
+    int tile_bufs = 2;         // transpose tiles per warp of the CUDA-core fills
     int *done_flags = nullptr; // device view of host-mapped words, one per instance (nullptr: none)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
     float ms = 0;

@@ -116,7 +116,7 @@ extern "C" int svmb_solve_dense_noalloc(int n, int ld, const float *X, const dou
     int stage_cap = (int)std::min<long long>(kSrcBatch, (48LL << 10) / ((long long)ld * 4));
     if (stage_cap < 2) stage_cap = 0;
     long long stage_bytes = (((long long)stage_cap * ld * 4) + 15) & ~15LL;
-    stage_bytes += kAuxBytes;   // transpose tiles / prefetch candidates
+    stage_bytes += kAuxBytes;   // transpose tiles (two per warp) / prefetch candidates
     const long long chunk_max = (budget - stage_bytes) / kChunkBytes;
     if (chunk_max < 64) { set_error("not enough shared memory for the solver state"); return -1; }
     int nb = (int)std::max<long long>(1, std::min<long long>(sms, (n + 1499) / 1500));
@@ -204,6 +204,7 @@ extern "C" int svmb_solve_dense_noalloc(int n, int ld, const float *X, const dou
     D.lazy_gbar = 0;
     D.tc_n = 0;
     D.done_flag = nullptr;
+    D.tile_bufs = 2;
     int block_inst[kNoAllocMaxBlocks];
     for (int b = 0; b < nb; b++) block_inst[b] = 0;
 

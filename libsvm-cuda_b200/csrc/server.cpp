@@ -272,7 +272,7 @@ void Server::admit(Slot &slot, std::unique_lock<std::mutex> &lk)
     for (Job *j : take) {
         j->t_start = now;
         j->rows.reset(new DeviceRows());
-        if (upload_csr(j->rowptr.data(), j->col.data(), j->val.data(), j->n, j->d, *j->rows, -1, slot.stream, true) != 0 ||
+        if (upload_csr(j->rowptr.data(), j->col.data(), j->val.data(), j->n, j->d, *j->rows, -1, slot.stream, kAllocAsync) != 0 ||
             j->rows->prepare_form(j->prm.form, slot.stream) != 0) {
             ok = false;
             err = last_error();

@@ -1339,11 +1339,12 @@ __device__ void scan_iup(Ctx &c, Shared &sh)
     iup_publish(c, sh, v, ix, pv, pix);
 }
 
-// Dot products of the 32 rows of a warp (lane L owns row r) with ns <= 2
-// staged dense sources.  Each 32-float column slice of the 32 rows is loaded
-// with one coalesced 128-byte load per row into a padded 32x33 shared tile,
-// then every lane accumulates ITS row in feature order from the tile -- the
-// reference's summation order, with coalesced memory traffic.
+// Dot products of the 32 rows of a warp (lane L owns row r) with up to 8
+// staged dense sources.  The 32 rows are read in 16-column slices with
+// coalesced 64-byte pieces per row (cp.async, 16 bytes per lane) into a padded
+// 32 x 20 shared tile, two tiles per warp so that the next slice is in flight
+// while the current one is used; every lane accumulates ITS row in feature
+// order from the tile -- the reference's summation order.
 template <int FORM, int NS>
 __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const StageSlots &ss, int ns, int r, float *tile,
                                                double (&out)[kPrefetchMax])
@@ -1359,23 +1360,38 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
         acc[k] = acc_t(0);
         src[k] = ss.sp[k < ns ? k : 0];
     }
-    // 16-column slices: lanes 0-15 load row 2q, lanes 16-31 row 2q+1, 64
-    // contiguous bytes each; row t of the tile = the row of lane t
-    const int half = lane >> 4, cl = lane & 15;
-    for (int c0 = 0; c0 < ld; c0 += 16) {
-        const int col = c0 + cl;
-        float v[16];
+    // a slice is 32 rows x 4 pieces of 16 bytes; lane L moves pieces L + 32i
+    // (i < 4): row (L + 32i) / 4, piece L % 4.  Row t of a tile = the row of lane t.
+    const float *prow[4];
 #pragma unroll
-        for (int qq = 0; qq < 16; qq++) {
-            const int rq = __shfl_sync(0xffffffffu, r, 2 * qq + half);
-            v[qq] = col < ld ? __ldg(X + (long long)rq * ld + col) : 0.0f;
+    for (int i = 0; i < 4; i++) prow[i] = X + (long long)__shfl_sync(0xffffffffu, r, (lane + 32 * i) >> 2) * ld + 4 * (lane & 3);
+    const uint32_t tile_s = tc::smem_addr(tile);
+    auto issue = [&](int c0, int buf) {
+        if (c0 < ld) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int t = (lane + 32 * i) >> 2;
+                const bool ok = c0 + 4 * (lane & 3) < ld;     // ld is a multiple of 4
+                tc::cp_async16(tile_s + (uint32_t)((buf * 32 * kTileStride + t * kTileStride + 4 * (lane & 3)) * 4),
+                               prow[i] + (ok ? c0 : 0), ok ? 16u : 0u);
+            }
         }
-#pragma unroll
-        for (int qq = 0; qq < 16; qq++) tile[(2 * qq + half) * kTileStride + cl] = v[qq];
+        tc::cp_async_commit();
+    };
+    const bool two = D.tile_bufs == 2;
+    issue(0, 0);
+    for (int c0 = 0, s = 0; c0 < ld; c0 += 16) {
+        if (two) {
+            issue(c0 + 16, s ^ 1);
+            tc::cp_async_wait<1>();                      // this slice has landed (for this lane)
+        } else {
+            tc::cp_async_wait<0>();
+        }
         __syncwarp();
+        const float *cur = tile + s * 32 * kTileStride;
         const int lim = ld - c0 < 16 ? ld - c0 : 16;    // multiple of 4
         for (int q = 0; q < lim; q += 4) {
-            const float4 xv = *reinterpret_cast<const float4 *>(tile + lane * kTileStride + q);
+            const float4 xv = *reinterpret_cast<const float4 *>(cur + lane * kTileStride + q);
 #pragma unroll
             for (int k = 0; k < NS; k++) {
                 const float4 w = *reinterpret_cast<const float4 *>(src[k] + c0 + q);
@@ -1386,6 +1402,8 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
             }
         }
         __syncwarp();
+        if (two) s ^= 1;
+        else issue(c0 + 16, 0);
     }
 #pragma unroll
     for (int k = 0; k < NS; k++) out[k] = (double)acc[k];
@@ -1415,7 +1433,7 @@ __device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const 
     if (D.x.X && D.stage_cap > 0) {
         // dense rows, staged sources: warp-tiled, whole warps per 32 positions
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        float *tile = c.tile + warp * (32 * kTileStride);
+        float *tile = c.tile + warp * (D.tile_bufs * 32 * kTileStride);
         for (int base = lo + warp * 32; base < hi; base += blockDim.x) {
             const int k = base + lane;
             const bool valid = k < hi;
@@ -1510,7 +1528,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
         off = (off + 15) & ~(size_t)15;
         c.tile = reinterpret_cast<float *>(dyn + off);
         c.pt = reinterpret_cast<PrefetchTable *>(dyn + off);
-        off += kAuxBytes;
+        off += aux_bytes(FORM, D.tile_bufs);
         const size_t cap = (size_t)D.chunk_cap;
         c.sG = reinterpret_cast<double *>(dyn + off); off += cap * 8;
         c.sA = reinterpret_cast<double *>(dyn + off); off += cap * 8;

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <clocale>
 #include <cmath>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -212,6 +213,7 @@ DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResul
     st.status = R.out.status;
     st.active_size = R.out.active_size;
     st.seconds = R.seconds;
+    st.launch = R.wave;
     st.sum_active = R.out.sum_active;
     st.q_evals = R.out.q_evals;
     st.lookups = R.out.lookups;
@@ -418,7 +420,7 @@ int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, i
     if (!train_supported(param)) return -1;
     // all rows once, in the problem's order (row id = index in prob)
     svmb::DeviceRows rows;
-    if (l > 0 && svmb::upload_rows(prob->x, l, rows, svmb::api_force_layout(), 0) != 0) {
+    if (l > 0 && svmb::upload_rows(prob->x, l, rows, svmb::api_force_layout(), 0, svmb::kAllocPooled) != 0) {
         info("ERROR: %s\n", svmb::last_error());
         return -1;
     }
@@ -525,20 +527,33 @@ struct svm_model *svm_train(const struct svm_problem *prob, const struct svm_par
         g_last_stats.clear();
     }
     if (!train_supported(param)) return NULL;
+    const auto t0 = std::chrono::steady_clock::now();
     TrainJob tj;
     setup_train(prob, param, nullptr, tj);
+    const auto t1 = std::chrono::steady_clock::now();
     // rows are uploaded once, in grouped order; every pair addresses them by id
     svmb::DeviceRows rows;
-    if (tj.l > 0 && svmb::upload_rows(tj.x.data(), tj.l, rows, svmb::api_force_layout(), 0) != 0) {
+    if (tj.l > 0 && svmb::upload_rows(tj.x.data(), tj.l, rows, svmb::api_force_layout(), 0, svmb::kAllocPooled) != 0) {
         info("ERROR: %s\n", svmb::last_error());
         return NULL;
     }
+    const auto t2 = std::chrono::steady_clock::now();
     std::vector<svmb::SolveResult> res;
     if (!tj.subs.empty() && svmb::solve_batch(rows, tj.subs, make_solve_params(param), res, 0) != 0) {
         info("ERROR: %s\n", svmb::last_error());
         return NULL;
     }
-    return assemble_model(tj, res, 0);
+    const auto t3 = std::chrono::steady_clock::now();
+    svm_model *model = assemble_model(tj, res, 0);
+    if (getenv("SVMB_TRACE") && *getenv("SVMB_TRACE") == '1') {
+        const auto t4 = std::chrono::steady_clock::now();
+        auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        fprintf(stderr, "[svmb] svm_train setup=%.2fms upload=%.2fms solve=%.2fms assemble=%.2fms\n", ms(t0, t1), ms(t1, t2),
+                ms(t2, t3), ms(t3, t4));
+    }
+    return model;
 }
 
 void svm_cross_validation(const struct svm_problem *prob, const struct svm_parameter *param, int nr_fold, double *target)

@@ -25,13 +25,13 @@ class EngineError(RuntimeError):
 class SolveStats(C.Structure):
     _fields_ = [("iters", C.c_longlong), ("obj", C.c_double), ("rho", C.c_double), ("r", C.c_double),
                 ("l", C.c_int), ("nr_sv", C.c_int), ("nr_bsv", C.c_int), ("status", C.c_int),
-                ("active_size", C.c_int), ("pad", C.c_int), ("seconds", C.c_double),
+                ("active_size", C.c_int), ("launch", C.c_int), ("seconds", C.c_double),
                 ("sum_active", C.c_longlong), ("q_evals", C.c_longlong), ("lookups", C.c_longlong),
                 ("hits", C.c_longlong), ("fills", C.c_longlong), ("prefetched", C.c_longlong),
                 ("prefetch_used", C.c_longlong), ("prof_cycles", C.c_longlong * 8)]
 
     def as_dict(self) -> dict:
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("pad", "prof_cycles")}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "prof_cycles"}
         d["prof_cycles"] = list(self.prof_cycles)
         return d
 
