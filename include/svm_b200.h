@@ -93,10 +93,20 @@ int svmb_device_available(void);                /* 1 if a CUDA device can be use
  *   "blocks" thread blocks per solve (0 = automatic)
  *   "layout" -1 automatic, 0 CSR, 1 dense device layout of the rows
  *   "prefetch" kernel rows per cache-miss pass (1 = none, 0 = automatic)
+ *   "autotune" 1 (default): per workload signature (form, layout, width,
+ *            instance sizes) the first calls try fill depths and block targets
+ *            and later calls use the fastest; results never depend on them.
+ *            0: fixed rules.  Instances with their own prefetch or blocks are
+ *            never tuned.
  *   "predict_form" SVMB_FORM_EXACT (default: the reference's kernel values bit
  *            for bit) or a tensor-core form: svm_predict* and svmb_predict_batch
  *            then evaluate K(test rows, SVs) as block products on the tensor cores */
 int svmb_set_option(const char *name, long long value);
+
+/* The autotuner's configuration of the last batched solve of this process:
+ * rows per fill pass (0 = as deep as staging allows), positions per block
+ * aimed at, and whether it was an exploring call. */
+void svmb_autotune_last(int *prefetch, int *rows_per_block, int *exploring);
 
 /* Per-subproblem statistics of the last svm_train / svm_cross_validation
  * call on this process; returns the number of records (copies at most cap). */

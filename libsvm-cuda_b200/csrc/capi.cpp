@@ -242,6 +242,11 @@ int svmb_rows_solve_many(const svmb_rows *rows, int ninst, const int *inst_ptr, 
 
 void svmb_rows_free(svmb_rows *rows) { delete rows; }
 
+void svmb_autotune_last(int *prefetch, int *rows_per_block, int *exploring)
+{
+    svmb::autotune_last(prefetch, rows_per_block, exploring);
+}
+
 int svmb_rows_kernel_block(const svmb_rows *rows, const svmb_params *params, int ma, const int *ia, int nb,
                            const int *ib, double *out)
 {

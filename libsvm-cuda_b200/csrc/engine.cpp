@@ -16,7 +16,9 @@
 #include <cstring>
 #include <atomic>
 #include <cstdlib>
+#include <map>
 #include <mutex>
+#include <string>
 #include <queue>
 
 #include "svm.h"
@@ -492,7 +494,10 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
               int capacity, Wave &w)
 {
     const int ninst = (int)subs.size();
+    const int tune_pf = w.tune_prefetch, tune_rpb = w.tune_rows_per_block;
     w = Wave();
+    w.tune_prefetch = tune_pf;
+    w.tune_rows_per_block = tune_rpb;
     w.first = first;
     w.form = prm.form;
     const long long budget = smem_budget();
@@ -570,7 +575,8 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
         const SubProblem &sp = subs[first + k];
         const long long l = (long long)sp.rows.size();
         const int bo = params_of(sp, prm).blocks_override;
-        long long want = bo > 0 ? bo : std::max<long long>(1, std::min<long long>(sms, (l + 499) / 500));
+        const long long rpb = std::max(1, w.tune_rows_per_block);
+        long long want = bo > 0 ? bo : std::max<long long>(1, std::min<long long>(sms, (l + rpb - 1) / rpb));
         want = std::min<long long>(want, std::max<long long>(1, l));
         want = std::min<long long>(want, std::min(kThreads, kMaxGroupBlocks));
         w.nb[k] = (int)nmin[k];
@@ -698,7 +704,8 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
         D.tile_bufs = w.tile_bufs;
         {
             const int limit = D.stage_cap > 0 ? std::min(kPrefetchMax, D.stage_cap) : kPrefetchMax;
-            D.prefetch = p.prefetch > 0 ? std::min(p.prefetch, limit) : limit;
+            const int pf = w.tune_prefetch > 0 ? w.tune_prefetch : p.prefetch;
+            D.prefetch = pf > 0 ? std::min(pf, limit) : limit;
             D.lazy_gbar = p.lazy_gbar < 0 ? (is_tc_form(prm.form) ? 1 : 0) : p.lazy_gbar;
         }
         for (int b = 0; b < w.nb[k]; b++) h_bmap[b0 + b] = k;
@@ -799,6 +806,112 @@ int wave_finish(Wave &w, std::vector<SolveResult> &res)
     return rc;
 }
 
+// ---------------------------------------------------------------------------
+// autotuner
+// ---------------------------------------------------------------------------
+namespace {
+
+// knobs that change only speed: rows per fill pass (prefetch depth) and the
+// positions per block a solve aims at (its block count)
+constexpr int kTunePrefetch[] = {0, 4, 2, 1};         // 0: as deep as staging allows
+constexpr int kTuneRowsPerBlock[] = {500, 250, 1000};
+
+struct TuneState {
+    int stage = 0;          // 0: trying depths, 1: trying block targets, 2: settled
+    int idx = 0;            // candidate being tried in the current stage
+    int best_pf = 0, best_rpb = 500;
+    double best_ms = 1e300;
+};
+
+std::mutex g_tune_mu;
+std::map<std::string, TuneState> g_tune;
+int g_tune_on = 1;
+int g_last_pf = 0, g_last_rpb = 500, g_last_explore = 0;
+
+}  // namespace
+
+struct TuneChoice {
+    std::string key;
+    int prefetch = 0, rows_per_block = 500;
+    bool active = false;
+};
+
+// signature: form, layout, width, and the instances' sizes rounded to powers of two
+static std::string tune_key(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm)
+{
+    std::vector<int> b;
+    for (const SubProblem &sp : subs) {
+        int l = (int)sp.rows.size(), k = 0;
+        while ((1 << k) < l) k++;
+        b.push_back(k);
+    }
+    std::sort(b.begin(), b.end());
+    std::string key = std::to_string(prm.form) + ":" + std::to_string(rows.dense) + ":" + std::to_string(rows.d) + ":";
+    for (int v : b) key += std::to_string(v) + ",";
+    return key;
+}
+
+TuneChoice tune_pick(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, bool user_fixed)
+{
+    TuneChoice c;
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_last_explore = 0;
+    if (!g_tune_on || user_fixed) {
+        g_last_pf = 0;
+        g_last_rpb = 500;
+        return c;
+    }
+    c.key = tune_key(rows, subs, prm);
+    c.active = true;
+    TuneState &t = g_tune[c.key];
+    if (t.stage == 0) {
+        c.prefetch = kTunePrefetch[t.idx];
+        c.rows_per_block = 500;
+        g_last_explore = 1;
+    } else if (t.stage == 1) {
+        c.prefetch = t.best_pf;
+        c.rows_per_block = kTuneRowsPerBlock[t.idx];
+        g_last_explore = 1;
+    } else {
+        c.prefetch = t.best_pf;
+        c.rows_per_block = t.best_rpb;
+    }
+    g_last_pf = c.prefetch;
+    g_last_rpb = c.rows_per_block;
+    return c;
+}
+
+void tune_record(const TuneChoice &c, double ms)
+{
+    if (!c.active) return;
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    TuneState &t = g_tune[c.key];
+    if (t.stage == 2) return;
+    if (ms < t.best_ms) {
+        t.best_ms = ms;
+        t.best_pf = c.prefetch;
+        t.best_rpb = c.rows_per_block;
+    }
+    t.idx++;
+    const int n0 = (int)(sizeof(kTunePrefetch) / sizeof(int)), n1 = (int)(sizeof(kTuneRowsPerBlock) / sizeof(int));
+    if (t.stage == 0 && t.idx >= n0) { t.stage = 1; t.idx = 1; }      // 500 rows per block was measured in stage 0
+    else if (t.stage == 1 && t.idx >= n1) t.stage = 2;
+}
+
+void set_autotune(int on)
+{
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune_on = on ? 1 : 0;
+}
+
+void autotune_last(int *prefetch, int *rows_per_block, int *exploring)
+{
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    if (prefetch) *prefetch = g_last_pf;
+    if (rows_per_block) *rows_per_block = g_last_rpb;
+    if (exploring) *exploring = g_last_explore;
+}
+
 int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm,
                 std::vector<SolveResult> &res, cudaStream_t s)
 {
@@ -845,9 +958,19 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
     std::vector<SolveResult> sorted_res;
     std::vector<SolveResult> &out = order.empty() ? res : sorted_res;
     if (!order.empty()) sorted_res.assign(ninst, SolveResult());
+    // autotuner: the configuration for this call
+    bool user_fixed = false;
+    for (const SubProblem &sp : subs) {
+        const SolveParams &p = params_of(sp, prm);
+        if (p.prefetch > 0 || p.blocks_override > 0) user_fixed = true;
+    }
+    TuneChoice tune = tune_pick(rows, subs, prm, user_fixed);
+    double total_ms = 0;
     int first = 0, nwave = 0;
     while (first < ninst) {
         Wave w;
+        w.tune_prefetch = tune.prefetch;
+        w.tune_rows_per_block = tune.rows_per_block;
         if (wave_plan(rows, *plan, prm, first, capacity, w) != 0) return -1;
         clk.mark("plan");
         char *arena = arena_reserve(w.dev_bytes);
@@ -866,11 +989,13 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         clk.mark("launch");
         if (wave_finish(w, out) != 0) return -1;
         clk.mark("finish");
+        total_ms += w.ms;
         for (int k = 0; k < w.count; k++) out[first + k].wave = nwave;
         nwave++;
         first += w.count;
     }
     for (size_t i = 0; i < order.size(); i++) res[order[i]] = std::move(sorted_res[i]);
+    tune_record(tune, total_ms);
     return 0;
 }
 

@@ -105,6 +105,8 @@ struct Wave {
     char *dev = nullptr, *host = nullptr;
     cudaStream_t stream = nullptr;
     bool cooperative = true;   // false: plain launch (the caller guarantees the blocks are co-resident)
+    int tune_prefetch = 0;     // autotuner: rows per fill pass for every instance (0: the instances' own)
+    int tune_rows_per_block = 500;   // autotuner: positions per block a solve aims at (caps its blocks)
     int tile_bufs = 2;         // transpose tiles per warp of the CUDA-core fills
     int *done_flags = nullptr; // device view of host-mapped words, one per instance (nullptr: none)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
@@ -129,6 +131,13 @@ int wave_finish(Wave &w, std::vector<SolveResult> &res);
 // groups of blocks).  Returns 0 on success.
 int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm,
                 std::vector<SolveResult> &res, cudaStream_t s);
+
+// Autotuner of solve_batch (on by default): for each workload signature it
+// times the first calls with different fill depths and block targets, then
+// keeps the fastest.  Every configuration gives the same results.
+void set_autotune(int on);
+// the configuration chosen for the last solve_batch call (diagnostics)
+void autotune_last(int *prefetch, int *rows_per_block, int *exploring);
 
 int device_sm_count();
 void count_launch(long long n = 1);

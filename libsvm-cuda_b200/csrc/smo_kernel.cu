@@ -408,14 +408,29 @@ __device__ void cache_rotate(CacheState &cs, const CacheView &cv, int rank)
     cs.ncur = 0;
 }
 
+// a cache set's metadata as stored in global memory, copied into shared memory
+struct SetStage {
+    int set;
+    int tag[kMaxWays], ep[kMaxWays];
+    unsigned long long st[kMaxWays];
+};
+
 __device__ void cache_read_set(const CacheState &cs, const CacheView &cv, int set, int *tag, int *ep,
-                               unsigned long long *st)
+                               unsigned long long *st, const SetStage *pre = nullptr)
 {
-    for (int w = 0; w < cv.nways; w++) {
-        const long long s = (long long)set * cv.nways + w;
-        tag[w] = __ldcg(&cv.tag[s]);
-        ep[w] = __ldcg(&cv.epoch[s]);
-        st[w] = __ldcg(&cv.stamp[s]);
+    if (pre && pre->set == set) {
+        for (int w = 0; w < cv.nways; w++) {
+            tag[w] = pre->tag[w];
+            ep[w] = pre->ep[w];
+            st[w] = pre->st[w];
+        }
+    } else {
+        for (int w = 0; w < cv.nways; w++) {
+            const long long s = (long long)set * cv.nways + w;
+            tag[w] = __ldcg(&cv.tag[s]);
+            ep[w] = __ldcg(&cv.epoch[s]);
+            st[w] = __ldcg(&cv.stamp[s]);
+        }
     }
     for (int k = 0; k < cs.nprev; k++)
         if (cs.prev[k].set == set) {
@@ -439,12 +454,13 @@ __device__ void cache_read_set(const CacheState &cs, const CacheView &cv, int se
 // evictable ways, so that the rows the solver must place later always find
 // one; otherwise it returns slot -1.
 __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, int cur_epoch,
-                               unsigned long long clk, int whole, unsigned long long protect, int prefetch)
+                               unsigned long long clk, int whole, unsigned long long protect, int prefetch,
+                               const SetStage *pre = nullptr)
 {
     int tag[kMaxWays], ep[kMaxWays];
     unsigned long long st[kMaxWays];
     const int set = local % cv.nsets;
-    cache_read_set(cs, cv, set, tag, ep, st);
+    cache_read_set(cs, cv, set, tag, ep, st, pre);
     int way = -1;
     for (int w = 0; w < cv.nways; w++)
         if (tag[w] == local) way = w;
@@ -521,6 +537,7 @@ struct Shared {
     int nfill;
     int pick[kPrefetchMax];
     int npick;
+    SetStage sset[kPrefetchMax];    // cache sets of the prefetch picks, read in one round trip
     // tensor-core block products (FORM_BF16X3, FORM_FP16X3): sources of the current pass
     // (row id, position, alpha, norm, C, inverse scale, label, status), the
     // pipeline's mbarriers (one per operand stage) and the TMEM base address
@@ -1681,32 +1698,61 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 // the rows of the group's most violating positions (this only
                 // fills the cache; it never changes which pair is chosen)
                 if (sh.nfill > 0 && D.prefetch > sh.nfill) {
+                    // the `want` highest-priority candidates, chosen by warp 0: every
+                    // lane keeps its own best few, then the lanes' heads are merged
+                    // (the order of prefetched rows affects only what is cached)
                     const int ncand = c.nb * kPrefetchCand;
                     const int want = D.prefetch - sh.nfill;
-                    if (threadIdx.x == 0) sh.npick = 0;
-                    for (int round = 0; round < want; round++) {
-                        double bv[1] = {-SVMB_INF};
-                        int be[1] = {-1};
-                        const int kind1[1] = {0};
-                        for (int e = threadIdx.x; e < ncand; e += blockDim.x) {
+                    if (threadIdx.x < 32) {
+                        double lv[kPrefetchMax];
+                        int li[kPrefetchMax];
+                        int cnt = 0;
+                        for (int e = threadIdx.x; e < ncand; e += 32) {
                             const int pos = c.pt->pos[e];
-                            if (pos >= 0 && pos != i0_prev_guard(sh, 0) && pos != i0_prev_guard(sh, 1) && c.pt->v[e] > -SVMB_INF)
-                                better_max(bv[0], be[0], c.pt->v[e], e);
+                            const double v = c.pt->v[e];
+                            if (pos < 0 || pos == i0_prev_guard(sh, 0) || pos == i0_prev_guard(sh, 1) || !(v > -SVMB_INF)) continue;
+                            if (cnt == want && !(v > lv[cnt - 1])) continue;
+                            int q = cnt < want ? cnt++ : want - 1;     // insertion into the descending list
+                            while (q > 0 && lv[q - 1] < v) { lv[q] = lv[q - 1]; li[q] = li[q - 1]; q--; }
+                            lv[q] = v;
+                            li[q] = e;
                         }
-                        block_reduce<1>(sh.red, bv, be, kind1);
-                        if (be[0] < 0) break;
-                        if (threadIdx.x == 0) {
-                            sh.pick[sh.npick++] = be[0];
-                            c.pt->v[be[0]] = -SVMB_INF;
+                        int head = 0, got = 0;
+                        for (; got < want; got++) {
+                            double bv = head < cnt ? lv[head] : -SVMB_INF;
+                            int bl = head < cnt ? (int)threadIdx.x : 32;
+                            for (int o = 16; o > 0; o >>= 1) {
+                                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                                const int ol = __shfl_xor_sync(0xffffffffu, bl, o);
+                                if (ov > bv || (ov == bv && ol < bl)) { bv = ov; bl = ol; }
+                            }
+                            if (bl == 32) break;
+                            if ((int)threadIdx.x == bl) {
+                                sh.pick[got] = li[head];
+                                head++;
+                            }
                         }
-                        __syncthreads();
+                        if (threadIdx.x == 0) sh.npick = got;
+                    }
+                    __syncthreads();
+                    // the picks' cache sets, read by one thread per way in a single round trip
+                    if (threadIdx.x < sh.npick * kMaxWays) {
+                        const int t = threadIdx.x / kMaxWays, w = threadIdx.x % kMaxWays;
+                        const int set = c.pt->loc[sh.pick[t]] % D.cache.nsets;
+                        if (w == 0) sh.sset[t].set = set;
+                        if (w < D.cache.nways) {
+                            const long long s = (long long)set * D.cache.nways + w;
+                            sh.sset[t].tag[w] = __ldcg(&D.cache.tag[s]);
+                            sh.sset[t].ep[w] = __ldcg(&D.cache.epoch[s]);
+                            sh.sset[t].st[w] = __ldcg(&D.cache.stamp[s]);
+                        }
                     }
                     __syncthreads();
                     if (threadIdx.x == 0) {
                         const int whole = c.A == l;
                         for (int t = 0; t < sh.npick && sh.nfill < D.prefetch; t++) {
                             const int e = sh.pick[t];
-                            Lookup L = cache_lookup(sh.cs, D.cache, c.pt->loc[e], c.epoch, clkA, whole, clkA, 1);
+                            Lookup L = cache_lookup(sh.cs, D.cache, c.pt->loc[e], c.epoch, clkA, whole, clkA, 1, &sh.sset[t]);
                             if (L.slot >= 0 && !L.valid_active) {
                                 sh.frow[sh.nfill] = c.pt->row[e];
                                 sh.fy[sh.nfill] = c.pt->y[e];

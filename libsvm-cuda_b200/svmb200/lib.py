@@ -109,6 +109,7 @@ def _load(path: str) -> C.CDLL:
                                            C.c_void_p]
     lib.svmb_cross_validation_grid.argtypes = [_P(svm_problem), _P(svm_parameter), C.c_int, C.c_int, C.c_void_p,
                                                C.c_void_p, C.c_void_p]
+    lib.svmb_autotune_last.argtypes = [_P(C.c_int), _P(C.c_int), _P(C.c_int)]
     lib.svmb_server_create.argtypes = [_P(ServerConfig), _P(C.c_void_p)]
     lib.svmb_server_submit.restype = C.c_longlong
     lib.svmb_server_submit.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -200,6 +201,11 @@ class Engine:
         out = np.zeros(max(p.n, 1))
         self.lib.svm_cross_validation(C.byref(rows.prob), C.byref(param), nfold, out.ctypes.data_as(_P(C.c_double)))
         return out[:p.n]
+
+    def autotune_last(self) -> dict:
+        pf, rpb, ex = C.c_int(), C.c_int(), C.c_int()
+        self.lib.svmb_autotune_last(C.byref(pf), C.byref(rpb), C.byref(ex))
+        return {"prefetch": pf.value, "rows_per_block": rpb.value, "exploring": bool(ex.value)}
 
     def cross_validation_grid(self, p: CSR, param: svm_parameter, nfold: int, Cs, gammas) -> np.ndarray:
         """svmb_cross_validation_grid: predictions [npoints][n] of every (C, gamma) point."""
