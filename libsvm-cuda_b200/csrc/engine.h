@@ -27,7 +27,7 @@ constexpr int kPrefetchCand = 4;        // prefetch candidates published per blo
 constexpr int kPrefetchMax = 8;         // rows evaluated per fill pass (the missing row + prefetched)
 constexpr int kNoTag = -1;
 constexpr int kMaxGroupBlocks = 160;     // blocks per instance (one per SM)
-constexpr int kTileStride = 20;         // floats per row of a warp's 32x16 transpose tile
+constexpr int kTileStride = 16;         // floats per row of a warp's 32x16 transpose tile (16-byte pieces swizzled)
 // shared memory shared by the transpose tiles (two per warp: the next column
 // slice loads while the current one is used) and the prefetch candidate table
 constexpr int kTileBytes = kWarps * 32 * kTileStride * 4;      // one tile per warp

@@ -1358,8 +1358,8 @@ __device__ void scan_iup(Ctx &c, Shared &sh)
 
 // Dot products of the 32 rows of a warp (lane L owns row r) with up to 8
 // staged dense sources.  The 32 rows are read in 16-column slices with
-// coalesced 64-byte pieces per row (cp.async, 16 bytes per lane) into a padded
-// 32 x 20 shared tile, two tiles per warp so that the next slice is in flight
+// coalesced 64-byte pieces per row (cp.async, 16 bytes per lane) into a
+// 32 x 16 shared tile (pieces swizzled), two tiles per warp so that the next slice is in flight
 // while the current one is used; every lane accumulates ITS row in feature
 // order from the tile -- the reference's summation order.
 template <int FORM, int NS>
@@ -1389,7 +1389,9 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
             for (int i = 0; i < 4; i++) {
                 const int t = (lane + 32 * i) >> 2;
                 const bool ok = c0 + 4 * (lane & 3) < ld;     // ld is a multiple of 4
-                tc::cp_async16(tile_s + (uint32_t)((buf * 32 * kTileStride + t * kTileStride + 4 * (lane & 3)) * 4),
+                // piece c of tile row t sits at piece position c ^ ((t >> 1) & 3): the
+                // 16-byte reads of 8 consecutive lanes then hit distinct banks
+                tc::cp_async16(tile_s + (uint32_t)((buf * 32 * kTileStride + t * kTileStride + 4 * ((lane & 3) ^ ((t >> 1) & 3))) * 4),
                                prow[i] + (ok ? c0 : 0), ok ? 16u : 0u);
             }
         }
@@ -1408,7 +1410,7 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
         const float *cur = tile + s * 32 * kTileStride;
         const int lim = ld - c0 < 16 ? ld - c0 : 16;    // multiple of 4
         for (int q = 0; q < lim; q += 4) {
-            const float4 xv = *reinterpret_cast<const float4 *>(cur + lane * kTileStride + q);
+            const float4 xv = *reinterpret_cast<const float4 *>(cur + lane * kTileStride + 4 * ((q >> 2) ^ ((lane >> 1) & 3)));
 #pragma unroll
             for (int k = 0; k < NS; k++) {
                 const float4 w = *reinterpret_cast<const float4 *>(src[k] + c0 + q);
