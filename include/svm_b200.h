@@ -93,6 +93,7 @@ int svmb_device_available(void);                /* 1 if a CUDA device can be use
  *   "blocks" thread blocks per solve (0 = automatic)
  *   "layout" -1 automatic, 0 CSR, 1 dense device layout of the rows
  *   "prefetch" kernel rows per cache-miss pass (1 = none, 0 = automatic)
+ *   "graphs" 1 (default): repeated launches replay a captured CUDA graph; 0: plain stream work
  *   "autotune" 1 (default): per workload signature (form, layout, width,
  *            instance sizes) the first calls try fill depths and block targets
  *            and later calls use the fastest; results never depend on them.
@@ -107,6 +108,12 @@ int svmb_set_option(const char *name, long long value);
  * rows per fill pass (0 = as deep as staging allows), positions per block
  * aimed at, and whether it was an exploring call. */
 void svmb_autotune_last(int *prefetch, int *rows_per_block, int *exploring);
+
+/* CUDA graphs of the engine's batched launches: graphs captured and graph
+ * launches so far in this process.  A launch whose layout, device block and
+ * host staging repeat an earlier one's replays that launch's captured stream
+ * work (upload, fills, kernel, timing events, download). */
+void svmb_graph_counts(long long *captured, long long *replayed);
 
 /* Per-subproblem statistics of the last svm_train / svm_cross_validation
  * call on this process; returns the number of records (copies at most cap). */

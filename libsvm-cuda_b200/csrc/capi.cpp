@@ -247,6 +247,8 @@ void svmb_autotune_last(int *prefetch, int *rows_per_block, int *exploring)
     svmb::autotune_last(prefetch, rows_per_block, exploring);
 }
 
+void svmb_graph_counts(long long *captured, long long *replayed) { svmb::graph_counts(captured, replayed); }
+
 int svmb_rows_kernel_block(const svmb_rows *rows, const svmb_params *params, int ma, const int *ia, int nb,
                            const int *ib, double *out)
 {

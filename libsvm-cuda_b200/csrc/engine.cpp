@@ -41,6 +41,11 @@ const char *last_error() { return g_last_error.c_str(); }
 static std::atomic<long long> g_launches{0};
 static std::atomic<long long> g_h2d{0}, g_d2h{0};
 void count_launch(long long n) { g_launches += n; }
+void count_transfer(long long h2d, long long d2h)
+{
+    g_h2d += h2d;
+    g_d2h += d2h;
+}
 long long launch_count() { return g_launches.load(); }
 void transfer_bytes(long long *h2d, long long *d2h)
 {
@@ -661,6 +666,113 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
     return 0;
 }
 
+// The stream work of a wave: upload, fills, the launch between two timing
+// events, the result download, and the completion event.
+static cudaError_t wave_issue(Wave &w, InstanceDesc *d_desc, int *d_block_inst, cudaStream_t s)
+{
+    char *dev = w.dev, *host = w.host;
+    cudaError_t e = xfer_async(dev, host, w.up_bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dev + w.o_zero, 0, w.zero_bytes, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dev + w.o_tag, 0xff, w.tag_bytes, s);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.ev0, s, cudaEventRecordExternal);
+    if (e == cudaSuccess) e = launch_smo(w.form, d_desc, d_block_inst, w.used, w.dyn_smem, w.cooperative, s);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.ev1, s, cudaEventRecordExternal);
+    if (e == cudaSuccess) e = xfer_async(host + w.up_bytes, dev + w.o_out, w.down_bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.done, s, cudaEventRecordExternal);
+    return e;
+}
+
+// ---- CUDA graphs of repeated waves ----------------------------------------
+// A wave whose layout, device block and host staging are the same as an
+// earlier one (the arena and the staging are reused) replays a graph of its
+// stream work captured the first time: one graph launch instead of seven
+// stream operations.  The graph owns its timing and completion events.
+namespace {
+struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
+    bool failed = false;
+};
+std::map<std::string, GraphEntry> g_graphs;     // guarded by the arena lock of solve_batch
+std::atomic<long long> g_graph_captured{0}, g_graph_replayed{0};
+
+std::string graph_key(const Wave &w)
+{
+    char buf[512];
+    snprintf(buf, sizeof buf, "%p:%p:%zu:%zu:%zu:%zu:%zu:%zu:%zu:%d:%zu:%d:%d", (void *)w.dev, (void *)w.host, w.up_bytes,
+             w.down_bytes, w.zero_bytes, w.tag_bytes, w.o_zero, w.o_tag, w.o_out, w.used, w.dyn_smem, w.form,
+             (int)w.cooperative);
+    return std::string(buf) + ":" + std::to_string(w.o_desc) + ":" + std::to_string(w.o_bmap);
+}
+}  // namespace
+
+void graph_counts(long long *captured, long long *replayed)
+{
+    if (captured) *captured = g_graph_captured.load();
+    if (replayed) *replayed = g_graph_replayed.load();
+}
+
+static int wave_issue_graph(Wave &w, InstanceDesc *d_desc, int *d_block_inst, cudaStream_t s)
+{
+    const std::string key = graph_key(w);
+    if (g_graphs.size() > 64) {
+        for (auto &kv : g_graphs) {
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+            if (kv.second.ev0) cudaEventDestroy(kv.second.ev0);
+            if (kv.second.ev1) cudaEventDestroy(kv.second.ev1);
+            if (kv.second.done) cudaEventDestroy(kv.second.done);
+        }
+        g_graphs.clear();
+    }
+    GraphEntry &ge = g_graphs[key];
+    if (!ge.ev0) {
+        CK(cudaEventCreate(&ge.ev0));
+        CK(cudaEventCreate(&ge.ev1));
+        CK(cudaEventCreateWithFlags(&ge.done, cudaEventDisableTiming));
+    }
+    w.ev0 = ge.ev0;
+    w.ev1 = ge.ev1;
+    w.done = ge.done;
+    w.own_events = false;
+    if (!ge.exec && !ge.failed) {
+        // capture once; a stream work that cannot be captured runs directly from then on
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            const cudaError_t ie = wave_issue(w, d_desc, d_block_inst, s);
+            e = cudaStreamEndCapture(s, &graph);
+            if (ie != cudaSuccess) e = ie;
+            // captured copies did not run: take back the bytes xfer_async counted
+            count_transfer(-(long long)w.up_bytes, -(long long)w.down_bytes);
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ge.exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (trace_on()) fprintf(stderr, "[svmb] graph capture: %s\n", cudaGetErrorString(e));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ge.exec = nullptr;
+            ge.failed = true;
+        } else {
+            g_graph_captured++;
+        }
+    }
+    if (ge.exec) {
+        // the captured copies do not pass through xfer_async: count their bytes here
+        count_transfer((long long)w.up_bytes, (long long)w.down_bytes);
+        CK(cudaGraphLaunch(ge.exec, s));
+        g_graph_replayed++;
+    } else {
+        cudaGetLastError();
+        cudaError_t le = wave_issue(w, d_desc, d_block_inst, s);
+        if (le != cudaSuccess) {
+            set_error(std::string("solver launch (after a graph capture that failed) failed: ") + cudaGetErrorString(le));
+            return -1;
+        }
+    }
+    count_launch();
+    return 0;
+}
+
 int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, Wave &w,
                char *dev, char *host, cudaStream_t s)
 {
@@ -739,22 +851,17 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
         memcpy(h_row + w.loff[k], sp.rows.data(), sizeof(int) * l);
         memcpy(h_y + w.loff[k], sp.y.data(), (size_t)l);
     }
-    CK(xfer_async(dev, host, w.up_bytes, cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(dev + w.o_zero, 0, w.zero_bytes, s));
-    CK(cudaMemsetAsync(dev + w.o_tag, 0xff, w.tag_bytes, s));
+    if (w.use_graph) return wave_issue_graph(w, d_desc, d_block_inst, s);
     CK(cudaEventCreate(&w.ev0));
     CK(cudaEventCreate(&w.ev1));
-    CK(cudaEventRecord(w.ev0, s));
-    cudaError_t le = launch_smo(w.form, d_desc, d_block_inst, w.used, w.dyn_smem, w.cooperative, s);
-    if (le == cudaSuccess) count_launch();
-    cudaEventRecord(w.ev1, s);
-    if (le == cudaSuccess) le = xfer_async(host + w.up_bytes, dev + w.o_out, w.down_bytes, cudaMemcpyDeviceToHost, s);
+    CK(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming));
+    w.own_events = true;
+    cudaError_t le = wave_issue(w, d_desc, d_block_inst, s);
     if (le != cudaSuccess) {
         set_error(std::string("solver launch failed: ") + cudaGetErrorString(le));
         return -1;
     }
-    CK(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming));
-    CK(cudaEventRecord(w.done, s));
+    count_launch();
     return 0;
 }
 
@@ -780,9 +887,11 @@ int wave_finish(Wave &w, std::vector<SolveResult> &res)
     cudaError_t se = w.done ? cudaEventSynchronize(w.done) : cudaErrorInvalidResourceHandle;
     float ms = 0;
     if (se == cudaSuccess) se = cudaEventElapsedTime(&ms, w.ev0, w.ev1);
-    if (w.ev0) cudaEventDestroy(w.ev0);
-    if (w.ev1) cudaEventDestroy(w.ev1);
-    if (w.done) cudaEventDestroy(w.done);
+    if (w.own_events) {
+        if (w.ev0) cudaEventDestroy(w.ev0);
+        if (w.ev1) cudaEventDestroy(w.ev1);
+        if (w.done) cudaEventDestroy(w.done);
+    }
     w.ev0 = w.ev1 = w.done = nullptr;
     if (se != cudaSuccess) {
         set_error(std::string("solver launch failed: ") + cudaGetErrorString(se));
@@ -912,6 +1021,23 @@ void autotune_last(int *prefetch, int *rows_per_block, int *exploring)
     if (exploring) *exploring = g_last_explore;
 }
 
+static int g_graphs_on = 1;
+void set_graphs(int on) { g_graphs_on = on ? 1 : 0; }
+
+// one non-blocking stream per device for the waves of solve_batch
+static cudaStream_t solver_stream()
+{
+    static std::map<int, cudaStream_t> streams;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    auto it = streams.find(dev);
+    if (it != streams.end()) return it->second;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    streams[dev] = st;
+    return st;
+}
+
 int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm,
                 std::vector<SolveResult> &res, cudaStream_t s)
 {
@@ -924,6 +1050,10 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         if (sp.rows_dev && const_cast<DeviceRows *>(sp.rows_dev)->prepare_form(prm.form, s) != 0) return -1;
     std::lock_guard<std::mutex> arena_lock(g_arena_mu);
     StageClock clk;
+    // the waves run on the engine's own non-blocking stream (a capturable one);
+    // everything they read was uploaded and synchronised before this call
+    cudaStream_t ws = solver_stream();
+    if (!ws) ws = s;
     const int sms = device_sm_count();
     if (sms <= 0) {
         set_error("no CUDA device");
@@ -985,7 +1115,8 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
             host = host_fallback.data();
         }
         clk.mark("arena");
-        if (wave_start(rows, *plan, prm, w, arena, host, s) != 0) return -1;
+        w.use_graph = g_graphs_on && host != host_fallback.data();
+        if (wave_start(rows, *plan, prm, w, arena, host, ws) != 0) return -1;
         clk.mark("launch");
         if (wave_finish(w, out) != 0) return -1;
         clk.mark("finish");

@@ -105,6 +105,8 @@ struct Wave {
     char *dev = nullptr, *host = nullptr;
     cudaStream_t stream = nullptr;
     bool cooperative = true;   // false: plain launch (the caller guarantees the blocks are co-resident)
+    bool use_graph = false;    // replay a captured graph of the stream work when the layout repeats
+    bool own_events = true;    // the events belong to this wave (not to a cached graph)
     int tune_prefetch = 0;     // autotuner: rows per fill pass for every instance (0: the instances' own)
     int tune_rows_per_block = 500;   // autotuner: positions per block a solve aims at (caps its blocks)
     int tile_bufs = 2;         // transpose tiles per warp of the CUDA-core fills
@@ -141,6 +143,10 @@ void autotune_last(int *prefetch, int *rows_per_block, int *exploring);
 
 int device_sm_count();
 void count_launch(long long n = 1);
+void count_transfer(long long h2d, long long d2h);
+// CUDA graphs of repeated waves in solve_batch (on by default)
+void set_graphs(int on);
+void graph_counts(long long *captured, long long *replayed);
 void transfer_bytes(long long *h2d, long long *d2h);
 cudaError_t xfer_async(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
 cudaError_t xfer(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind);

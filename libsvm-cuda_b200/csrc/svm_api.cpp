@@ -497,6 +497,8 @@ int api_set_option(const char *name, long long value)
         g_opt.blocks = (int)value;
     } else if (!strcmp(name, "layout")) {
         g_opt.force_layout = (int)value;
+    } else if (!strcmp(name, "graphs")) {
+        set_graphs((int)value);
     } else if (!strcmp(name, "autotune")) {
         set_autotune((int)value);
     } else if (!strcmp(name, "predict_form")) {

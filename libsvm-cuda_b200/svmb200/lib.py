@@ -110,6 +110,7 @@ def _load(path: str) -> C.CDLL:
     lib.svmb_cross_validation_grid.argtypes = [_P(svm_problem), _P(svm_parameter), C.c_int, C.c_int, C.c_void_p,
                                                C.c_void_p, C.c_void_p]
     lib.svmb_autotune_last.argtypes = [_P(C.c_int), _P(C.c_int), _P(C.c_int)]
+    lib.svmb_graph_counts.argtypes = [_P(C.c_longlong), _P(C.c_longlong)]
     lib.svmb_server_create.argtypes = [_P(ServerConfig), _P(C.c_void_p)]
     lib.svmb_server_submit.restype = C.c_longlong
     lib.svmb_server_submit.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -201,6 +202,11 @@ class Engine:
         out = np.zeros(max(p.n, 1))
         self.lib.svm_cross_validation(C.byref(rows.prob), C.byref(param), nfold, out.ctypes.data_as(_P(C.c_double)))
         return out[:p.n]
+
+    def graph_counts(self) -> dict:
+        a, b = C.c_longlong(), C.c_longlong()
+        self.lib.svmb_graph_counts(C.byref(a), C.byref(b))
+        return {"captured": a.value, "replayed": b.value}
 
     def autotune_last(self) -> dict:
         pf, rpb, ex = C.c_int(), C.c_int(), C.c_int()
