@@ -483,7 +483,9 @@ StagePlan stage_plan(const DeviceRows &rows, int form, long long budget, int til
             p.stage_cap = (int)std::min<long long>(kSrcBatch, (budget / 2) / ((long long)std::max(rows.d, 1) * 4));
         }
         if (p.stage_cap < 2) p.stage_cap = 0;
-        p.bytes = (((long long)p.stage_cap * p.stage_lds * 4) + 15) & ~15LL;
+        // the exact form stages its source values as float64
+        const long long elem = form == FORM_EXACT ? 8 : 4;
+        p.bytes = (((long long)p.stage_cap * p.stage_lds * elem) + 15) & ~15LL;
     }
     p.bytes += aux_bytes(form, tile_bufs);   // transpose tiles / prefetch candidates / block-product partial sums
     p.chunk_max = (budget - p.bytes) / kChunkBytes;
@@ -668,17 +670,18 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
 
 // The stream work of a wave: upload, fills, the launch between two timing
 // events, the result download, and the completion event.
-static cudaError_t wave_issue(Wave &w, InstanceDesc *d_desc, int *d_block_inst, cudaStream_t s)
+static cudaError_t wave_issue(Wave &w, InstanceDesc *d_desc, int *d_block_inst, cudaStream_t s, bool capturing = false)
 {
+    const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     char *dev = w.dev, *host = w.host;
     cudaError_t e = xfer_async(dev, host, w.up_bytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(dev + w.o_zero, 0, w.zero_bytes, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(dev + w.o_tag, 0xff, w.tag_bytes, s);
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.ev0, s, cudaEventRecordExternal);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.ev0, s, rec);
     if (e == cudaSuccess) e = launch_smo(w.form, d_desc, d_block_inst, w.used, w.dyn_smem, w.cooperative, s);
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.ev1, s, cudaEventRecordExternal);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.ev1, s, rec);
     if (e == cudaSuccess) e = xfer_async(host + w.up_bytes, dev + w.o_out, w.down_bytes, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.done, s, cudaEventRecordExternal);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.done, s, rec);
     return e;
 }
 
@@ -739,7 +742,7 @@ static int wave_issue_graph(Wave &w, InstanceDesc *d_desc, int *d_block_inst, cu
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            const cudaError_t ie = wave_issue(w, d_desc, d_block_inst, s);
+            const cudaError_t ie = wave_issue(w, d_desc, d_block_inst, s, true);
             e = cudaStreamEndCapture(s, &graph);
             if (ie != cudaSuccess) e = ie;
             // captured copies did not run: take back the bytes xfer_async counted

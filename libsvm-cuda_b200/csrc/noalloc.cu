@@ -115,7 +115,9 @@ extern "C" int svmb_solve_dense_noalloc(int n, int ld, const float *X, const dou
     const long long budget = (long long)smem_total - smo_static_smem() - 1024;
     int stage_cap = (int)std::min<long long>(kSrcBatch, (48LL << 10) / ((long long)ld * 4));
     if (stage_cap < 2) stage_cap = 0;
-    long long stage_bytes = (((long long)stage_cap * ld * 4) + 15) & ~15LL;
+    // staged source values are float64 in the exact form
+    const int elem = params->form == SVMB_FORM_EXACT ? 8 : 4;
+    long long stage_bytes = (((long long)stage_cap * ld * elem) + 15) & ~15LL;
     stage_bytes += kAuxBytes;   // transpose tiles (two per warp) / prefetch candidates
     const long long chunk_max = (budget - stage_bytes) / kChunkBytes;
     if (chunk_max < 64) { set_error("not enough shared memory for the solver state"); return -1; }

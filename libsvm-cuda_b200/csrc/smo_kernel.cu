@@ -77,22 +77,42 @@ __device__ __forceinline__ int ld_relaxed_i32(const int *p)
 // instance's stage_cap > 0 (dense rows copied; sparse rows scattered into
 // zeroed dense vectors), otherwise read from global memory (dense) or merged
 // against the target's CSR row (sparse).  `sp[k]` points at source k.
+// The exact form stages its sources as float64 (`dbl`): a float -> double
+// conversion per use would otherwise outnumber the float64 multiply-adds
+// (conversions issue at a quarter of their rate), and the value is the same.
 struct StageSlots {
-    const float *sp[kSrcBatch];
+    const void *sp[kSrcBatch];
     int rows[kSrcBatch];
     int ns;
+    int dbl;
 };
+
+// bytes of one staged value in the form
+__host__ __device__ constexpr int stage_elem(int form) { return form == FORM_EXACT ? 8 : 4; }
 
 __device__ void stage_sources(const InstanceDesc &D, float *stage, StageSlots &ss, const int *rows, int ns)
 {
     const DevX &x = D.x;
+    const bool dbl = D.form == FORM_EXACT && D.stage_cap > 0;
+    double *stage_d = reinterpret_cast<double *>(stage);
     if (threadIdx.x < ns) ss.rows[threadIdx.x] = rows[threadIdx.x];
-    if (threadIdx.x == 0) ss.ns = ns;
+    if (threadIdx.x == 0) {
+        ss.ns = ns;
+        ss.dbl = dbl ? 1 : 0;
+    }
     if (x.X) {
         const int ld4 = x.ld >> 2;
         for (int k = 0; k < ns; k++) {
             const float4 *src = reinterpret_cast<const float4 *>(x.X + (long long)rows[k] * x.ld);
-            if (D.stage_cap > 0) {
+            if (dbl) {
+                double2 *dst = reinterpret_cast<double2 *>(stage_d + (long long)k * D.stage_lds);
+                for (int t = threadIdx.x; t < ld4; t += blockDim.x) {
+                    const float4 v = __ldg(src + t);
+                    dst[2 * t] = make_double2((double)v.x, (double)v.y);
+                    dst[2 * t + 1] = make_double2((double)v.z, (double)v.w);
+                }
+                if (threadIdx.x == 0) ss.sp[k] = stage_d + (long long)k * D.stage_lds;
+            } else if (D.stage_cap > 0) {
                 float4 *dst = reinterpret_cast<float4 *>(stage + (long long)k * D.stage_lds);
                 for (int t = threadIdx.x; t < ld4; t += blockDim.x) dst[t] = __ldg(src + t);
                 if (threadIdx.x == 0) ss.sp[k] = stage + (long long)k * D.stage_lds;
@@ -103,9 +123,15 @@ __device__ void stage_sources(const InstanceDesc &D, float *stage, StageSlots &s
     } else if (D.stage_cap > 0) {
         for (int k = 0; k < ns; k++) {
             const long long a = x.rowptr[rows[k]], b = x.rowptr[rows[k] + 1];
-            float *dst = stage + (long long)k * D.stage_lds;
-            for (long long e = a + threadIdx.x; e < b; e += blockDim.x) dst[x.col[e]] = x.val[e];
-            if (threadIdx.x == 0) ss.sp[k] = dst;
+            if (dbl) {
+                double *dst = stage_d + (long long)k * D.stage_lds;
+                for (long long e = a + threadIdx.x; e < b; e += blockDim.x) dst[x.col[e]] = (double)x.val[e];
+                if (threadIdx.x == 0) ss.sp[k] = dst;
+            } else {
+                float *dst = stage + (long long)k * D.stage_lds;
+                for (long long e = a + threadIdx.x; e < b; e += blockDim.x) dst[x.col[e]] = x.val[e];
+                if (threadIdx.x == 0) ss.sp[k] = dst;
+            }
         }
     }
     __syncthreads();
@@ -119,8 +145,13 @@ __device__ void unstage_sources(const InstanceDesc &D, float *stage, StageSlots 
     if (!x.X && D.stage_cap > 0) {
         for (int k = 0; k < ss.ns; k++) {
             const long long a = x.rowptr[ss.rows[k]], b = x.rowptr[ss.rows[k] + 1];
-            float *dst = stage + (long long)k * D.stage_lds;
-            for (long long e = a + threadIdx.x; e < b; e += blockDim.x) dst[x.col[e]] = 0.0f;
+            if (ss.dbl) {
+                double *dst = reinterpret_cast<double *>(stage) + (long long)k * D.stage_lds;
+                for (long long e = a + threadIdx.x; e < b; e += blockDim.x) dst[x.col[e]] = 0.0;
+            } else {
+                float *dst = stage + (long long)k * D.stage_lds;
+                for (long long e = a + threadIdx.x; e < b; e += blockDim.x) dst[x.col[e]] = 0.0f;
+            }
         }
     }
     __syncthreads();
@@ -137,12 +168,27 @@ __device__ __forceinline__ typename Acc<FORM>::type mac(float a, float b, typena
     if (FORM == FORM_EXACT) return fma((double)a, (double)b, (double)acc);
     return fmaf(a, b, (float)acc);
 }
+// a source staged as float64 (exact form): only the target value is converted
+template <int FORM>
+__device__ __forceinline__ typename Acc<FORM>::type mac(float a, double b, typename Acc<FORM>::type acc)
+{
+    return fma((double)a, b, (double)acc);
+}
+
+// four staged source values starting at feature 4*i: float4 or two double2
+__device__ __forceinline__ float4 src4(const float *p, int i) { return reinterpret_cast<const float4 *>(p)[i]; }
+struct D4 { double x, y, z, w; };
+__device__ __forceinline__ D4 src4(const double *p, int i)
+{
+    const double2 a = reinterpret_cast<const double2 *>(p)[2 * i], b = reinterpret_cast<const double2 *>(p)[2 * i + 1];
+    return D4{a.x, a.y, b.x, b.y};
+}
 
 // Dot products of target row `r` with NS staged sources, accumulated in
 // feature order (the order of the reference's Kernel::dot, svm.cpp:305-325:
 // only matching indices contribute; zero products leave the sum unchanged).
 // Dense rows are streamed 8 x 16 bytes at a time per thread.
-template <int FORM, int NS>
+template <int FORM, int NS, typename S>
 __device__ __forceinline__ void row_dots_n(const InstanceDesc &D, const StageSlots &ss, int ns, int r,
                                            double (&out)[kSrcBatch])
 {
@@ -153,9 +199,9 @@ __device__ __forceinline__ void row_dots_n(const InstanceDesc &D, const StageSlo
     for (int k = 0; k < NS; k++) acc[k] = acc_t(0);
     if (x.X) {
         const float4 *row = reinterpret_cast<const float4 *>(x.X + (long long)r * x.ld);
-        const float4 *src[NS];
+        const S *src[NS];
 #pragma unroll
-        for (int k = 0; k < NS; k++) src[k] = reinterpret_cast<const float4 *>(ss.sp[k < ns ? k : 0]);
+        for (int k = 0; k < NS; k++) src[k] = reinterpret_cast<const S *>(ss.sp[k < ns ? k : 0]);
         const int ld4 = x.ld >> 2;
         int c = 0;
         for (; c + 8 <= ld4; c += 8) {
@@ -167,7 +213,7 @@ __device__ __forceinline__ void row_dots_n(const InstanceDesc &D, const StageSlo
 #pragma unroll
                 for (int k = 0; k < NS; k++) {
                     if (NS == kSrcBatch && k >= ns) continue;
-                    const float4 w = src[k][c + u];
+                    const auto w = src4(src[k], c + u);
                     acc[k] = mac<FORM>(v[u].x, w.x, acc[k]);
                     acc[k] = mac<FORM>(v[u].y, w.y, acc[k]);
                     acc[k] = mac<FORM>(v[u].z, w.z, acc[k]);
@@ -180,7 +226,7 @@ __device__ __forceinline__ void row_dots_n(const InstanceDesc &D, const StageSlo
 #pragma unroll
             for (int k = 0; k < NS; k++) {
                 if (NS == kSrcBatch && k >= ns) continue;
-                const float4 w = src[k][c];
+                const auto w = src4(src[k], c);
                 acc[k] = mac<FORM>(v.x, w.x, acc[k]);
                 acc[k] = mac<FORM>(v.y, w.y, acc[k]);
                 acc[k] = mac<FORM>(v.z, w.z, acc[k]);
@@ -200,7 +246,7 @@ __device__ __forceinline__ void row_dots_n(const InstanceDesc &D, const StageSlo
 #pragma unroll
                 for (int k = 0; k < NS; k++) {
                     if (NS == kSrcBatch && k >= ns) continue;
-                    acc[k] = mac<FORM>(vv[u], ss.sp[k][cc[u]], acc[k]);
+                    acc[k] = mac<FORM>(vv[u], reinterpret_cast<const S *>(ss.sp[k])[cc[u]], acc[k]);
                 }
             }
         }
@@ -210,7 +256,7 @@ __device__ __forceinline__ void row_dots_n(const InstanceDesc &D, const StageSlo
 #pragma unroll
             for (int k = 0; k < NS; k++) {
                 if (NS == kSrcBatch && k >= ns) continue;
-                acc[k] = mac<FORM>(vv, ss.sp[k][cc], acc[k]);
+                acc[k] = mac<FORM>(vv, reinterpret_cast<const S *>(ss.sp[k])[cc], acc[k]);
             }
         }
     } else {
@@ -245,9 +291,15 @@ template <int FORM>
 __device__ __forceinline__ void row_dots(const InstanceDesc &D, const StageSlots &ss, int ns, int r,
                                          double (&out)[kSrcBatch])
 {
-    if (ns == 1) row_dots_n<FORM, 1>(D, ss, ns, r, out);
-    else if (ns == 2) row_dots_n<FORM, 2>(D, ss, ns, r, out);
-    else row_dots_n<FORM, kSrcBatch>(D, ss, ns, r, out);
+    if (FORM == FORM_EXACT && ss.dbl) {
+        if (ns == 1) row_dots_n<FORM, 1, double>(D, ss, ns, r, out);
+        else if (ns == 2) row_dots_n<FORM, 2, double>(D, ss, ns, r, out);
+        else row_dots_n<FORM, kSrcBatch, double>(D, ss, ns, r, out);
+    } else {
+        if (ns == 1) row_dots_n<FORM, 1, float>(D, ss, ns, r, out);
+        else if (ns == 2) row_dots_n<FORM, 2, float>(D, ss, ns, r, out);
+        else row_dots_n<FORM, kSrcBatch, float>(D, ss, ns, r, out);
+    }
 }
 
 // --------------------------------------------------------------------------
@@ -1362,7 +1414,7 @@ __device__ void scan_iup(Ctx &c, Shared &sh)
 // 32 x 16 shared tile (pieces swizzled), two tiles per warp so that the next slice is in flight
 // while the current one is used; every lane accumulates ITS row in feature
 // order from the tile -- the reference's summation order.
-template <int FORM, int NS>
+template <int FORM, int NS, typename S>
 __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const StageSlots &ss, int ns, int r, float *tile,
                                                double (&out)[kPrefetchMax])
 {
@@ -1371,11 +1423,11 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
     const int ld = D.x.ld;   // multiple of 4
     const float *X = D.x.X;
     acc_t acc[NS];
-    const float *src[NS];
+    const S *src[NS];
 #pragma unroll
     for (int k = 0; k < NS; k++) {
         acc[k] = acc_t(0);
-        src[k] = ss.sp[k < ns ? k : 0];
+        src[k] = reinterpret_cast<const S *>(ss.sp[k < ns ? k : 0]);
     }
     // a slice is 32 rows x 4 pieces of 16 bytes; lane L moves pieces L + 32i
     // (i < 4): row (L + 32i) / 4, piece L % 4.  Row t of a tile = the row of lane t.
@@ -1413,7 +1465,7 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
             const float4 xv = *reinterpret_cast<const float4 *>(cur + lane * kTileStride + 4 * ((q >> 2) ^ ((lane >> 1) & 3)));
 #pragma unroll
             for (int k = 0; k < NS; k++) {
-                const float4 w = *reinterpret_cast<const float4 *>(src[k] + c0 + q);
+                const auto w = src4(src[k], (c0 + q) >> 2);
                 acc[k] = mac<FORM>(xv.x, w.x, acc[k]);
                 acc[k] = mac<FORM>(xv.y, w.y, acc[k]);
                 acc[k] = mac<FORM>(xv.z, w.z, acc[k]);
@@ -1468,10 +1520,18 @@ __device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const 
                 col = c.sCol[kk];
             }
             double dots[kPrefetchMax];
-            if (ns == 1) warp_tile_dots<FORM, 1>(D, sh.ss, ns, r, tile, dots);
-            else if (ns == 2) warp_tile_dots<FORM, 2>(D, sh.ss, ns, r, tile, dots);
-            else if (ns <= 4) warp_tile_dots<FORM, 4>(D, sh.ss, ns, r, tile, dots);
-            else warp_tile_dots<FORM, 8>(D, sh.ss, ns, r, tile, dots);
+            if (FORM == FORM_EXACT) {
+                // staged sources are float64 in the exact form
+                if (ns == 1) warp_tile_dots<FORM, 1, double>(D, sh.ss, ns, r, tile, dots);
+                else if (ns == 2) warp_tile_dots<FORM, 2, double>(D, sh.ss, ns, r, tile, dots);
+                else if (ns <= 4) warp_tile_dots<FORM, 4, double>(D, sh.ss, ns, r, tile, dots);
+                else warp_tile_dots<FORM, 8, double>(D, sh.ss, ns, r, tile, dots);
+            } else {
+                if (ns == 1) warp_tile_dots<FORM, 1, float>(D, sh.ss, ns, r, tile, dots);
+                else if (ns == 2) warp_tile_dots<FORM, 2, float>(D, sh.ss, ns, r, tile, dots);
+                else if (ns <= 4) warp_tile_dots<FORM, 4, float>(D, sh.ss, ns, r, tile, dots);
+                else warp_tile_dots<FORM, 8, float>(D, sh.ss, ns, r, tile, dots);
+            }
             if (valid) {
                 const double xe = D.x.xsq ? D.x.xsq[r] : 0.0;
 #pragma unroll
@@ -1543,7 +1603,7 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
             off = (size_t)tc_area_bytes(D.tc_n);
         }
         c.stage = reinterpret_cast<float *>(dyn + off);
-        off += (size_t)D.stage_cap * D.stage_lds * sizeof(float);
+        off += (size_t)D.stage_cap * D.stage_lds * stage_elem(FORM);
         off = (off + 15) & ~(size_t)15;
         c.tile = reinterpret_cast<float *>(dyn + off);
         c.pt = reinterpret_cast<PrefetchTable *>(dyn + off);
@@ -1578,7 +1638,8 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
     } while (0)
     if (threadIdx.x == 0) { sh.cs.nprev = 0; sh.cs.ncur = 0; }
     if (!D.x.X && D.stage_cap > 0)
-        for (long long k = threadIdx.x; k < (long long)D.stage_lds * D.stage_cap; k += blockDim.x) c.stage[k] = 0.0f;
+        for (long long k = threadIdx.x; k < (long long)D.stage_lds * D.stage_cap * (stage_elem(FORM) / 4); k += blockDim.x)
+            c.stage[k] = 0.0f;
     __syncthreads();
 
     // ---- initial state (svm.cpp:525-572, QD svm.cpp:1321-1327) on the global copies ----
