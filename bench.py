@@ -324,6 +324,34 @@ def serving_extra(eng, make_params):
             "first8_identical_alone": bool(same)}
 
 
+def profile_case(name):
+    """One solver launch for an ncu capture (autotuner and graphs off, so that
+    the launch is a plain kernel launch):
+      ovo45_half     the one-vs-one workload at half size, exact form, 45 solves
+      pixels8k_fp16  dense pixel rows n=8000 d=784, one solve in the fp16x3 tensor form"""
+    from svmb200 import Engine
+    from svmb200.lib import ResidentRows, make_params
+    eng = Engine()
+    eng.set_option("autotune", 0)
+    eng.set_option("graphs", 0)
+    if name == "ovo45_half":
+        tr, _, _ = datagen.multiclass_geo(n_classes=10, largest=12000, ratio=0.8, d=D, seed=4, scale=0.5)
+        rows, ys = pair_instances(tr)
+        prm = [make_params(svm_type=0, kernel_type=2, gamma=GAMMA, C_pos=CVAL) for _ in rows]
+        res = ResidentRows(eng, tr)
+    elif name == "pixels8k_fp16":
+        tr, _ = datagen.dense_pixels(n=8000, n_test=10)
+        rows = [np.arange(tr.n, dtype=np.int32)]
+        ys = [tr.y.astype(np.float64)]
+        prm = [make_params(svm_type=0, kernel_type=2, gamma=1.0 / 784, C_pos=10.0, cache_mb=400.0, form=3)]
+        res = ResidentRows(eng, tr, layout=1)
+    else:
+        raise SystemExit(f"unknown profile case {name}")
+    _, st = res.solve_many(rows, ys, prm)
+    print(json.dumps({"profile_case": name, "instances": len(rows), "kernel_ms": st[0]["seconds"] * 1e3}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,7 +360,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the precision-form, CV-grid and serving workloads")
+    ap.add_argument("--profile-case", default=None, help="run one solver launch for a profiler capture and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args.profile_case)
     if args.warmup < 3:
         args.warmup = 3
 

@@ -18,7 +18,10 @@
 
 namespace svmb {
 
-constexpr int kThreads = 512;           // threads per block of the persistent solver
+#ifndef SVMB_THREADS
+#define SVMB_THREADS 512
+#endif
+constexpr int kThreads = SVMB_THREADS;  // threads per block of the persistent solver (a multiple of 128)
 constexpr int kWarps = kThreads / 32;
 constexpr int kSrcBatch = 8;            // source rows staged per pass in the row-block product
 constexpr int kMaxWays = 8;             // set associativity of the Q-row cache
@@ -42,7 +45,8 @@ SVMB_HD constexpr int aux_bytes(int form, int tile_bufs) { return (form == 2 || 
 // tensor-core (FORM_BF16X3) block products inside the solver
 constexpr int kTcM = 128;               // targets per tile (MMA M); rows are TMEM lanes
 constexpr int kTcStages = 3;            // operand stages of the cp.async -> MMA pipeline
-constexpr int kTcMaxN = 64;             // sources per block-product pass (MMA N, TMEM columns)
+constexpr int kTcMaxN = 4 * (kThreads / 32) < 64 ? 4 * (kThreads / 32) : 64;   // sources per block-product pass
+                                        // (MMA N; the epilogue reads 16 columns per group of 4 warps)
 // bytes of one operand stage: target tile (128 rows x 64 bf16, hi and lo) + n source rows (hi and lo)
 SVMB_HD constexpr int tc_stage_bytes(int n) { return 2 * kTcM * 128 + n * 256; }
 SVMB_HD constexpr int tc_area_bytes(int n) { return 1024 + kTcStages * tc_stage_bytes(n); }
