@@ -89,7 +89,7 @@ int svmb_version(void);                         /* LIBSVM_VERSION * 100 + engine
 int svmb_device_available(void);                /* 1 if a CUDA device can be used */
 
 /* Process-wide engine options used by svm_train / svm_cross_validation:
- *   "form"   SVMB_FORM_EXACT (default) or SVMB_FORM_FP32
+ *   "form"   SVMB_FORM_EXACT (default), SVMB_FORM_FP32, SVMB_FORM_BF16X3 or SVMB_FORM_FP16X3
  *   "blocks" thread blocks per solve (0 = automatic)
  *   "layout" -1 automatic, 0 CSR, 1 dense device layout of the rows
  *   "prefetch" kernel rows per cache-miss pass (1 = none, 0 = automatic)
@@ -99,6 +99,9 @@ int svmb_device_available(void);                /* 1 if a CUDA device can be use
  *            and later calls use the fastest; results never depend on them.
  *            0: fixed rules.  Instances with their own prefetch or blocks are
  *            never tuned.
+ *   "fill_depth" 1..4 (default 2): deepest ring of column slices per warp in the
+ *            CUDA-core row fills (a launch takes the deepest that keeps its
+ *            instances in one launch); speed only, results never depend on it
  *   "predict_form" SVMB_FORM_EXACT (default: the reference's kernel values bit
  *            for bit) or a tensor-core form: svm_predict* and svmb_predict_batch
  *            then evaluate K(test rows, SVs) as block products on the tensor cores */

@@ -516,9 +516,9 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
     std::vector<StagePlan> sp_all;
     std::vector<long long> nmin;
     int last = first;
-    // the instances from `first` that one launch holds, with 2 or 1 transpose
-    // tiles per warp (two keep the next column slice in flight; one leaves
-    // more shared memory for state, so that more instances fit one launch)
+    // the instances from `first` that one launch holds with `bufs` transpose
+    // tiles per warp.  Returns -1 on an error that no depth avoids, -2 when the
+    // first instance does not fit at this depth (reported only at depth 1).
     auto fit = [&](int bufs, std::vector<StagePlan> &sps, std::vector<long long> &nms, int &end) -> int {
         sps.clear();
         nms.clear();
@@ -533,6 +533,7 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
             }
             const StagePlan st = stage_plan(rows_of(sp, rows), prm.form, budget, bufs);
             if (st.chunk_max < 64) {
+                if (bufs > 1) return -2;
                 set_error("not enough shared memory for the solver state");
                 return -1;
             }
@@ -540,6 +541,7 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
             const long long nm = std::max<long long>(1, (l + st.chunk_max - 1) / st.chunk_max);
             if (nm > capacity) {
                 if (end == first) {
+                    if (bufs > 1) return -2;
                     set_error("problem too large: more positions than the device's blocks can hold in shared memory");
                     return -1;
                 }
@@ -553,17 +555,26 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
         }
         return 0;
     };
-    if (fit(2, sp_all, nmin, last) != 0) return -1;
-    if (last < ninst && !is_tc_form(prm.form)) {
-        std::vector<StagePlan> sp1;
-        std::vector<long long> nm1;
-        int last1 = first;
-        if (fit(1, sp1, nm1, last1) != 0) return -1;
-        if (last1 > last) {
-            sp_all.swap(sp1);
-            nmin.swap(nm1);
-            last = last1;
+    if (is_tc_form(prm.form)) {
+        // the tensor forms have no transpose tiles
+        if (fit(2, sp_all, nmin, last) != 0) return -1;
+    } else {
+        // the deepest ring (deeper rings keep more of a fill in flight) among
+        // those that put the most instances into this launch
+        int best = first;
+        std::vector<StagePlan> spb;
+        std::vector<long long> nmb;
+        for (int bufs = fill_depth(); bufs >= 1; bufs--) {
+            int end = first;
+            const int rc = fit(bufs, spb, nmb, end);
+            if (rc == -1) return -1;
+            if (rc == 0 && end > best) {
+                best = end;
+                sp_all.swap(spb);
+                nmin.swap(nmb);
+            }
         }
+        last = best;
     }
     const int count = last - first;
     w.count = count;
@@ -1026,6 +1037,15 @@ void autotune_last(int *prefetch, int *rows_per_block, int *exploring)
 
 static int g_graphs_on = 1;
 void set_graphs(int on) { g_graphs_on = on ? 1 : 0; }
+
+static int g_fill_depth = 2;
+int set_fill_depth(int bufs)
+{
+    if (bufs < 1 || bufs > kMaxTileBufs) return -1;
+    g_fill_depth = bufs;
+    return 0;
+}
+int fill_depth() { return g_fill_depth; }
 
 // one non-blocking stream per device for the waves of solve_batch
 static cudaStream_t solver_stream()

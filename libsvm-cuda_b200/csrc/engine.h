@@ -40,7 +40,11 @@ constexpr int kAuxBytes1 = ((kTileBytes > kCandBytes ? kTileBytes : kCandBytes) 
 // tensor forms: no transpose tiles; candidates or the block-product partial sums
 constexpr int kRedBytes = 8 * 128 * 8;
 constexpr int kAuxBytesTc = ((kCandBytes > kRedBytes ? kCandBytes : kRedBytes) + 15) / 16 * 16;
-SVMB_HD constexpr int aux_bytes(int form, int tile_bufs) { return (form == 2 || form == 3) ? kAuxBytesTc : tile_bufs == 1 ? kAuxBytes1 : kAuxBytes; }
+// transpose tiles per warp in the CUDA-core fills: a ring of up to 4 column
+// slices, all but the one in use in flight
+constexpr int kMaxTileBufs = 4;
+SVMB_HD constexpr int tile_aux_bytes(int bufs) { return ((bufs * kTileBytes > kCandBytes ? bufs * kTileBytes : kCandBytes) + 15) / 16 * 16; }
+SVMB_HD constexpr int aux_bytes(int form, int tile_bufs) { return (form == 2 || form == 3) ? kAuxBytesTc : tile_aux_bytes(tile_bufs); }
 
 // tensor-core (FORM_BF16X3) block products inside the solver
 constexpr int kTcM = 128;               // targets per tile (MMA M); rows are TMEM lanes
@@ -184,7 +188,7 @@ struct InstanceDesc {
     int lazy_gbar;
     int tc_n;                   // FORM_BF16X3: sources per tensor-core pass (16, 32 or 64); 0 otherwise
     int *done_flag;             // host-mapped word set to 1 once the whole instance has written its results, or nullptr
-    int tile_bufs;              // transpose tiles per warp in the CUDA-core fills (1 or 2; same in every instance of a launch)
+    int tile_bufs;              // transpose tiles per warp in the CUDA-core fills (1 to kMaxTileBufs; same in every instance of a launch)
 };
 
 }  // namespace svmb

@@ -146,6 +146,12 @@ void count_launch(long long n = 1);
 void count_transfer(long long h2d, long long d2h);
 // CUDA graphs of repeated waves in solve_batch (on by default)
 void set_graphs(int on);
+// deepest ring of transpose tiles per warp the CUDA-core fills may use (1 to
+// kMaxTileBufs, default 2: deeper rings measured no faster on B200, the rows
+// being L2-resident); a launch takes the deepest that still fits its
+// instances into one launch.  Results do not depend on it.
+int set_fill_depth(int bufs);
+int fill_depth();
 void graph_counts(long long *captured, long long *replayed);
 void transfer_bytes(long long *h2d, long long *d2h);
 cudaError_t xfer_async(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s);

@@ -49,6 +49,9 @@ namespace svmb {
 #define SVMB_INF __longlong_as_double(0x7ff0000000000000ULL)
 constexpr double kTau = 1e-12;                     // reference svm.cpp:42
 constexpr long long kWaitTimeout = 60000000000LL;  // ~30 s of SM clock
+// positions a thread takes at a time in the chunk scans that read Q rows from
+// global memory: their loads are issued together
+constexpr int kScanGroup = 8;
 
 // --------------------------------------------------------------------------
 // memory-model helpers
@@ -101,24 +104,27 @@ __device__ void stage_sources(const InstanceDesc &D, float *stage, StageSlots &s
         ss.dbl = dbl ? 1 : 0;
     }
     if (x.X) {
+        // all sources in one pass: thread e moves 16 bytes of source e / ld4
         const int ld4 = x.ld >> 2;
-        for (int k = 0; k < ns; k++) {
-            const float4 *src = reinterpret_cast<const float4 *>(x.X + (long long)rows[k] * x.ld);
-            if (dbl) {
-                double2 *dst = reinterpret_cast<double2 *>(stage_d + (long long)k * D.stage_lds);
-                for (int t = threadIdx.x; t < ld4; t += blockDim.x) {
-                    const float4 v = __ldg(src + t);
+        if (D.stage_cap > 0) {
+            const int total = ns * ld4;
+            for (int e = threadIdx.x; e < total; e += blockDim.x) {
+                const int k = e / ld4, t = e - k * ld4;
+                const float4 v = __ldg(reinterpret_cast<const float4 *>(x.X + (long long)rows[k] * x.ld) + t);
+                if (dbl) {
+                    double2 *dst = reinterpret_cast<double2 *>(stage_d + (long long)k * D.stage_lds);
                     dst[2 * t] = make_double2((double)v.x, (double)v.y);
                     dst[2 * t + 1] = make_double2((double)v.z, (double)v.w);
+                } else {
+                    reinterpret_cast<float4 *>(stage + (long long)k * D.stage_lds)[t] = v;
                 }
-                if (threadIdx.x == 0) ss.sp[k] = stage_d + (long long)k * D.stage_lds;
-            } else if (D.stage_cap > 0) {
-                float4 *dst = reinterpret_cast<float4 *>(stage + (long long)k * D.stage_lds);
-                for (int t = threadIdx.x; t < ld4; t += blockDim.x) dst[t] = __ldg(src + t);
-                if (threadIdx.x == 0) ss.sp[k] = stage + (long long)k * D.stage_lds;
-            } else if (threadIdx.x == 0) {
-                ss.sp[k] = x.X + (long long)rows[k] * x.ld;
             }
+        }
+        if (threadIdx.x < ns) {
+            const int k = threadIdx.x;
+            if (dbl) ss.sp[k] = stage_d + (long long)k * D.stage_lds;
+            else if (D.stage_cap > 0) ss.sp[k] = stage + (long long)k * D.stage_lds;
+            else ss.sp[k] = x.X + (long long)rows[k] * x.ld;
         }
     } else if (D.stage_cap > 0) {
         for (int k = 0; k < ns; k++) {
@@ -586,6 +592,10 @@ struct Shared {
     // rows of the current fill pass: row id, label, slot
     int frow[kPrefetchMax], fy[kPrefetchMax];
     long long fslot[kPrefetchMax];
+    // per source of the fill pass running now: norm, label, destination row
+    double fsx[kPrefetchMax];
+    int fsy[kPrefetchMax];
+    float *fsd[kPrefetchMax];
     int nfill;
     int pick[kPrefetchMax];
     int npick;
@@ -1410,10 +1420,33 @@ __device__ void scan_iup(Ctx &c, Shared &sh)
 
 // Dot products of the 32 rows of a warp (lane L owns row r) with up to 8
 // staged dense sources.  The 32 rows are read in 16-column slices with
-// coalesced 64-byte pieces per row (cp.async, 16 bytes per lane) into a
-// 32 x 16 shared tile (pieces swizzled), two tiles per warp so that the next slice is in flight
-// while the current one is used; every lane accumulates ITS row in feature
-// order from the tile -- the reference's summation order.
+// coalesced 64-byte pieces per row (cp.async, 16 bytes per lane) into 32 x 16
+// shared tiles (pieces swizzled).  The warp's tiles form a ring of
+// D.tile_bufs slices: all but the one in use are in flight, so a warp moves
+// tile_bufs slices per memory round trip.  Every lane accumulates ITS row in
+// feature order from the tile -- the reference's summation order.
+// shared-memory loads by 32-bit shared-window address (volatile: they stay
+// after the cp.async wait and __syncwarp that publish the tile)
+__device__ __forceinline__ float4 lds_f4(uint32_t a)
+{
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ double2 lds_d2(uint32_t a)
+{
+    double2 v;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
+    return v;
+}
+// four staged source values at byte address a: float4, or two double2
+__device__ __forceinline__ float4 src4_at(uint32_t a, float) { return lds_f4(a); }
+__device__ __forceinline__ D4 src4_at(uint32_t a, double)
+{
+    const double2 p = lds_d2(a), q = lds_d2(a + 16);
+    return D4{p.x, p.y, q.x, q.y};
+}
+
 template <int FORM, int NS, typename S>
 __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const StageSlots &ss, int ns, int r, float *tile,
                                                double (&out)[kPrefetchMax])
@@ -1423,12 +1456,11 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
     const int ld = D.x.ld;   // multiple of 4
     const float *X = D.x.X;
     acc_t acc[NS];
-    const S *src[NS];
 #pragma unroll
-    for (int k = 0; k < NS; k++) {
-        acc[k] = acc_t(0);
-        src[k] = reinterpret_cast<const S *>(ss.sp[k < ns ? k : 0]);
-    }
+    for (int k = 0; k < NS; k++) acc[k] = acc_t(0);
+    // the staged sources lie D.stage_lds values apart from the first
+    const uint32_t src0 = tc::smem_addr(ss.sp[0]);
+    const uint32_t sstride = (uint32_t)(D.stage_lds * (int)sizeof(S));
     // a slice is 32 rows x 4 pieces of 16 bytes; lane L moves pieces L + 32i
     // (i < 4): row (L + 32i) / 4, piece L % 4.  Row t of a tile = the row of lane t.
     const float *prow[4];
@@ -1449,23 +1481,23 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
         }
         tc::cp_async_commit();
     };
-    const bool two = D.tile_bufs == 2;
-    issue(0, 0);
+    const int nb = D.tile_bufs;
+    // prologue: slices 0 .. nb-2 in flight
+    for (int p = 0; p + 1 < nb; p++) issue(16 * p, p);
     for (int c0 = 0, s = 0; c0 < ld; c0 += 16) {
-        if (two) {
-            issue(c0 + 16, s ^ 1);
-            tc::cp_async_wait<1>();                      // this slice has landed (for this lane)
-        } else {
-            tc::cp_async_wait<0>();
-        }
+        // slice s + nb - 1 goes to the buffer used by slice s - 1 (consumed
+        // before the __syncwarp that ended the previous step)
+        issue(c0 + 16 * (nb - 1), s == 0 ? nb - 1 : s - 1);
+        tc::cp_async_wait_n(nb - 1);                     // slice s has landed (for this lane)
         __syncwarp();
-        const float *cur = tile + s * 32 * kTileStride;
+        const uint32_t cur = tile_s + (uint32_t)(s * 32 * kTileStride * 4 + lane * kTileStride * 4);
         const int lim = ld - c0 < 16 ? ld - c0 : 16;    // multiple of 4
         for (int q = 0; q < lim; q += 4) {
-            const float4 xv = *reinterpret_cast<const float4 *>(cur + lane * kTileStride + 4 * ((q >> 2) ^ ((lane >> 1) & 3)));
+            const float4 xv = lds_f4(cur + (uint32_t)(16 * ((q >> 2) ^ ((lane >> 1) & 3))));
+            const uint32_t soff = (uint32_t)((c0 + q) * (int)sizeof(S));
 #pragma unroll
             for (int k = 0; k < NS; k++) {
-                const auto w = src4(src[k], (c0 + q) >> 2);
+                const auto w = src4_at(src0 + (uint32_t)(k < ns ? k : 0) * sstride + soff, S());
                 acc[k] = mac<FORM>(xv.x, w.x, acc[k]);
                 acc[k] = mac<FORM>(xv.y, w.y, acc[k]);
                 acc[k] = mac<FORM>(xv.z, w.z, acc[k]);
@@ -1473,8 +1505,7 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
             }
         }
         __syncwarp();
-        if (two) s ^= 1;
-        else issue(c0 + 16, 0);
+        s = s + 1 == nb ? 0 : s + 1;
     }
 #pragma unroll
     for (int k = 0; k < NS; k++) out[k] = (double)acc[k];
@@ -1483,23 +1514,35 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
 // Evaluate the Q rows of `ns` (<= kPrefetchMax, <= stage_cap when staged)
 // sources into cache slots on my chunk of [0,A) (tail = 0, from shared
 // memory) or of [A,l) (tail = 1, global state).
+template <int FORM, typename S>
+__device__ __forceinline__ void tile_dots_ns(const InstanceDesc &D, const StageSlots &ss, int ns, int r, float *tile,
+                                             double (&dots)[kPrefetchMax])
+{
+    switch (ns) {
+    case 1: warp_tile_dots<FORM, 1, S>(D, ss, ns, r, tile, dots); break;
+    case 2: warp_tile_dots<FORM, 2, S>(D, ss, ns, r, tile, dots); break;
+    case 3: warp_tile_dots<FORM, 3, S>(D, ss, ns, r, tile, dots); break;
+    case 4: warp_tile_dots<FORM, 4, S>(D, ss, ns, r, tile, dots); break;
+    case 5: warp_tile_dots<FORM, 5, S>(D, ss, ns, r, tile, dots); break;
+    case 6: warp_tile_dots<FORM, 6, S>(D, ss, ns, r, tile, dots); break;
+    default: warp_tile_dots<FORM, 8, S>(D, ss, ns, r, tile, dots); break;
+    }
+}
+
 template <int FORM>
 __device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const int *src_y, const long long *slot,
                           int tail)
 {
     const InstanceDesc &D = *c.D;
     if (ns == 0) return;
-    stage_sources(D, c.stage, sh.ss, src_row, ns);
-    double xs[kPrefetchMax];
-    float *dst[kPrefetchMax];
-    int sy[kPrefetchMax];
-#pragma unroll
-    for (int k = 0; k < kPrefetchMax; k++) {
-        const int kk = k < ns ? k : 0;
-        xs[k] = D.x.xsq ? D.x.xsq[src_row[kk]] : 0.0;
-        dst[k] = D.cache.data + slot[kk] * D.cache.stride;
-        sy[k] = src_y[kk];
+    // per-source constants of this pass, read from shared memory where used
+    if (threadIdx.x < ns) {
+        const int k = threadIdx.x;
+        sh.fsx[k] = D.x.xsq ? D.x.xsq[src_row[k]] : 0.0;
+        sh.fsy[k] = src_y[k];
+        sh.fsd[k] = D.cache.data + slot[k] * D.cache.stride;
     }
+    stage_sources(D, c.stage, sh.ss, src_row, ns);   // ends with a barrier
     const int lo = tail ? c.t0 : 0, hi = tail ? c.t1 : c.a1 - c.a0;
     if (D.x.X && D.stage_cap > 0) {
         // dense rows, staged sources: warp-tiled, whole warps per 32 positions
@@ -1520,23 +1563,14 @@ __device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const 
                 col = c.sCol[kk];
             }
             double dots[kPrefetchMax];
-            if (FORM == FORM_EXACT) {
-                // staged sources are float64 in the exact form
-                if (ns == 1) warp_tile_dots<FORM, 1, double>(D, sh.ss, ns, r, tile, dots);
-                else if (ns == 2) warp_tile_dots<FORM, 2, double>(D, sh.ss, ns, r, tile, dots);
-                else if (ns <= 4) warp_tile_dots<FORM, 4, double>(D, sh.ss, ns, r, tile, dots);
-                else warp_tile_dots<FORM, 8, double>(D, sh.ss, ns, r, tile, dots);
-            } else {
-                if (ns == 1) warp_tile_dots<FORM, 1, float>(D, sh.ss, ns, r, tile, dots);
-                else if (ns == 2) warp_tile_dots<FORM, 2, float>(D, sh.ss, ns, r, tile, dots);
-                else if (ns <= 4) warp_tile_dots<FORM, 4, float>(D, sh.ss, ns, r, tile, dots);
-                else warp_tile_dots<FORM, 8, float>(D, sh.ss, ns, r, tile, dots);
-            }
+            // staged sources are float64 in the exact form
+            if (FORM == FORM_EXACT) tile_dots_ns<FORM, double>(D, sh.ss, ns, r, tile, dots);
+            else tile_dots_ns<FORM, float>(D, sh.ss, ns, r, tile, dots);
             if (valid) {
                 const double xe = D.x.xsq ? D.x.xsq[r] : 0.0;
 #pragma unroll
                 for (int s2 = 0; s2 < kPrefetchMax; s2++)
-                    if (s2 < ns) dst[s2][col] = q_value(D.kp, sy[s2] * yp, dots[s2], xs[s2], xe);
+                    if (s2 < ns) sh.fsd[s2][col] = q_value(D.kp, sh.fsy[s2] * yp, dots[s2], sh.fsx[s2], xe);
             }
         }
     } else {
@@ -1556,7 +1590,7 @@ __device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const 
             const double xe = D.x.xsq ? D.x.xsq[r] : 0.0;
 #pragma unroll
             for (int s2 = 0; s2 < kPrefetchMax; s2++)
-                if (s2 < ns) dst[s2][col] = q_value(D.kp, sy[s2] * yp, dots[s2], xs[s2], xe);
+                if (s2 < ns) sh.fsd[s2][col] = q_value(D.kp, sh.fsy[s2] * yp, dots[s2], sh.fsx[s2], xe);
         }
     }
     unstage_sources(D, c.stage, sh.ss);
@@ -1853,34 +1887,50 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 const double QDi0 = sh.bd[2], QDi1 = sh.bd[5];
                 const double two_yi0 = __dmul_rn(2.0, (double)sh.bi[3]);
                 const int n = c.a1 - c.a0;
-                for (int k = threadIdx.x; k < n; k += blockDim.x) {
-                    const unsigned char s = c.sS[k];
-                    const double G = c.sG[k];
-                    const int col = c.sCol[k];
-                    if (c.sY[k] == +1) {
-                        if (s != ST_LOWER) {
-                            const double grad_diff = __dadd_rn(Gmax0, G);
-                            v[1] = fmax(v[1], G);
-                            if (grad_diff > 0) {
-                                double quad;
-                                if (!nu) quad = __dsub_rn(__dadd_rn(QDi0, c.sQD[k]), __dmul_rn(two_yi0, (double)Qi0[col]));
-                                else quad = __dsub_rn(__dadd_rn(QDi0, c.sQD[k]), (double)__fmul_rn(2.0f, Qi0[col]));
-                                const double num = __dmul_rn(grad_diff, grad_diff);
-                                const double od = quad > 0 ? -__ddiv_rn(num, quad) : -__ddiv_rn(num, kTau);
-                                better_min(v[0], ix[0], od, c.a0 + k);
-                            }
+                // kScanGroup positions per thread at a time: their Q_i values are
+                // loaded together (one L2 round trip per group, not per position)
+                for (int k0 = threadIdx.x; k0 < n; k0 += kScanGroup * blockDim.x) {
+                    float qv[kScanGroup];
+#pragma unroll
+                    for (int u = 0; u < kScanGroup; u++) {
+                        const int k = k0 + u * (int)blockDim.x;
+                        qv[u] = 0.0f;
+                        if (k < n) {
+                            const float *Qr = (nu && c.sY[k] != +1) ? Qi1 : Qi0;
+                            if (Qr) qv[u] = Qr[c.sCol[k]];
                         }
-                    } else {
-                        if (s != ST_UPPER) {
-                            const double grad_diff = __dsub_rn(nu ? Gmax1 : Gmax0, G);
-                            if (nu) v[2] = fmax(v[2], -G); else v[1] = fmax(v[1], -G);
-                            if (grad_diff > 0) {
-                                double quad;
-                                if (!nu) quad = __dadd_rn(__dadd_rn(QDi0, c.sQD[k]), __dmul_rn(two_yi0, (double)Qi0[col]));
-                                else quad = __dsub_rn(__dadd_rn(QDi1, c.sQD[k]), (double)__fmul_rn(2.0f, Qi1[col]));
-                                const double num = __dmul_rn(grad_diff, grad_diff);
-                                const double od = quad > 0 ? -__ddiv_rn(num, quad) : -__ddiv_rn(num, kTau);
-                                better_min(v[0], ix[0], od, c.a0 + k);
+                    }
+#pragma unroll
+                    for (int u = 0; u < kScanGroup; u++) {
+                        const int k = k0 + u * (int)blockDim.x;
+                        if (k >= n) continue;
+                        const unsigned char s = c.sS[k];
+                        const double G = c.sG[k];
+                        if (c.sY[k] == +1) {
+                            if (s != ST_LOWER) {
+                                const double grad_diff = __dadd_rn(Gmax0, G);
+                                v[1] = fmax(v[1], G);
+                                if (grad_diff > 0) {
+                                    double quad;
+                                    if (!nu) quad = __dsub_rn(__dadd_rn(QDi0, c.sQD[k]), __dmul_rn(two_yi0, (double)qv[u]));
+                                    else quad = __dsub_rn(__dadd_rn(QDi0, c.sQD[k]), (double)__fmul_rn(2.0f, qv[u]));
+                                    const double num = __dmul_rn(grad_diff, grad_diff);
+                                    const double od = quad > 0 ? -__ddiv_rn(num, quad) : -__ddiv_rn(num, kTau);
+                                    better_min(v[0], ix[0], od, c.a0 + k);
+                                }
+                            }
+                        } else {
+                            if (s != ST_UPPER) {
+                                const double grad_diff = __dsub_rn(nu ? Gmax1 : Gmax0, G);
+                                if (nu) v[2] = fmax(v[2], -G); else v[1] = fmax(v[1], -G);
+                                if (grad_diff > 0) {
+                                    double quad;
+                                    if (!nu) quad = __dadd_rn(__dadd_rn(QDi0, c.sQD[k]), __dmul_rn(two_yi0, (double)qv[u]));
+                                    else quad = __dsub_rn(__dadd_rn(QDi1, c.sQD[k]), (double)__fmul_rn(2.0f, qv[u]));
+                                    const double num = __dmul_rn(grad_diff, grad_diff);
+                                    const double od = quad > 0 ? -__ddiv_rn(num, quad) : -__ddiv_rn(num, kTau);
+                                    better_min(v[0], ix[0], od, c.a0 + k);
+                                }
                             }
                         }
                     }
@@ -2072,25 +2122,45 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 double pv = -SVMB_INF;
                 int pix = -1;
                 const int n = c.a1 - c.a0;
-                for (int k = threadIdx.x; k < n; k += blockDim.x) {
-                    const int col = c.sCol[k];
-                    const float qi = Qi[col], qj = Qj[col];
-                    const double G = __dadd_rn(c.sG[k], __dadd_rn(__dmul_rn((double)qi, dai), __dmul_rn((double)qj, daj)));
-                    c.sG[k] = G;
-                    if (bar_i || bar_j) {
-                        const int p = c.a0 + k;
-                        double gb = D.G_bar[p];
-                        if (bar_i) gb = (old_si == ST_UPPER) ? __dsub_rn(gb, __dmul_rn(C_i, (double)qi)) : __dadd_rn(gb, __dmul_rn(C_i, (double)qi));
-                        if (bar_j) gb = (old_sj == ST_UPPER) ? __dsub_rn(gb, __dmul_rn(C_j, (double)qj)) : __dadd_rn(gb, __dmul_rn(C_j, (double)qj));
-                        D.G_bar[p] = gb;
+                const bool gbar = bar_i || bar_j;
+                // kScanGroup positions per thread at a time, their Q_i, Q_j (and
+                // G_bar) values loaded together before any is used
+                for (int k0 = threadIdx.x; k0 < n; k0 += kScanGroup * blockDim.x) {
+                    float qi[kScanGroup], qj[kScanGroup];
+                    double gb[kScanGroup];
+#pragma unroll
+                    for (int u = 0; u < kScanGroup; u++) {
+                        const int k = k0 + u * (int)blockDim.x;
+                        qi[u] = 0.0f;
+                        qj[u] = 0.0f;
+                        gb[u] = 0.0;
+                        if (k < n) {
+                            const int col = c.sCol[k];
+                            qi[u] = Qi[col];
+                            qj[u] = Qj[col];
+                            if (gbar) gb[u] = D.G_bar[c.a0 + k];
+                        }
                     }
-                    const unsigned char s = c.sS[k];
-                    if (c.sY[k] == +1) {
-                        if (s != ST_UPPER) better_max(v[0], ix[0], -G, c.a0 + k);
-                    } else {
-                        if (s != ST_LOWER) better_max(v[nu], ix[nu], G, c.a0 + k);
+#pragma unroll
+                    for (int u = 0; u < kScanGroup; u++) {
+                        const int k = k0 + u * (int)blockDim.x;
+                        if (k >= n) continue;
+                        const double G = __dadd_rn(c.sG[k], __dadd_rn(__dmul_rn((double)qi[u], dai), __dmul_rn((double)qj[u], daj)));
+                        c.sG[k] = G;
+                        if (gbar) {
+                            double g = gb[u];
+                            if (bar_i) g = (old_si == ST_UPPER) ? __dsub_rn(g, __dmul_rn(C_i, (double)qi[u])) : __dadd_rn(g, __dmul_rn(C_i, (double)qi[u]));
+                            if (bar_j) g = (old_sj == ST_UPPER) ? __dsub_rn(g, __dmul_rn(C_j, (double)qj[u])) : __dadd_rn(g, __dmul_rn(C_j, (double)qj[u]));
+                            D.G_bar[c.a0 + k] = g;
+                        }
+                        const unsigned char s = c.sS[k];
+                        if (c.sY[k] == +1) {
+                            if (s != ST_UPPER) better_max(v[0], ix[0], -G, c.a0 + k);
+                        } else {
+                            if (s != ST_LOWER) better_max(v[nu], ix[nu], G, c.a0 + k);
+                        }
+                        better_max(pv, pix, prefetch_priority(c.sY[k], s, G), c.a0 + k);
                     }
-                    better_max(pv, pix, prefetch_priority(c.sY[k], s, G), c.a0 + k);
                 }
                 if (bar_i || bar_j) {
                     for (int p = c.t0 + threadIdx.x; p < c.t1; p += blockDim.x) {

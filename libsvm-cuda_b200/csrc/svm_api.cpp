@@ -501,6 +501,8 @@ int api_set_option(const char *name, long long value)
         set_graphs((int)value);
     } else if (!strcmp(name, "autotune")) {
         set_autotune((int)value);
+    } else if (!strcmp(name, "fill_depth")) {
+        if (set_fill_depth((int)value) != 0) return -1;
     } else if (!strcmp(name, "predict_form")) {
         if (predict_set_form((int)value) != 0) return -1;
     } else if (!strcmp(name, "prefetch")) {

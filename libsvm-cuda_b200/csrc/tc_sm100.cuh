@@ -164,6 +164,14 @@ __device__ __forceinline__ void cp_async16(uint32_t saddr, const void *gptr, uin
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+// the same with a run-time count (0..3): at most n of this thread's groups still pending
+__device__ __forceinline__ void cp_async_wait_n(int n)
+{
+    if (n <= 0) cp_async_wait<0>();
+    else if (n == 1) cp_async_wait<1>();
+    else if (n == 2) cp_async_wait<2>();
+    else cp_async_wait<3>();
+}
 
 // byte offset of 16-byte piece q (0..7) of row r inside a 128B-swizzled K-major tile
 __host__ __device__ __forceinline__ uint32_t sw128_offset(int r, int q)
