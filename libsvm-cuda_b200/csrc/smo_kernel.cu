@@ -1491,8 +1491,7 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
         tc::cp_async_wait_n(nb - 1);                     // slice s has landed (for this lane)
         __syncwarp();
         const uint32_t cur = tile_s + (uint32_t)(s * 32 * kTileStride * 4 + lane * kTileStride * 4);
-        const int lim = ld - c0 < 16 ? ld - c0 : 16;    // multiple of 4
-        for (int q = 0; q < lim; q += 4) {
+        auto step = [&](int q) {    // columns c0 + q .. c0 + q + 3
             const float4 xv = lds_f4(cur + (uint32_t)(16 * ((q >> 2) ^ ((lane >> 1) & 3))));
             const uint32_t soff = (uint32_t)((c0 + q) * (int)sizeof(S));
 #pragma unroll
@@ -1503,6 +1502,15 @@ __device__ __forceinline__ void warp_tile_dots(const InstanceDesc &D, const Stag
                 acc[k] = mac<FORM>(xv.z, w.z, acc[k]);
                 acc[k] = mac<FORM>(xv.w, w.w, acc[k]);
             }
+        };
+        if (FORM == FORM_EXACT && ld - c0 >= 16) {
+            // a whole slice, its four steps unrolled (the fp32 form keeps the
+            // loop: eight float4 sources per step would not fit registers)
+#pragma unroll
+            for (int q = 0; q < 16; q += 4) step(q);
+        } else {
+            const int lim = ld - c0 < 16 ? ld - c0 : 16;    // multiple of 4
+            for (int q = 0; q < lim; q += 4) step(q);
         }
         __syncwarp();
         s = s + 1 == nb ? 0 : s + 1;
@@ -1562,12 +1570,13 @@ __device__ void fill_rows(Ctx &c, Shared &sh, int ns, const int *src_row, const 
                 yp = c.sY[kk];
                 col = c.sCol[kk];
             }
+            // the target's norm is loaded before the dots so that its latency hides behind them
+            const double xe = D.x.xsq ? D.x.xsq[r] : 0.0;
             double dots[kPrefetchMax];
             // staged sources are float64 in the exact form
             if (FORM == FORM_EXACT) tile_dots_ns<FORM, double>(D, sh.ss, ns, r, tile, dots);
             else tile_dots_ns<FORM, float>(D, sh.ss, ns, r, tile, dots);
             if (valid) {
-                const double xe = D.x.xsq ? D.x.xsq[r] : 0.0;
 #pragma unroll
                 for (int s2 = 0; s2 < kPrefetchMax; s2++)
                     if (s2 < ns) sh.fsd[s2][col] = q_value(D.kp, sh.fsy[s2] * yp, dots[s2], sh.fsx[s2], xe);
