@@ -900,11 +900,16 @@ __device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool glob
     const int warp = threadIdx.x >> 5;
     const int lg = warp & 3, cg = warp >> 2;
     const bool reader = cg * 16 < N;
+    // the last warp issues the MMAs and takes no part in the loads, so that
+    // the issue overlaps the other warps' absorb and loads
+    const int issuer = (int)(blockDim.x >> 5) - 1;
+    const int nload = (int)blockDim.x - 32;
     auto load = [&](int g) {
+        if (warp == issuer) return;
         const int tile = g / NK, kc = g - tile * NK;
         const uint32_t sa = c.tcbase + (uint32_t)((c.tc_g + g) % kTcStages) * sbytes;
         const int tb = lo + tile * kTcM;
-        for (int i = threadIdx.x; i < kTcM * 16; i += blockDim.x) {
+        for (int i = threadIdx.x; i < kTcM * 16; i += nload) {
             const int r = i >> 4, q = i & 15;
             const int t = tb + r;
             const bool ok = t < hi;
@@ -912,7 +917,7 @@ __device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool glob
             tc::cp_async16(sa + (q >= 8 ? a_lo : 0u) + tc::sw128_offset(r, q & 7),
                            Xs + (long long)row * rs + kc * 128 + q * 8, ok ? 16u : 0u);
         }
-        for (int i = threadIdx.x; i < N * 16; i += blockDim.x) {
+        for (int i = threadIdx.x; i < N * 16; i += nload) {
             const int r = i >> 4, q = i & 15;
             const bool ok = r < ns;
             const int row = ok ? sh.tsrow[r] : 0;
@@ -946,16 +951,15 @@ __device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool glob
     for (int g = 0; g < total; g++) {
         const long long G = c.tc_g + g;
         const int tile = g / NK, kc = g - tile * NK;
-        // the MMAs of step g-1 have read their stage and written their accumulator
-        bool w = true;
-        if (g >= 1) w = tc::mbar_wait(&sh.tbar[(G - 1) % kTcStages], (unsigned)(((G - 1) / kTcStages) & 1));
-        if (w && g + kTcStages - 1 < total) load(g + kTcStages - 1);
-        tc::cp_async_commit();
-        tc::cp_async_wait<kTcStages - 1>();             // step g has landed
+        // step g has landed: the groups of steps g+1 .. g+kTcStages-2 may still be pending
+        tc::cp_async_wait<kTcStages - 2>();
         tc::fence_async_smem();
-        ok = __syncthreads_and(w) != 0;
-        if (!ok) break;
-        if (threadIdx.x == 0) {
+        __syncthreads();
+        // step g's MMAs go in before step g-1's are waited for, so the tensor
+        // core always has the next step queued.  Its accumulator (G & 1) was
+        // last read by the absorb of step G-2, which ended before the barrier
+        // that closed the previous iteration.
+        if (threadIdx.x == (unsigned)(issuer * 32)) {
             tc::tc_fence_after();
             const uint32_t sa = c.tcbase + (uint32_t)(G % kTcStages) * sbytes;
             const uint32_t dst = sh.tmem + (uint32_t)((G & 1) * kTcMaxN);
@@ -969,12 +973,21 @@ __device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool glob
             }
             tc::mma_commit(&sh.tbar[G % kTcStages]);
         }
+        bool w = true;
         if (g >= 1) {
-            absorb(G - 1);
-            if (kc == 0) finish_tile(tile - 1);
-            tc::tc_fence_before();
+            // step g-1's MMAs have read their stage and written their accumulator
+            w = tc::mbar_wait(&sh.tbar[(G - 1) % kTcStages], (unsigned)(((G - 1) / kTcStages) & 1));
+            if (w) {
+                absorb(G - 1);
+                if (kc == 0) finish_tile(tile - 1);
+            }
         }
-        __syncthreads();
+        // the stage of step g-1 is free: step g + kTcStages - 1 goes there
+        if (w && g + kTcStages - 1 < total) load(g + kTcStages - 1);
+        tc::cp_async_commit();
+        tc::tc_fence_before();
+        ok = __syncthreads_and(w) != 0;
+        if (!ok) break;
     }
     if (ok) {
         const long long G = c.tc_g + total - 1;
