@@ -473,35 +473,45 @@ struct SetStage {
     unsigned long long st[kMaxWays];
 };
 
-__device__ void cache_read_set(const CacheState &cs, const CacheView &cv, int set, int *tag, int *ep,
-                               unsigned long long *st, const SetStage *pre = nullptr)
+// The set's metadata with this phase's and the previous phase's decisions
+// laid over it.  Ways are visited by constant index (unrolled, guarded by the
+// set's way count) so that the arrays stay in registers, and the global reads
+// of a set go out together.
+__device__ __forceinline__ void cache_read_set(const CacheState &cs, const CacheView &cv, int set, int (&tag)[kMaxWays],
+                                               int (&ep)[kMaxWays], unsigned long long (&st)[kMaxWays],
+                                               const SetStage *pre = nullptr)
 {
     if (pre && pre->set == set) {
-        for (int w = 0; w < cv.nways; w++) {
-            tag[w] = pre->tag[w];
-            ep[w] = pre->ep[w];
-            st[w] = pre->st[w];
-        }
+#pragma unroll
+        for (int w = 0; w < kMaxWays; w++)
+            if (w < cv.nways) {
+                tag[w] = pre->tag[w];
+                ep[w] = pre->ep[w];
+                st[w] = pre->st[w];
+            }
     } else {
-        for (int w = 0; w < cv.nways; w++) {
-            const long long s = (long long)set * cv.nways + w;
-            tag[w] = __ldcg(&cv.tag[s]);
-            ep[w] = __ldcg(&cv.epoch[s]);
-            st[w] = __ldcg(&cv.stamp[s]);
-        }
+        const long long s0 = (long long)set * cv.nways;
+#pragma unroll
+        for (int w = 0; w < kMaxWays; w++)
+            if (w < cv.nways) {
+                tag[w] = __ldcg(&cv.tag[s0 + w]);
+                ep[w] = __ldcg(&cv.epoch[s0 + w]);
+                st[w] = __ldcg(&cv.stamp[s0 + w]);
+            }
     }
+    auto overlay = [&](const CacheRec &r) {
+#pragma unroll
+        for (int w = 0; w < kMaxWays; w++)
+            if (w == r.way) {
+                tag[w] = r.tag;
+                ep[w] = r.epoch;
+                st[w] = r.stamp;
+            }
+    };
     for (int k = 0; k < cs.nprev; k++)
-        if (cs.prev[k].set == set) {
-            tag[cs.prev[k].way] = cs.prev[k].tag;
-            ep[cs.prev[k].way] = cs.prev[k].epoch;
-            st[cs.prev[k].way] = cs.prev[k].stamp;
-        }
+        if (cs.prev[k].set == set) overlay(cs.prev[k]);
     for (int k = 0; k < cs.ncur; k++)
-        if (cs.cur[k].set == set) {
-            tag[cs.cur[k].way] = cs.cur[k].tag;
-            ep[cs.cur[k].way] = cs.cur[k].epoch;
-            st[cs.cur[k].way] = cs.cur[k].stamp;
-        }
+        if (cs.cur[k].set == set) overlay(cs.cur[k]);
 }
 
 // Decide where row `local` lives; records the decision.  whole: the rows
@@ -519,9 +529,15 @@ __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, i
     unsigned long long st[kMaxWays];
     const int set = local % cv.nsets;
     cache_read_set(cs, cv, set, tag, ep, st, pre);
-    int way = -1;
-    for (int w = 0; w < cv.nways; w++)
-        if (tag[w] == local) way = w;
+    int way = -1, ep_hit = 0;
+    unsigned long long st_hit = 0;
+#pragma unroll
+    for (int w = 0; w < kMaxWays; w++)
+        if (w < cv.nways && tag[w] == local) {
+            way = w;
+            ep_hit = ep[w];
+            st_hit = st[w];
+        }
     Lookup L;
     L.was_prefetched = 0;
     CacheRec rec;
@@ -529,20 +545,28 @@ __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, i
     rec.stamp = prefetch ? (clk | kPrefetchMark) : clk;
     rec.tag = local;
     if (way >= 0) {
-        const int va = ep[way] == kEpochFull || ep[way] == cur_epoch;
+        const int va = ep_hit == kEpochFull || ep_hit == cur_epoch;
         L.valid_active = va;
-        L.was_prefetched = va && (st[way] & kPrefetchMark) ? 1 : 0;
-        if (prefetch && va) rec.stamp = st[way];   // a prefetch hit changes nothing
+        L.was_prefetched = va && (st_hit & kPrefetchMark) ? 1 : 0;
+        if (prefetch && va) rec.stamp = st_hit;   // a prefetch hit changes nothing
         rec.way = way;
-        rec.epoch = whole ? kEpochFull : (va ? ep[way] : cur_epoch);
+        rec.epoch = whole ? kEpochFull : (va ? ep_hit : cur_epoch);
     } else {
-        int victim = -1, evictable = 0;
-        for (int w = 0; w < cv.nways; w++) {
-            if (tag[w] != kNoTag && (st[w] & ~kPrefetchMark) >= protect) continue;
+        // victim: an empty way, else the least recently stamped evictable one
+        // (the first such way on equal stamps)
+        int victim = -1, evictable = 0, vtag = kNoTag;
+        unsigned long long vst = 0;
+#pragma unroll
+        for (int w = 0; w < kMaxWays; w++) {
+            if (w >= cv.nways) continue;
+            const unsigned long long sw = st[w] & ~kPrefetchMark;
+            if (tag[w] != kNoTag && sw >= protect) continue;
             evictable++;
-            if (victim < 0 || tag[w] == kNoTag ||
-                (tag[victim] != kNoTag && (st[w] & ~kPrefetchMark) < (st[victim] & ~kPrefetchMark)))
+            if (victim < 0 || tag[w] == kNoTag || (vtag != kNoTag && sw < vst)) {
                 victim = w;
+                vtag = tag[w];
+                vst = sw;
+            }
         }
         if (victim < 0 || (prefetch && evictable < 3)) {
             L.slot = -1;
@@ -704,10 +728,9 @@ __device__ bool exchange(Ctx &c, Shared &sh)
     Partial *mine = my_partial(c);
     int ok = 1;
     if (c.nb > 1) {
-        if (threadIdx.x == 0) {
-            __threadfence();
-            st_release_i32(&mine->seq, want);
-        }
+        // the release store orders this thread's writes and, through the
+        // barrier above, the whole block's before the record is seen
+        if (threadIdx.x == 0) st_release_i32(&mine->seq, want);
         const Partial *all = c.D->partials + (long long)(c.phase & 1) * c.nb;
         for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
             const long long t0 = clock64();
@@ -1751,25 +1774,28 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 const int kind[2] = {0, 0};
                 RecVals r;
                 r.n[0] = r.n[4] = -1;
+                if (D.prefetch > 1) {
+                    // the group's prefetch candidates into shared memory, one
+                    // candidate per thread (its five fields loaded together)
+                    const int ncand = c.nb * kPrefetchCand;
+                    for (int e = threadIdx.x; e < ncand; e += blockDim.x) {
+                        const Partial *pr = &all[e / kPrefetchCand];
+                        const int t = e % kPrefetchCand;
+                        double cv;
+                        int cpos, cloc, crow, cy;
+                        if (c.nb == 1) {
+                            cv = pr->cv[t]; cpos = pr->cpos[t]; cloc = pr->cloc[t]; crow = pr->crow[t]; cy = pr->cy[t];
+                        } else {
+                            cv = __ldcg(&pr->cv[t]); cpos = __ldcg(&pr->cpos[t]); cloc = __ldcg(&pr->cloc[t]);
+                            crow = __ldcg(&pr->crow[t]); cy = __ldcg(&pr->cy[t]);
+                        }
+                        c.pt->v[e] = cv; c.pt->pos[e] = cpos; c.pt->loc[e] = cloc; c.pt->row[e] = crow; c.pt->y[e] = cy;
+                    }
+                }
                 if (threadIdx.x < c.nb) {
                     rec_load(c, &all[threadIdx.x], r, 1, 0);
                     better_max(v[0], ix[0], r.v[0], r.n[0]);
                     better_max(v[1], ix[1], r.v[3], r.n[4]);
-                    if (D.prefetch > 1) {
-                        // this block's prefetch candidates into shared memory
-                        const Partial *pr = &all[threadIdx.x];
-                        for (int t = 0; t < kPrefetchCand; t++) {
-                            const int e = threadIdx.x * kPrefetchCand + t;
-                            if (c.nb == 1) {
-                                c.pt->v[e] = pr->cv[t]; c.pt->pos[e] = pr->cpos[t];
-                                c.pt->loc[e] = pr->cloc[t]; c.pt->row[e] = pr->crow[t]; c.pt->y[e] = pr->cy[t];
-                            } else {
-                                c.pt->v[e] = __ldcg(&pr->cv[t]); c.pt->pos[e] = __ldcg(&pr->cpos[t]);
-                                c.pt->loc[e] = __ldcg(&pr->cloc[t]); c.pt->row[e] = __ldcg(&pr->crow[t]);
-                                c.pt->y[e] = __ldcg(&pr->cy[t]);
-                            }
-                        }
-                    }
                 }
                 block_reduce<2>(sh.red, v, ix, kind);
                 // the thread holding a winning record publishes its payload
@@ -1823,35 +1849,33 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                     const int ncand = c.nb * kPrefetchCand;
                     const int want = D.prefetch - sh.nfill;
                     if (threadIdx.x < 32) {
-                        double lv[kPrefetchMax];
-                        int li[kPrefetchMax];
-                        int cnt = 0;
-                        for (int e = threadIdx.x; e < ncand; e += 32) {
-                            const int pos = c.pt->pos[e];
-                            const double v = c.pt->v[e];
-                            if (pos < 0 || pos == i0_prev_guard(sh, 0) || pos == i0_prev_guard(sh, 1) || !(v > -SVMB_INF)) continue;
-                            if (cnt == want && !(v > lv[cnt - 1])) continue;
-                            int q = cnt < want ? cnt++ : want - 1;     // insertion into the descending list
-                            while (q > 0 && lv[q - 1] < v) { lv[q] = lv[q - 1]; li[q] = li[q - 1]; q--; }
-                            lv[q] = v;
-                            li[q] = e;
-                        }
-                        int head = 0, got = 0;
+                        // `want` rounds of a warp argmax over the candidates
+                        // (largest priority, the lowest table index on ties); lane
+                        // L owns entries L + 32j and marks the ones taken in a mask
+                        const int lane = threadIdx.x;
+                        const int g0 = i0_prev_guard(sh, 0), g1 = i0_prev_guard(sh, 1);
+                        unsigned taken = 0;
+                        int got = 0;
                         for (; got < want; got++) {
-                            double bv = head < cnt ? lv[head] : -SVMB_INF;
-                            int bl = head < cnt ? (int)threadIdx.x : 32;
+                            double bv = -SVMB_INF;
+                            int be = 0x7fffffff;
+                            for (int e = lane, j = 0; e < ncand; e += 32, j++) {
+                                if ((taken >> j) & 1u) continue;
+                                const int pos = c.pt->pos[e];
+                                const double v = c.pt->v[e];
+                                if (pos < 0 || pos == g0 || pos == g1 || !(v > -SVMB_INF)) continue;
+                                if (v > bv) { bv = v; be = e; }
+                            }
                             for (int o = 16; o > 0; o >>= 1) {
                                 const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                                const int ol = __shfl_xor_sync(0xffffffffu, bl, o);
-                                if (ov > bv || (ov == bv && ol < bl)) { bv = ov; bl = ol; }
+                                const int oe = __shfl_xor_sync(0xffffffffu, be, o);
+                                if (ov > bv || (ov == bv && oe < be)) { bv = ov; be = oe; }
                             }
-                            if (bl == 32) break;
-                            if ((int)threadIdx.x == bl) {
-                                sh.pick[got] = li[head];
-                                head++;
-                            }
+                            if (be == 0x7fffffff) break;
+                            if ((be & 31) == lane) taken |= 1u << (be >> 5);
+                            if (lane == 0) sh.pick[got] = be;
                         }
-                        if (threadIdx.x == 0) sh.npick = got;
+                        if (lane == 0) sh.npick = got;
                     }
                     __syncthreads();
                     // the picks' cache sets, read by one thread per way in a single round trip
