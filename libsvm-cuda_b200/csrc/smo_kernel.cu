@@ -735,7 +735,9 @@ __device__ bool exchange(Ctx &c, Shared &sh)
         for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
             const long long t0 = clock64();
             long long spins = 0;
-            while (ld_acquire_i32(&all[b].seq) != want) {
+            // spin with relaxed loads; one acquire load of the awaited value
+            // then synchronizes with the record's release store
+            while (ld_relaxed_i32(&all[b].seq) != want) {
                 if ((++spins & 63) == 0) {
                     if (ld_relaxed_i32(&c.D->sync->error) != 0 || clock64() - t0 > kWaitTimeout) {
                         atomicExch(&c.D->sync->error, 1);
@@ -744,13 +746,13 @@ __device__ bool exchange(Ctx &c, Shared &sh)
                     }
                 }
             }
+            if (ok) (void)ld_acquire_i32(&all[b].seq);
         }
     }
+    // the pollers' acquire loads, followed by the barrier, order every later
+    // read of this block after the other blocks' releases
     ok = __syncthreads_and(ok);
-    if (threadIdx.x == 0) {
-        if (c.nb > 1) __threadfence();
-        cache_rotate(sh.cs, c.D->cache, c.rank);
-    }
+    if (threadIdx.x == 0) cache_rotate(sh.cs, c.D->cache, c.rank);
     c.phase++;
     __syncthreads();
     return ok != 0;
