@@ -278,16 +278,30 @@ void setup_train(const svm_problem *prob, const svm_parameter *param, const int 
             weighted_C[j] *= param->weight[i];
     }
     auto id = [&](int g) { return row_id ? row_id[tj.perm[g]] : g; };   // grouped index -> uploaded row id
+    // the one-vs-one subproblems in pair order (class i rows +1, then class j
+    // rows -1), built in parallel: they are independent
+    std::vector<std::pair<int, int>> pairs;
     for (int i = 0; i < nr_class; i++)
-        for (int j = i + 1; j < nr_class; j++) {
-            std::vector<int> r;
-            std::vector<signed char> y;
-            std::vector<double> yv;
-            for (int k = 0; k < tj.count[i]; k++) { r.push_back(id(tj.start[i] + k)); y.push_back(+1); yv.push_back(+1); }
-            for (int k = 0; k < tj.count[j]; k++) { r.push_back(id(tj.start[j] + k)); y.push_back(-1); yv.push_back(-1); }
-            tj.subs.push_back(make_sub(r, y, param, weighted_C[i], weighted_C[j]));
-            tj.subys.push_back(yv);
+        for (int j = i + 1; j < nr_class; j++) pairs.emplace_back(i, j);
+    const size_t first = tj.subs.size();
+    tj.subs.resize(first + pairs.size());
+    tj.subys.resize(first + pairs.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int q = 0; q < (int)pairs.size(); q++) {
+        const int i = pairs[q].first, j = pairs[q].second;
+        const int n = tj.count[i] + tj.count[j];
+        std::vector<int> r(n);
+        std::vector<signed char> y(n);
+        std::vector<double> yv(n);
+        for (int k = 0; k < tj.count[i]; k++) { r[k] = id(tj.start[i] + k); y[k] = +1; yv[k] = +1; }
+        for (int k = 0; k < tj.count[j]; k++) {
+            r[tj.count[i] + k] = id(tj.start[j] + k);
+            y[tj.count[i] + k] = -1;
+            yv[tj.count[i] + k] = -1;
         }
+        tj.subs[first + q] = make_sub(r, y, param, weighted_C[i], weighted_C[j]);
+        tj.subys[first + q] = std::move(yv);
+    }
     tj.own = make_solve_params(param);
 }
 
