@@ -901,10 +901,11 @@ __device__ void accumulate_rows(Ctx &c, Shared &sh, int src_end, int pick_free_o
 // if 16(w/4) < N, columns 16(w/4)..+15 (sources) of the tile in acc[16].
 //
 // Operand stages (kTcStages deep) are filled by cp.async with 16-byte pieces
-// of gathered rows into 128B-swizzled K-major tiles; thread 0 issues the
-// MMAs and commits each step to its stage's mbarrier.  Every commit is waited
-// for exactly once, in order, so the phase parities follow from the running
-// step counter c.tc_g.  A wait that times out sets the group's error flag and
+// of gathered rows into 128B-swizzled K-major tiles by all warps but the
+// last; lane 0 of the last warp issues the MMAs and commits each step to its
+// stage's mbarrier, queueing step g before step g-1 is waited for.  Every
+// commit is waited for exactly once, in order, so the phase parities follow
+// from the running step counter c.tc_g.  A wait that times out sets the group's error flag and
 // the product returns false.
 template <class Epi>
 __device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool global_targets, Epi &&epi)
