@@ -40,6 +40,10 @@ from svmb200 import cabi, datagen  # noqa: E402
 WORKLOAD = "ovo45_rbf_d256: 10 classes 12000*0.8^k (53646 rows), d=256, RBF g=1/256, C=1, eps=1e-3, 100MB cache/solve"
 D = 256
 GAMMA = 1.0 / 256
+# DRAM bytes read + written by one batched launch of this workload, from an ncu
+# capture (dram__bytes_read.sum 9.16 GB + dram__bytes_write.sum 2.39 GB; one
+# pass, so the full-size launch was captured); a profiler figure, not timed here
+TRAFFIC_PER_LAUNCH = 11.55e9
 CVAL = 1.0
 
 
@@ -519,7 +523,10 @@ def main():
                     "h2d_bytes_per_step": int(sum(h2d) / len(h2d)), "d2h_bytes_per_step": int(sum(d2h) / len(d2h)),
                     "api": "svm_train (svm.h) from pinned host svm_node rows"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": "smo_persistent<FORM_EXACT>",
+                         "traffic": TRAFFIC_PER_LAUNCH if world == 1 else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one steady-state "
+                                           "launch of this workload (profiles/smo_persistent_exact_ovo45_dram.txt)",
+                         "kernel": "smo_persistent<FORM_EXACT>",
                          "algorithmic_bytes_per_launch": abytes, "kernel_ms": kavg * 1e3,
                          "peak_kind": f"{peak_kind} hbm_gbs"},
             "cpu_baseline": cpu,
