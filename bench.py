@@ -460,6 +460,10 @@ def main():
     prob.l = p.n
     prob.y = yv.ctypes.data_as(C.POINTER(C.c_double))
     prob.x = C.cast(ptrs.ctypes.data, C.POINTER(C.POINTER(cabi.svm_node)))
+    # training output goes to the library's own no-op print function (a
+    # Python print callback would put interpreter time into the measurement)
+    silent = cabi.PRINT_FUNC(("svmb_print_nothing", eng.lib))
+    eng.lib.svm_set_print_string_function(silent)
     for _ in range(args.warmup):
         m = eng.lib.svm_train(C.byref(prob), C.byref(prm))
         eng.lib.svm_free_and_destroy_model(C.byref(m))
@@ -481,6 +485,7 @@ def main():
         h2d.append(hb1.value - hb0.value)
         d2h.append(db1.value - db0.value)
         eng.lib.svm_free_and_destroy_model(C.byref(m))
+    eng.lib.svm_set_print_string_function(eng._cb)
     e2e_mean = sum(e2e_ms) / len(e2e_ms)
     if world > 1:
         tm = torch.tensor([e2e_mean], device="cuda", dtype=torch.float64)

@@ -87,6 +87,10 @@ long long svmb_kernel_launches(void);
 void svmb_transfer_bytes(long long *h2d, long long *d2h);
 int svmb_version(void);                         /* LIBSVM_VERSION * 100 + engine revision */
 int svmb_device_available(void);                /* 1 if a CUDA device can be used */
+/* A print function that discards its text: svm_set_print_string_function(
+ * svmb_print_nothing) silences training output without a call back into the
+ * caller (no counterpart in the reference, whose callers write their own). */
+void svmb_print_nothing(const char *s);
 
 /* Process-wide engine options used by svm_train / svm_cross_validation:
  *   "form"   SVMB_FORM_EXACT (default), SVMB_FORM_FP32, SVMB_FORM_BF16X3 or SVMB_FORM_FP16X3

@@ -935,4 +935,6 @@ void svm_set_print_string_function(void (*print_func)(const char *))
     svm_print_string = print_func == NULL ? &print_string_stdout : print_func;
 }
 
+void svmb_print_nothing(const char *) {}
+
 }  // extern "C"
