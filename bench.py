@@ -267,20 +267,31 @@ def cv_grid_extra(eng):
     Cs = [c for c in (0.5, 1.0, 2.0, 4.0, 8.0) for g in (1 / 256, 4 / 256)]
     gs = [g for c in (0.5, 1.0, 2.0, 4.0, 8.0) for g in (1 / 256, 4 / 256)]
     libc = ctypes.CDLL(None)
-    libc.srand(1)
-    t0 = time.perf_counter()
-    grid = eng.cross_validation_grid(tr, prm, 5, Cs, gs)
-    t_grid = time.perf_counter() - t0
-    nsub = len(eng.last_stats())
-    t_seq = 0.0
-    same = True
-    for q in range(len(Cs)):
-        p2 = cabi.make_param(svm_type=0, kernel_type=2, gamma=gs[q], C_=Cs[q], cache_size=100.0, eps=1e-3, shrinking=1)
+    # both sides with the autotuner off (the same fixed launch rules) and after
+    # one untimed call each (row pool, first-use costs)
+    eng.set_option("autotune", 0)
+    try:
+        libc.srand(1)
+        eng.cross_validation_grid(tr, prm, 5, Cs, gs)
+        libc.srand(1)
+        eng.cross_validation(tr, prm, 5)
         libc.srand(1)
         t0 = time.perf_counter()
-        one = eng.cross_validation(tr, p2, 5)
-        t_seq += time.perf_counter() - t0
-        same = same and bool(np.array_equal(one, grid[q]))
+        grid = eng.cross_validation_grid(tr, prm, 5, Cs, gs)
+        t_grid = time.perf_counter() - t0
+        nsub = len(eng.last_stats())
+        t_seq = 0.0
+        same = True
+        for q in range(len(Cs)):
+            p2 = cabi.make_param(svm_type=0, kernel_type=2, gamma=gs[q], C_=Cs[q], cache_size=100.0, eps=1e-3,
+                                 shrinking=1)
+            libc.srand(1)
+            t0 = time.perf_counter()
+            one = eng.cross_validation(tr, p2, 5)
+            t_seq += time.perf_counter() - t0
+            same = same and bool(np.array_equal(one, grid[q]))
+    finally:
+        eng.set_option("autotune", 1)
     acc = [float((grid[q] == tr.y).mean()) for q in range(len(Cs))]
     return {"workload": f"5-fold CV, 10 (C,gamma) points, 10 classes {sizes[0]}*0.8^k ({tr.n} rows), d=256",
             "subproblems": nsub, "grid_seconds": t_grid, "one_point_at_a_time_seconds": t_seq,

@@ -432,6 +432,11 @@ int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, i
     }
     for (long long k = 0; k < (long long)npoints * l; k++) target[k] = NAN;
     if (!train_supported(param)) return -1;
+    const bool trace = getenv("SVMB_TRACE") && *getenv("SVMB_TRACE") == '1';
+    const auto c0 = std::chrono::steady_clock::now();
+    auto since = [&](std::chrono::steady_clock::time_point a) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+    };
     // all rows once, in the problem's order (row id = index in prob)
     svmb::DeviceRows rows;
     if (l > 0 && svmb::upload_rows(prob->x, l, rows, svmb::api_force_layout(), 0, svmb::kAllocPooled) != 0) {
@@ -479,10 +484,14 @@ int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, i
         std::lock_guard<std::mutex> g(g_stats_mu);
         g_last_stats.clear();
     }
+    const double t_setup = since(c0);
+    const auto c1 = std::chrono::steady_clock::now();
     if (!all.empty() && svmb::solve_batch(rows, all, jobs[0].own, res, 0) != 0) {
         info("ERROR: %s\n", svmb::last_error());
         return -1;
     }
+    const double t_solve = since(c1);
+    const auto c2 = std::chrono::steady_clock::now();
     for (int q = 0; q < npoints; q++)
         for (int i = 0; i < nr_fold; i++) {
             const size_t k = (size_t)q * nr_fold + i;
@@ -495,6 +504,9 @@ int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, i
                 for (int j = begin; j < end; j++) target[(size_t)q * l + perm[j]] = lab[j - begin];
             svm_free_and_destroy_model(&m);
         }
+    if (trace)
+        fprintf(stderr, "[svmb] cv_grid points=%d folds=%d subproblems=%zu setup=%.2fms solve=%.2fms predict=%.2fms\n", npoints,
+                nr_fold, all.size(), t_setup, t_solve, since(c2));
     return 0;
 }
 
