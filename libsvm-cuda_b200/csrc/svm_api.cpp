@@ -56,6 +56,17 @@ void info(const char *fmt, ...)
     (*svm_print_string)(buf);
 }
 
+// the same text appended to `out` (printed later, in order)
+void info_to(std::string &out, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    out += buf;
+}
+
 // engine options settable through svmb_set_option (process wide)
 struct Options {
     int form = svmb::FORM_EXACT;
@@ -162,19 +173,21 @@ struct DecisionFunction {
 };
 
 // Post-processing of one solve (svm.cpp:1517-1532, :1572-1587 and svm_train_one :1739-1766).
+// One subproblem's decision function and statistics; its messages go to
+// `log` (the caller prints the logs of all pairs in pair order).
 DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResult &R, const svm_parameter *param,
-                              const double *yvals)
+                              const double *yvals, std::string &log, svmb_solve_stats &st)
 {
     DecisionFunction f;
     const int l = (int)sp.rows.size();
     f.alpha = R.alpha;
     double rho = R.out.rho, obj = R.out.obj;
     double upper_p, upper_n;
-    info("\noptimization finished, #iter = %lld\n", R.out.iters);
-    if (R.out.status == 1) fprintf(stderr, "\nWARNING: reaching max number of iterations\n");
+    info_to(log, "\noptimization finished, #iter = %lld\n", R.out.iters);
+    // (the max_iter warning goes to stderr from the caller, in pair order)
     if (sp.nu) {
         const double r = R.out.r;
-        info("C = %f\n", 1 / r);
+        info_to(log, "C = %f\n", 1 / r);
         for (int i = 0; i < l; i++) f.alpha[i] *= sp.y[i] / r;
         rho /= r;
         obj /= (r * r);
@@ -182,13 +195,13 @@ DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResul
     } else {
         double sum_alpha = 0;
         for (int i = 0; i < l; i++) sum_alpha += f.alpha[i];
-        if (sp.Cp == sp.Cn) info("nu = %f\n", sum_alpha / (sp.Cp * l));
+        if (sp.Cp == sp.Cn) info_to(log, "nu = %f\n", sum_alpha / (sp.Cp * l));
         for (int i = 0; i < l; i++) f.alpha[i] *= sp.y[i];
         upper_p = sp.Cp;
         upper_n = sp.Cn;
     }
     f.rho = rho;
-    info("obj = %f, rho = %f\n", obj, rho);
+    info_to(log, "obj = %f, rho = %f\n", obj, rho);
     int nSV = 0, nBSV = 0;
     for (int i = 0; i < l; i++) {
         if (fabs(f.alpha[i]) > 0) {
@@ -200,8 +213,7 @@ DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResul
             }
         }
     }
-    info("nSV = %d, nBSV = %d\n", nSV, nBSV);
-    svmb_solve_stats st;
+    info_to(log, "nSV = %d, nBSV = %d\n", nSV, nBSV);
     memset(&st, 0, sizeof st);
     st.iters = R.out.iters;
     st.obj = obj;
@@ -222,10 +234,6 @@ DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResul
     st.prefetched = R.out.prefetched;
     st.prefetch_used = R.out.prefetch_used;
     for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
-    {
-        std::lock_guard<std::mutex> g(g_stats_mu);
-        g_last_stats.push_back(st);
-    }
     return f;
 }
 
@@ -312,7 +320,19 @@ svm_model *assemble_model(const TrainJob &tj, const std::vector<svmb::SolveResul
     const int l = tj.l, nr_class = tj.nr_class;
     const std::vector<int> &start = tj.start, &count = tj.count;
     std::vector<DecisionFunction> f(tj.subs.size());
-    for (size_t p = 0; p < tj.subs.size(); p++) f[p] = finish_solve(tj.subs[p], res[first + p], param, tj.subys[p].data());
+    // the pairs' decision functions in parallel; their messages, warnings and
+    // statistics then in pair order
+    std::vector<std::string> logs(tj.subs.size());
+    std::vector<svmb_solve_stats> sts(tj.subs.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int p = 0; p < (int)tj.subs.size(); p++)
+        f[p] = finish_solve(tj.subs[p], res[first + p], param, tj.subys[p].data(), logs[p], sts[p]);
+    for (size_t p = 0; p < tj.subs.size(); p++) {
+        (*svm_print_string)(logs[p].c_str());
+        if (res[first + p].out.status == 1) fprintf(stderr, "\nWARNING: reaching max number of iterations\n");
+        std::lock_guard<std::mutex> g(g_stats_mu);
+        g_last_stats.push_back(sts[p]);
+    }
     svm_model *model = (svm_model *)malloc(sizeof(svm_model));
     model->param = *param;
     model->free_sv = 0;
