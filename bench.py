@@ -27,6 +27,7 @@ import multiprocessing as mp
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -374,6 +375,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clocks-dir", default=None, help="where to keep the nvidia-smi clock samples (default: temp dir)")
     ap.add_argument("--no-extras", action="store_true", help="skip the precision-form, CV-grid and serving workloads")
     ap.add_argument("--profile-case", default=None, help="run one solver launch for a profiler capture and exit")
     args = ap.parse_args()
@@ -424,8 +426,8 @@ def main():
     tuned = eng.autotune_last()
     for _ in range(args.warmup):
         res.solve_many(rows, ys, params)
-    clocks = Clocks(local, os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv")) if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else Clocks(local, f"/tmp/svmb_clocks_{rank}.csv")
+    clocks_dir = args.clocks_dir or tempfile.gettempdir()
+    clocks = Clocks(local, os.path.join(clocks_dir, f"svmb_clocks_rank{rank}.csv"))
     step_ms, kern_s, alg_bytes, stats_all = [], [], [], []
     launches0 = eng.launches()
     for _ in range(args.steps):
