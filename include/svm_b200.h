@@ -165,14 +165,16 @@ int svmb_solve_many_csr(int n, int d, const long long *rowptr, const int *col, c
  * counterpart in the reference.  It is for callers that cannot allocate device
  * memory once they are running (a server with a fixed device-memory pool, a
  * host application that owns every allocation): rows X [n][ld] (float32,
- * row-major, ld a multiple of 4), labels y[n] (y > 0 is the positive class)
+ * row-major, ld a multiple of 4, X 16-byte aligned), labels y[n] (y > 0 is the positive class)
  * and alpha_out[n] are DEVICE pointers the caller owns; params and stats are
  * host pointers (stats may be NULL; its nr_sv/nr_bsv/seconds are not filled).
  * All solver state lives in a fixed 8 MiB workspace compiled into the library
  * (held by every GPU that loads it, until exit), so n is limited to 16384 and
  * the Q-row cache to what remains of the workspace; larger n is rejected.
  * The first call on each device looks up the workspace address, so make it
- * before any stream capture.  Calls share the workspace: two calls whose work
+ * before any stream capture; the address is kept for the process's lifetime,
+ * so it is stale after the caller resets the device (cudaDeviceReset).  Calls
+ * share the workspace: two calls whose work
  * overlaps on the GPU race on it.  `stream` is a cudaStream_t (NULL = legacy
  * default stream); the call returns after the solve has finished. */
 int svmb_solve_dense_noalloc(int n, int ld, const float *X, const double *y, const svmb_params *params,

@@ -14,7 +14,8 @@
 // The workspace is a file-scope __device__ array, so every GPU that loads the
 // library holds it until the process exits.  Its address is looked up once per
 // device with cudaGetSymbolAddress (the first call on a device does this, so
-// make that first call before any stream capture).  All calls share the one
+// make that first call before any stream capture) and kept for the life of the
+// process: after a cudaDeviceReset by the caller the kept address is stale.  All calls share the one
 // workspace and it keeps the previous call's contents: each call re-clears
 // what the solver needs to start from zero, and two calls whose work overlaps
 // on the GPU (different streams, different host threads) race on it.
@@ -22,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 
@@ -79,6 +81,9 @@ extern "C" int svmb_solve_dense_noalloc(int n, int ld, const float *X, const dou
         return -1;
     }
     if (ld < 4 || ld % 4 != 0) { set_error("svmb_solve_dense_noalloc: ld must be a positive multiple of 4"); return -1; }
+    // rows are read as 16-byte pieces (float4 loads, cp.async): a misaligned
+    // base would fault inside the kernel, so it is refused before any launch
+    if (((uintptr_t)X & 15) != 0) { set_error("svmb_solve_dense_noalloc: X must be 16-byte aligned"); return -1; }
     if (params->svm_type != C_SVC) { set_error("svmb_solve_dense_noalloc: only C_SVC"); return -1; }
     if (params->kernel_type < LINEAR || params->kernel_type > SIGMOID) { set_error("kernel_type must be LINEAR, POLY, RBF or SIGMOID"); return -1; }
     if (params->C_pos <= 0 || params->C_neg <= 0 || params->eps <= 0 || params->gamma < 0 || params->degree < 0) {

@@ -56,15 +56,16 @@ void info(const char *fmt, ...)
     (*svm_print_string)(buf);
 }
 
-// the same text appended to `out` (printed later, in order)
-void info_to(std::string &out, const char *fmt, ...)
+// the text of one info() call kept as one entry of `out` (printed later, in
+// order, one print-hook call per entry as the reference makes them)
+void info_to(std::vector<std::string> &out, const char *fmt, ...)
 {
     char buf[1024];
     va_list ap;
     va_start(ap, fmt);
     vsnprintf(buf, sizeof buf, fmt, ap);
     va_end(ap);
-    out += buf;
+    out.emplace_back(buf);
 }
 
 // engine options settable through svmb_set_option (process wide)
@@ -176,7 +177,7 @@ struct DecisionFunction {
 // One subproblem's decision function and statistics; its messages go to
 // `log` (the caller prints the logs of all pairs in pair order).
 DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResult &R, const svm_parameter *param,
-                              const double *yvals, std::string &log, svmb_solve_stats &st)
+                              const double *yvals, std::vector<std::string> &log, svmb_solve_stats &st)
 {
     DecisionFunction f;
     const int l = (int)sp.rows.size();
@@ -322,14 +323,15 @@ svm_model *assemble_model(const TrainJob &tj, const std::vector<svmb::SolveResul
     std::vector<DecisionFunction> f(tj.subs.size());
     // the pairs' decision functions in parallel; their messages, warnings and
     // statistics then in pair order
-    std::vector<std::string> logs(tj.subs.size());
+    std::vector<std::vector<std::string>> logs(tj.subs.size());
     std::vector<svmb_solve_stats> sts(tj.subs.size());
 #pragma omp parallel for schedule(dynamic, 1)
     for (int p = 0; p < (int)tj.subs.size(); p++)
         f[p] = finish_solve(tj.subs[p], res[first + p], param, tj.subys[p].data(), logs[p], sts[p]);
     for (size_t p = 0; p < tj.subs.size(); p++) {
-        (*svm_print_string)(logs[p].c_str());
+        // the solver's max_iter warning precedes its "optimization finished" line (svm.cpp:779-787)
         if (res[first + p].out.status == 1) fprintf(stderr, "\nWARNING: reaching max number of iterations\n");
+        for (const std::string &line : logs[p]) (*svm_print_string)(line.c_str());
         std::lock_guard<std::mutex> g(g_stats_mu);
         g_last_stats.push_back(sts[p]);
     }

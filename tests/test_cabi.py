@@ -53,7 +53,7 @@ def test_struct_layout_matches_reference_abi():
         sizeof(struct svm_parameter), sizeof(struct svm_model), offsetof(struct svm_parameter, svm_type),
         offsetof(struct svm_parameter, shrinking), offsetof(struct svm_model, nr_class), offsetof(struct svm_model, free_sv));
       return 0; }'''
-    ref_inc = "/root/reference/libsvm"
+    ref_inc = os.path.join(os.environ.get("LIBSVM_REFERENCE", "/root/reference"), "libsvm")
     with tempfile.TemporaryDirectory() as td:
         res = {}
         for tag, inc in (("ours", INCLUDE), ("ref", ref_inc)):

@@ -38,16 +38,22 @@ def test_noalloc_matches_allocating_entry_point(engine, kernel, gamma, C_):
     out = torch.zeros(tr.n, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
     fn = _noalloc_fn(engine)
+    free_after = []
     for call in range(2):
         out.fill_(float("nan"))
         st = SolveStats()
         rc = fn(tr.n, X.shape[1], X.data_ptr(), y.data_ptr(), C.byref(params), out.data_ptr(), C.byref(st), None)
         assert rc == 0, engine.error()
+        torch.cuda.synchronize()
+        free_after.append(torch.cuda.mem_get_info()[0])
         got = out.cpu().numpy()
         np.testing.assert_allclose(got, want, rtol=0, atol=1e-9, err_msg=f"call {call}")
         assert st.iters == st_want["iters"]
         assert abs(st.rho - st_want["rho"]) <= 1e-9
         assert abs(st.obj - st_want["obj"]) <= 1e-9 * abs(st_want["obj"])
+    # the property the entry point exists for: a call takes no device memory
+    # (the first call may still load the module; the second must not allocate)
+    assert abs(free_after[1] - free_after[0]) <= 2 << 20, free_after
 
 
 def test_noalloc_rejects_sizes_beyond_the_workspace(engine):
@@ -60,3 +66,19 @@ def test_noalloc_rejects_sizes_beyond_the_workspace(engine):
     rc = fn(n, 4, X.data_ptr(), y.data_ptr(), C.byref(make_params()), out.data_ptr(), None, None)
     assert rc != 0
     assert "16384" in engine.error()
+
+
+def test_noalloc_rejects_a_misaligned_row_pointer(engine):
+    """Rows are read in 16-byte pieces; a view 4 bytes into a buffer is refused
+    before anything is launched, so the caller's context stays usable."""
+    import torch
+    n, ld = 64, 8
+    X = torch.zeros((n + 1) * ld, dtype=torch.float32, device="cuda")
+    y = torch.ones(n, dtype=torch.float64, device="cuda")
+    y[::2] = -1
+    out = torch.zeros(n, dtype=torch.float64, device="cuda")
+    fn = _noalloc_fn(engine)
+    rc = fn(n, ld, X.data_ptr() + 4, y.data_ptr(), C.byref(make_params()), out.data_ptr(), None, None)
+    assert rc != 0
+    assert "aligned" in engine.error()
+    torch.cuda.synchronize()
