@@ -50,21 +50,22 @@ typedef struct svmb_solve_stats {
 
 /* Parameters of a binary solve (the subset of svm_parameter the solver reads). */
 typedef struct svmb_params {
-    int svm_type;        /* C_SVC or NU_SVC */
+    int svm_type;        /* C_SVC, NU_SVC, ONE_CLASS, EPSILON_SVR or NU_SVR */
     int kernel_type;     /* LINEAR, POLY, RBF, SIGMOID */
     int degree;
     int shrinking;
     double gamma;
     double coef0;
-    double C_pos;        /* C-SVC: C for y>0 (reference solve_c_svc Cp) */
+    double C_pos;        /* C-SVC: C for y>0 (reference solve_c_svc Cp); epsilon-SVR / nu-SVR: C */
     double C_neg;        /* C-SVC: C for y<=0 (Cn) */
-    double nu;           /* nu-SVC */
+    double nu;           /* nu-SVC, one-class, nu-SVR */
     double eps;
     double cache_mb;     /* Q-row cache budget per solve, MB (svm_parameter.cache_size) */
     int form;            /* SVMB_FORM_* */
     int blocks;          /* thread blocks per solve; 0 = automatic */
     int prefetch;        /* kernel rows evaluated per cache-miss pass (1 = only the missing row); 0 = automatic */
     int gbar_mode;       /* SVMB_GBAR_*: how the gradient of the inactive variables is kept */
+    double p;            /* epsilon-SVR: half-width of the insensitive tube (svm_parameter.p) */
 } svmb_params;
 
 #define SVMB_GBAR_AUTO        0  /* incremental for EXACT and FP32, recomputed for the tensor forms */
@@ -136,15 +137,26 @@ int svmb_cross_validation_grid(const struct svm_problem *prob, const struct svm_
                                int npoints, const double *C, const double *gamma, double *target);
 
 /* Decision values of n rows in one device pass (the batched form of
- * svm_predict_values, reference svm.cpp:2569-2643).  labels[n];
- * dec_values may be NULL or [n][nr_class*(nr_class-1)/2]. */
+ * svm_predict_values, reference svm.cpp:2569-2643).  labels[n] (one-class:
+ * +1/-1; epsilon-SVR / nu-SVR: the predicted value); dec_values may be NULL
+ * or [n][nr_class*(nr_class-1)/2] (one value per row for one-class and SVR). */
 int svmb_predict_batch(const struct svm_model *model, const struct svm_node *const *rows, int n,
                        double *labels, double *dec_values);
 
-/* One binary solve from host CSR rows (0-based columns, n rows, d columns).
- * y[i] > 0 is the positive class.  alpha_out[n] receives the signed
- * coefficients y_i*alpha_i (nu-SVC: divided by r), i.e. the reference's
- * decision_function.alpha (svm.cpp:1532, :1578-1584); stats may be NULL.
+/* Labels and class probabilities of n rows (the batched form of
+ * svm_predict_probability, reference svm.cpp:2660-2697) of a C-SVC / nu-SVC
+ * model trained with probability = 1: the pairs' decision values in one
+ * device pass, then each pair's sigmoid and the pairwise coupling.
+ * labels[n], prob_estimates[n][nr_class] in the model's label order. */
+int svmb_predict_probability_batch(const struct svm_model *model, const struct svm_node *const *rows, int n,
+                                   double *labels, double *prob_estimates);
+
+/* One solve from host CSR rows (0-based columns, n rows, d columns) in the
+ * formulation params->svm_type.  Classifiers: y[i] > 0 is the positive class;
+ * one-class: y is ignored; SVR: y are the regression targets.  alpha_out[n]
+ * receives the reference's decision_function.alpha: y_i*alpha_i for C-SVC
+ * (nu-SVC: divided by r), alpha_i for one-class, alpha_i - alpha*_i for SVR
+ * (svm.cpp:1532, :1578-1584, :1650-1655, :1691-1692); stats may be NULL.
  * Host buffers; host<->device copies are part of the call. */
 int svmb_solve_binary_csr(int n, int d, const long long *rowptr, const int *col, const float *val,
                           const double *y, const svmb_params *params, double *alpha_out,
@@ -179,6 +191,17 @@ int svmb_solve_many_csr(int n, int d, const long long *rowptr, const int *col, c
  * default stream); the call returns after the solve has finished. */
 int svmb_solve_dense_noalloc(int n, int ld, const float *X, const double *y, const svmb_params *params,
                              double *alpha_out, svmb_solve_stats *stats, void *stream);
+
+/* Read a libsvm text file ("label idx:val ...") with the acceptance rules of
+ * the reference's read_problem (svm-train/svm-train.c:288-389), parsed by all
+ * host threads.  On success prob->l, prob->y, prob->x (rows terminated by
+ * index -1, pointing into *x_space) and *max_index (largest feature index, 0
+ * if none) are set; free them with svmb_free_problem.  Returns -1 if the file
+ * cannot be read, -2 for a malformed line, whose 1-based number goes to
+ * *bad_line (may be NULL), as the reference's "Wrong input format at line N". */
+int svmb_read_problem(const char *path, struct svm_problem *prob, struct svm_node **x_space, int *max_index,
+                      long long *bad_line);
+void svmb_free_problem(struct svm_problem *prob, struct svm_node *x_space);
 
 /* Resident rows: upload once, solve many times (the data stays in HBM). */
 typedef struct svmb_rows svmb_rows;

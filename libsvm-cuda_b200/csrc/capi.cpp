@@ -13,6 +13,7 @@
 #include "predict.hpp"
 #include "svm_b200.h"
 #include "capi_internal.hpp"
+#include "formulation.hpp"
 
 namespace svmb {
 int api_set_option(const char *name, long long value);
@@ -29,14 +30,19 @@ namespace capi {
 int check_params(const svmb_params *p)
 {
     if (!p) { svmb::set_error("params is NULL"); return -1; }
-    if (p->svm_type != C_SVC && p->svm_type != NU_SVC) { svmb::set_error("svm_type must be C_SVC or NU_SVC"); return -1; }
+    if (p->svm_type < C_SVC || p->svm_type > NU_SVR) { svmb::set_error("unknown svm_type"); return -1; }
     if (p->kernel_type < LINEAR || p->kernel_type > SIGMOID) { svmb::set_error("kernel_type must be LINEAR, POLY, RBF or SIGMOID"); return -1; }
     if (p->gamma < 0) { svmb::set_error("gamma < 0"); return -1; }
     if (p->degree < 0) { svmb::set_error("degree of polynomial kernel < 0"); return -1; }
     if (p->eps <= 0) { svmb::set_error("eps <= 0"); return -1; }
     if (p->cache_mb <= 0) { svmb::set_error("cache_size <= 0"); return -1; }
     if (p->svm_type == C_SVC && (p->C_pos <= 0 || p->C_neg <= 0)) { svmb::set_error("C <= 0"); return -1; }
-    if (p->svm_type == NU_SVC && (p->nu <= 0 || p->nu > 1)) { svmb::set_error("nu <= 0 or nu > 1"); return -1; }
+    if ((p->svm_type == EPSILON_SVR || p->svm_type == NU_SVR) && p->C_pos <= 0) { svmb::set_error("C <= 0"); return -1; }
+    if ((p->svm_type == NU_SVC || p->svm_type == ONE_CLASS || p->svm_type == NU_SVR) && (p->nu <= 0 || p->nu > 1)) {
+        svmb::set_error("nu <= 0 or nu > 1");
+        return -1;
+    }
+    if (p->svm_type == EPSILON_SVR && p->p < 0) { svmb::set_error("p < 0"); return -1; }
     if (p->form != SVMB_FORM_EXACT && p->form != SVMB_FORM_FP32 && p->form != SVMB_FORM_BF16X3 &&
         p->form != SVMB_FORM_FP16X3) { svmb::set_error("unknown form"); return -1; }
     if (p->gbar_mode < SVMB_GBAR_AUTO || p->gbar_mode > SVMB_GBAR_RECOMPUTE) { svmb::set_error("unknown gbar_mode"); return -1; }
@@ -60,62 +66,40 @@ SolveParams to_solve_params(const svmb_params &p)
     return prm;
 }
 
-// one binary subproblem in the formulation of solve_c_svc / solve_nu_svc
-// (reference svm.cpp:1500-1588): labels, initial alpha, linear term, bounds
+// one problem in the reference's formulation of params.svm_type
+// (svm.cpp:1500-1699), over the rows with ids rows[0..l)
 int make_subproblem(const svmb_params &p, int l, const int *rows, const double *y, int nrows, SubProblem &sp)
 {
     if (l < 0) { set_error("inst_ptr must be non-decreasing"); return -1; }
-    sp.rows.assign(rows, rows + l);
-    for (int r : sp.rows)
-        if (r < 0 || r >= nrows) { set_error("row id out of range"); return -1; }
-    sp.y.resize(l);
-    for (int i = 0; i < l; i++) sp.y[i] = y[i] > 0 ? +1 : -1;
-    sp.alpha0.assign(l, 0.0);
-    sp.p.assign(l, 0.0);
+    for (int i = 0; i < l; i++)
+        if (rows[i] < 0 || rows[i] >= nrows) { set_error("row id out of range"); return -1; }
     if (p.svm_type == NU_SVC) {
-        // solve_nu_svc initial point (reference svm.cpp:1546-1564)
+        // the feasibility test of svm_check_parameter (svm.cpp:3164-3213)
         int npos = 0, nneg = 0;
-        for (int i = 0; i < l; i++) (sp.y[i] > 0 ? npos : nneg)++;
+        for (int i = 0; i < l; i++) (y[i] > 0 ? npos : nneg)++;
         if (p.nu * l / 2 > std::min(npos, nneg)) { set_error("specified nu is infeasible"); return -1; }
-        double sum_pos = p.nu * l / 2, sum_neg = p.nu * l / 2;
-        for (int i = 0; i < l; i++) {
-            if (sp.y[i] == +1) { sp.alpha0[i] = std::min(1.0, sum_pos); sum_pos -= sp.alpha0[i]; }
-            else { sp.alpha0[i] = std::min(1.0, sum_neg); sum_neg -= sp.alpha0[i]; }
-        }
-        sp.nu = 1;
-        sp.Cp = sp.Cn = 1.0;
-    } else {
-        for (int i = 0; i < l; i++) sp.p[i] = -1;
-        sp.Cp = p.C_pos;
-        sp.Cn = p.C_neg;
     }
-    return 0;
+    return formulate(p.svm_type, rows, y, l, p.C_pos, p.C_neg, p.C_pos, p.nu, p.p, sp);
 }
 
-// signed coefficients y_i alpha_i (nu-SVC: / r) and the statistics of one solve
-void finish_instance(const SubProblem &sp, const SolveResult &R, double *alpha_out, svmb_solve_stats *stats)
+// coefficients per point (svm_train_one's decision function: y_i alpha_i,
+// nu-SVC / r, SVR alpha_i - alpha*_i) and the statistics of one solve
+void finish_instance(const svmb_params &p, const SubProblem &sp, const SolveResult &R, const double *y, int l,
+                     double *alpha_out, svmb_solve_stats *stats)
 {
-    const int l = (int)sp.rows.size();
-    double rho = R.out.rho, obj = R.out.obj, up = sp.Cp, un = sp.Cn;
-    for (int i = 0; i < l; i++) {
-        double v = R.alpha[i];
-        if (sp.nu) v *= sp.y[i] / R.out.r;
-        else v *= sp.y[i];
-        alpha_out[i] = v;
-    }
-    if (sp.nu) {
-        rho /= R.out.r;
-        obj /= (R.out.r * R.out.r);
-        up = un = 1 / R.out.r;
-    }
+    Decision f;
+    decide(p.svm_type, sp, R, y, l, f);
+    for (int i = 0; i < l; i++) alpha_out[i] = f.coef[i];
     if (!stats) return;
     svmb_solve_stats &st = *stats;
     memset(&st, 0, sizeof st);
     st.iters = R.out.iters;
-    st.obj = obj;
-    st.rho = rho;
+    st.obj = f.obj;
+    st.rho = f.rho;
     st.r = R.out.r;
     st.l = l;
+    st.nr_sv = f.nSV;
+    st.nr_bsv = f.nBSV;
     st.status = R.out.status;
     st.active_size = R.out.active_size;
     st.seconds = R.seconds;
@@ -128,13 +112,6 @@ void finish_instance(const SubProblem &sp, const SolveResult &R, double *alpha_o
     st.prefetched = R.out.prefetched;
     st.prefetch_used = R.out.prefetch_used;
     for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
-    for (int i = 0; i < l; i++) {
-        const double v = alpha_out[i];
-        if (v != 0) {
-            st.nr_sv++;
-            if (fabs(v) >= (sp.y[i] > 0 ? up : un)) st.nr_bsv++;
-        }
-    }
 }
 
 int solve_many(const DeviceRows &rows, int ninst, const int *inst_ptr, const int *inst_rows, const double *inst_y,
@@ -161,7 +138,8 @@ int solve_many(const DeviceRows &rows, int ninst, const int *inst_ptr, const int
     std::vector<SolveResult> res;
     if (solve_batch(rows, subs, own[0], res, 0) != 0) return -1;
     for (int k = 0; k < ninst; k++)
-        finish_instance(subs[k], res[k], alpha_out + inst_ptr[k], stats ? &stats[k] : nullptr);
+        finish_instance(params[k], subs[k], res[k], inst_y + inst_ptr[k], inst_ptr[k + 1] - inst_ptr[k],
+                        alpha_out + inst_ptr[k], stats ? &stats[k] : nullptr);
     return 0;
 }
 

@@ -25,19 +25,36 @@ namespace svmb {
 namespace {
 
 struct Rows {
-    // dense [n][ld] or CSR
+    // dense [n][ld] or CSR; each array grows on demand and is reused by later
+    // uploads into the same Rows (capacities in bytes)
     float *X = nullptr;
     long long *rowptr = nullptr;
     int *col = nullptr;
     float *val = nullptr;
+    size_t capX = 0, capRp = 0, capCol = 0, capVal = 0;
     int n = 0, ld = 0;
     bool dense = true;
     void release()
     {
         cudaFree(X); cudaFree(rowptr); cudaFree(col); cudaFree(val);
         X = nullptr; rowptr = nullptr; col = nullptr; val = nullptr;
+        capX = capRp = capCol = capVal = 0;
     }
 };
+
+// device buffer of at least `bytes`, reallocated only when it must grow
+template <typename T>
+cudaError_t grow(T *&p, size_t &cap, size_t bytes)
+{
+    if (bytes <= cap && p) return cudaSuccess;
+    cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+}
 
 __device__ __forceinline__ double powi_p(double base, int times)
 {
@@ -178,12 +195,14 @@ struct Session {
     double rho0 = 0;
     // device copy
     Rows sv;
+    Rows sv_csr;                // CSR copy of dense SVs for the merge path (made on first need)
     int d = 0, base = 1;
     double *coef = nullptr, *rho = nullptr;
     int *start = nullptr, *nsv = nullptr;
     void release()
     {
         sv.release();
+        sv_csr.release();
         cudaFree(coef); cudaFree(rho); cudaFree(start); cudaFree(nsv);
         coef = rho = nullptr;
         start = nsv = nullptr;
@@ -193,6 +212,14 @@ struct Session {
 std::mutex g_mu;
 std::map<const svm_model *, std::unique_ptr<Session>> g_sessions;
 int g_predict_form = FORM_EXACT;
+
+// Per-process prediction buffers, grown on demand and kept (a loop of
+// single-row svm_predict calls allocates nothing after its first call).
+struct Workspace {
+    double *kv = nullptr, *dec = nullptr;
+    size_t cap_kv = 0, cap_dec = 0;
+    Rows T;                     // test rows of the current chunk
+} g_ws;
 
 #define PK(call)                                                                  \
     do {                                                                          \
@@ -216,7 +243,7 @@ int upload_nodes(const svm_node *const *x, int n, int d, int base, bool dense, R
                 const int c = p->index - base;
                 if (c >= 0 && c < out.ld) h[(size_t)r * out.ld + c] = (float)p->value;
             }
-        PK(cudaMalloc(&out.X, h.size() * sizeof(float)));
+        PK(grow(out.X, out.capX, h.size() * sizeof(float)));
         PK(xfer(out.X, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
     } else {
         std::vector<long long> rp(n + 1, 0);
@@ -231,9 +258,9 @@ int upload_nodes(const svm_node *const *x, int n, int d, int base, bool dense, R
         }
         rp[n] = (long long)col.size();
         if (col.empty()) { col.push_back(0); val.push_back(0); }
-        PK(cudaMalloc(&out.rowptr, rp.size() * sizeof(long long)));
-        PK(cudaMalloc(&out.col, col.size() * sizeof(int)));
-        PK(cudaMalloc(&out.val, val.size() * sizeof(float)));
+        PK(grow(out.rowptr, out.capRp, rp.size() * sizeof(long long)));
+        PK(grow(out.col, out.capCol, col.size() * sizeof(int)));
+        PK(grow(out.val, out.capVal, val.size() * sizeof(float)));
         PK(xfer(out.rowptr, rp.data(), rp.size() * sizeof(long long), cudaMemcpyHostToDevice));
         PK(xfer(out.col, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice));
         PK(xfer(out.val, val.data(), val.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -271,7 +298,9 @@ Session *get_session(const svm_model *m)
     for (int j = 0; j < k - 1; j++)
         for (int i = 0; i < m->l; i++) coef[(size_t)j * m->l + i] = m->sv_coef[j][i];
     std::vector<int> start(std::max(k, 1), 0), nsv(std::max(k, 1), 0);
-    for (int i = 0; i < k; i++) nsv[i] = m->nSV ? m->nSV[i] : 0;
+    // one-class and SVR models have no classes: all SVs form one group and
+    // the value is the single "pair" sum over it (svm.cpp:2571-2587)
+    for (int i = 0; i < k; i++) nsv[i] = m->nSV ? m->nSV[i] : (i == 0 ? m->l : 0);
     for (int i = 1; i < k; i++) start[i] = start[i - 1] + nsv[i - 1];
     std::vector<double> rho(std::max(npair, 1), 0.0);
     for (int p = 0; p < npair; p++) rho[p] = m->rho[p];
@@ -362,14 +391,16 @@ void predict_forget(const svm_model *model)
 
 int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double *labels, double *dec_out)
 {
-    if (m->param.svm_type != C_SVC && m->param.svm_type != NU_SVC) {
-        set_error("prediction supports C_SVC and NU_SVC models");
+    const int type = m->param.svm_type;
+    if (type < C_SVC || type > NU_SVR) {
+        set_error("unknown svm_type in the model");
         return -1;
     }
     if (m->param.kernel_type == PRECOMPUTED) {
         set_error("precomputed kernels are not supported on the GPU");
         return -1;
     }
+    const bool classify = type == C_SVC || type == NU_SVC;
     std::lock_guard<std::mutex> g(g_mu);
     Session *s = get_session(m);
     if (!s) return -1;
@@ -381,12 +412,12 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
         // chunk test rows so that the kvalue block stays below ~1 GB
         const long long per_row = (long long)m->l * 8;
         const int chunk = (int)std::max<long long>(1, std::min<long long>(n, (1LL << 30) / per_row));
-        double *kv = nullptr, *d_dec = nullptr;
-        PK(cudaMalloc(&kv, (size_t)chunk * per_row));
-        PK(cudaMalloc(&d_dec, (size_t)chunk * npair * 8));
+        PK(grow(g_ws.kv, g_ws.cap_kv, (size_t)chunk * per_row));
+        PK(grow(g_ws.dec, g_ws.cap_dec, (size_t)chunk * npair * 8));
+        double *kv = g_ws.kv, *d_dec = g_ws.dec;
+        Rows &T = g_ws.T;
         for (int t0 = 0; t0 < n; t0 += chunk) {
             const int tn = std::min(chunk, n - t0);
-            Rows T;
             // test rows: features beyond the SVs' width cannot meet an SV feature in a
             // dot product but still count in the RBF distance, so widen to cover them
             int maxi = s->d - 1;
@@ -394,55 +425,49 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
                 for (const svm_node *p = rows[t0 + r]; p->index != -1; ++p) maxi = std::max(maxi, p->index);
             const bool wider = maxi + 1 > s->d;
             if (is_tc_form(g_predict_form)) {
-                if (kvalue_tensor(m, rows + t0, tn, g_predict_form, kv) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
+                if (kvalue_tensor(m, rows + t0, tn, g_predict_form, kv) != 0) return -1;
             } else if (s->sv.dense && !wider) {
-                if (upload_nodes(rows + t0, tn, s->d, s->base, true, T) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
-                dim3 grid((m->l + 255) / 256, (tn + kTT - 1) / kTT);
                 const size_t smem = (size_t)kTT * s->sv.ld * sizeof(float);
                 if (smem > 200 * 1024) {
-                    T.release();
                     set_error("feature dimension too large for the dense prediction path");
-                    cudaFree(kv); cudaFree(d_dec);
                     return -1;
                 }
+                if (upload_nodes(rows + t0, tn, s->d, s->base, true, T) != 0) return -1;
+                dim3 grid((m->l + 255) / 256, (tn + kTT - 1) / kTT);
                 cudaFuncSetAttribute(kvalue_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 kvalue_dense<<<grid, 256, smem>>>(kp, T.X, tn, s->sv.X, m->l, s->sv.ld, kv);
                 count_launch();
             } else {
-                Rows Sc = s->sv;
-                Rows svcsr;
-                if (s->sv.dense) {
-                    // a CSR copy of the SVs for the merge path
-                    if (upload_nodes(m->SV, m->l, s->d, s->base, false, svcsr) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
-                    Sc = svcsr;
-                }
-                if (upload_nodes(rows + t0, tn, maxi + 1, s->base, false, T) != 0) { cudaFree(kv); cudaFree(d_dec); return -1; }
+                if (s->sv.dense && !s->sv_csr.rowptr &&
+                    upload_nodes(m->SV, m->l, s->d, s->base, false, s->sv_csr) != 0)
+                    return -1;
+                const Rows &Sc = s->sv.dense ? s->sv_csr : s->sv;
+                if (upload_nodes(rows + t0, tn, maxi + 1, s->base, false, T) != 0) return -1;
                 kvalue_csr<<<std::min<long long>(((long long)tn * m->l + 255) / 256, 148 * 16), 256>>>(kp, T, Sc, kv);
                 count_launch();
-                if (s->sv.dense) {
-                    cudaDeviceSynchronize();
-                    svcsr.release();
-                }
             }
             pair_sums<<<std::min<long long>(((long long)tn * npair + 127) / 128, 148 * 8), 128>>>(kv, tn, m->l, k, s->start, s->nsv, s->coef, s->rho, d_dec);
             count_launch();
             cudaError_t e = cudaDeviceSynchronize();
-            T.release();
             if (e != cudaSuccess) {
                 set_error(std::string("prediction kernels failed: ") + cudaGetErrorString(e));
-                cudaFree(kv); cudaFree(d_dec);
                 return -1;
             }
             PK(xfer(dec.data() + (size_t)t0 * npair, d_dec, (size_t)tn * npair * 8, cudaMemcpyDeviceToHost));
         }
-        cudaFree(kv);
-        cudaFree(d_dec);
     } else if (npair > 0) {
         for (int t = 0; t < n; t++)
             for (int p = 0; p < npair; p++) dec[(size_t)t * npair + p] = -m->rho[p];
     }
-    // votes, ties to the lowest class index (svm.cpp:2627-2637)
     for (int t = 0; t < n; t++) {
+        if (!classify) {
+            // one-class: the side of the boundary; SVR: the value (svm.cpp:2585-2587)
+            const double v = dec[t];
+            labels[t] = type == ONE_CLASS ? (v > 0 ? 1 : -1) : v;
+            if (dec_out) dec_out[t] = v;
+            continue;
+        }
+        // votes, ties to the lowest class index (svm.cpp:2627-2637)
         std::vector<int> vote(std::max(k, 1), 0);
         int p = 0;
         for (int i = 0; i < k; i++)

@@ -57,6 +57,7 @@ struct Job {
     std::vector<int> col;
     std::vector<float> val;
     svmb_params params{};
+    std::vector<double> y;      // targets of the points
     SolveParams prm;
     SubProblem sub;
     std::unique_ptr<DeviceRows> rows;
@@ -161,7 +162,7 @@ void Server::collect(Slot &slot)
         const int rc = wave_fetch(slot.w, k, r, copy_stream);
         if (rc == 0) {
             j->alpha.assign(j->n, 0.0);
-            capi::finish_instance(j->sub, r, j->alpha.data(), &j->stats);
+            capi::finish_instance(j->params, j->sub, r, j->y.data(), j->n, j->alpha.data(), &j->stats);
         }
         const std::string err = rc ? std::string(last_error()) : std::string();
         slot.delivered[k] = 1;
@@ -190,7 +191,7 @@ void Server::reap(Slot &slot)
         j->rows->release_async(slot.stream);
         if (rc == 0) {
             j->alpha.assign(j->n, 0.0);
-            capi::finish_instance(j->sub, res[k], j->alpha.data(), &j->stats);
+            capi::finish_instance(j->params, j->sub, res[k], j->y.data(), j->n, j->alpha.data(), &j->stats);
         }
     }
     std::lock_guard<std::mutex> g(mu);
@@ -450,6 +451,7 @@ long long svmb_server_submit(svmb_server *h, int n, int d, const long long *rowp
     j->col.assign(col, col + rowptr[n]);
     j->val.assign(val, val + rowptr[n]);
     j->params = *params;
+    j->y.assign(y, y + n);
     j->prm = svmb::capi::to_solve_params(*params);
     if (j->prm.blocks_override <= 0)
         j->prm.blocks_override = std::max(1, std::min(svmb::device_sm_count(), n / h->s.cfg.rows_per_block));

@@ -26,6 +26,7 @@
 
 #include "engine.hpp"
 #include "predict.hpp"
+#include "training.hpp"
 #include "svm.h"
 #include "svm_b200.h"
 
@@ -56,18 +57,6 @@ void info(const char *fmt, ...)
     (*svm_print_string)(buf);
 }
 
-// the text of one info() call kept as one entry of `out` (printed later, in
-// order, one print-hook call per entry as the reference makes them)
-void info_to(std::vector<std::string> &out, const char *fmt, ...)
-{
-    char buf[1024];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    out.emplace_back(buf);
-}
-
 // engine options settable through svmb_set_option (process wide)
 struct Options {
     int form = svmb::FORM_EXACT;
@@ -79,78 +68,6 @@ struct Options {
 // statistics of the last svm_train call (svmb_last_train_stats)
 std::vector<svmb_solve_stats> g_last_stats;
 std::mutex g_stats_mu;
-
-// Labels in first-occurrence order; -1/+1 with -1 first are swapped so that
-// +1 is class 0 (reference svm.cpp:2081-2154).
-void group_classes(const svm_problem *prob, int *nr_class_ret, std::vector<int> &label, std::vector<int> &start,
-                   std::vector<int> &count, std::vector<int> &perm)
-{
-    const int l = prob->l;
-    label.clear();
-    count.clear();
-    std::vector<int> data_label(l);
-    for (int i = 0; i < l; i++) {
-        const int this_label = (int)prob->y[i];
-        int j;
-        for (j = 0; j < (int)label.size(); j++)
-            if (this_label == label[j]) {
-                ++count[j];
-                break;
-            }
-        data_label[i] = j;
-        if (j == (int)label.size()) {
-            label.push_back(this_label);
-            count.push_back(1);
-        }
-    }
-    const int nr_class = (int)label.size();
-    if (nr_class == 2 && label[0] == -1 && label[1] == 1) {
-        std::swap(label[0], label[1]);
-        std::swap(count[0], count[1]);
-        for (int i = 0; i < l; i++) data_label[i] = data_label[i] == 0 ? 1 : 0;
-    }
-    start.assign(nr_class, 0);
-    for (int i = 1; i < nr_class; i++) start[i] = start[i - 1] + count[i - 1];
-    perm.assign(l, 0);
-    std::vector<int> fill = start;
-    for (int i = 0; i < l; i++) perm[fill[data_label[i]]++] = i;
-    *nr_class_ret = nr_class;
-}
-
-// One binary subproblem in the form the formulations build it
-// (solve_c_svc svm.cpp:1500-1533, solve_nu_svc :1535-1588).
-svmb::SubProblem make_sub(const std::vector<int> &rows, const std::vector<signed char> &y, const svm_parameter *param,
-                          double Cp, double Cn)
-{
-    svmb::SubProblem sp;
-    const int l = (int)rows.size();
-    sp.rows = rows;
-    sp.y = y;
-    sp.alpha0.assign(l, 0.0);
-    sp.p.assign(l, 0.0);
-    if (param->svm_type == NU_SVC) {
-        const double nu = param->nu;
-        double sum_pos = nu * l / 2, sum_neg = nu * l / 2;
-        for (int i = 0; i < l; i++) {
-            if (y[i] == +1) {
-                sp.alpha0[i] = std::min(1.0, sum_pos);
-                sum_pos -= sp.alpha0[i];
-            } else {
-                sp.alpha0[i] = std::min(1.0, sum_neg);
-                sum_neg -= sp.alpha0[i];
-            }
-        }
-        sp.nu = 1;
-        sp.Cp = 1.0;
-        sp.Cn = 1.0;
-    } else {
-        for (int i = 0; i < l; i++) sp.p[i] = -1;
-        sp.nu = 0;
-        sp.Cp = Cp;
-        sp.Cn = Cn;
-    }
-    return sp;
-}
 
 svmb::SolveParams make_solve_params(const svm_parameter *param)
 {
@@ -168,243 +85,36 @@ svmb::SolveParams make_solve_params(const svm_parameter *param)
     return prm;
 }
 
-struct DecisionFunction {
-    std::vector<double> alpha;   // signed coefficients
-    double rho = 0;
-};
-
-// Post-processing of one solve (svm.cpp:1517-1532, :1572-1587 and svm_train_one :1739-1766).
-// One subproblem's decision function and statistics; its messages go to
-// `log` (the caller prints the logs of all pairs in pair order).
-DecisionFunction finish_solve(const svmb::SubProblem &sp, const svmb::SolveResult &R, const svm_parameter *param,
-                              const double *yvals, std::vector<std::string> &log, svmb_solve_stats &st)
-{
-    DecisionFunction f;
-    const int l = (int)sp.rows.size();
-    f.alpha = R.alpha;
-    double rho = R.out.rho, obj = R.out.obj;
-    double upper_p, upper_n;
-    info_to(log, "\noptimization finished, #iter = %lld\n", R.out.iters);
-    // (the max_iter warning goes to stderr from the caller, in pair order)
-    if (sp.nu) {
-        const double r = R.out.r;
-        info_to(log, "C = %f\n", 1 / r);
-        for (int i = 0; i < l; i++) f.alpha[i] *= sp.y[i] / r;
-        rho /= r;
-        obj /= (r * r);
-        upper_p = upper_n = 1 / r;
-    } else {
-        double sum_alpha = 0;
-        for (int i = 0; i < l; i++) sum_alpha += f.alpha[i];
-        if (sp.Cp == sp.Cn) info_to(log, "nu = %f\n", sum_alpha / (sp.Cp * l));
-        for (int i = 0; i < l; i++) f.alpha[i] *= sp.y[i];
-        upper_p = sp.Cp;
-        upper_n = sp.Cn;
-    }
-    f.rho = rho;
-    info_to(log, "obj = %f, rho = %f\n", obj, rho);
-    int nSV = 0, nBSV = 0;
-    for (int i = 0; i < l; i++) {
-        if (fabs(f.alpha[i]) > 0) {
-            ++nSV;
-            if (yvals[i] > 0) {
-                if (fabs(f.alpha[i]) >= upper_p) ++nBSV;
-            } else {
-                if (fabs(f.alpha[i]) >= upper_n) ++nBSV;
-            }
-        }
-    }
-    info_to(log, "nSV = %d, nBSV = %d\n", nSV, nBSV);
-    memset(&st, 0, sizeof st);
-    st.iters = R.out.iters;
-    st.obj = obj;
-    st.rho = rho;
-    st.r = R.out.r;
-    st.l = l;
-    st.nr_sv = nSV;
-    st.nr_bsv = nBSV;
-    st.status = R.out.status;
-    st.active_size = R.out.active_size;
-    st.seconds = R.seconds;
-    st.launch = R.wave;
-    st.sum_active = R.out.sum_active;
-    st.q_evals = R.out.q_evals;
-    st.lookups = R.out.lookups;
-    st.hits = R.out.hits;
-    st.fills = R.out.fills;
-    st.prefetched = R.out.prefetched;
-    st.prefetch_used = R.out.prefetch_used;
-    for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
-    return f;
-}
-
-bool svm_type_supported(int t) { return t == C_SVC || t == NU_SVC; }
 
 bool train_supported(const svm_parameter *param)
 {
-    if (!svm_type_supported(param->svm_type) || param->kernel_type == PRECOMPUTED) {
-        svmb::set_error("only C_SVC and NU_SVC with linear/poly/rbf/sigmoid kernels are trained on the GPU");
+    if (param->kernel_type == PRECOMPUTED) {
+        svmb::set_error("precomputed kernels are not trained on the GPU");
+        info("ERROR: %s\n", svmb::last_error());
+        return false;
+    }
+    if (param->svm_type < C_SVC || param->svm_type > NU_SVR) {
+        svmb::set_error("unknown svm type");
         info("ERROR: %s\n", svmb::last_error());
         return false;
     }
     return true;
 }
 
-// One svm_train call (reference svm.cpp:2159-2404) split into its one-vs-one
-// subproblems -- which address the rows of an uploaded row set by id -- and
-// the model assembly from their solutions, so that the subproblems of many
-// trainings (CV folds, grid points) can share one batched solve.
-struct TrainJob {
-    const svm_problem *prob = nullptr;
-    svm_parameter param{};
-    int l = 0, nr_class = 0;
-    std::vector<int> label, start, count, perm;
-    std::vector<svm_node *> x;                 // rows in grouped order
-    std::vector<svmb::SubProblem> subs;
-    std::vector<std::vector<double>> subys;
-    svmb::SolveParams own;                     // solve parameters of this training
-};
-
-// row_id[i]: id of prob row i in the uploaded row set (nullptr: rows uploaded in grouped order)
-void setup_train(const svm_problem *prob, const svm_parameter *param, const int *row_id, TrainJob &tj)
+void record_stats(const std::vector<svmb_solve_stats> &st)
 {
-    tj.prob = prob;
-    tj.param = *param;
-    tj.l = prob->l;
-    group_classes(prob, &tj.nr_class, tj.label, tj.start, tj.count, tj.perm);
-    const int nr_class = tj.nr_class;
-    if (nr_class == 1) info("WARNING: training data in only one class. See README for details.\n");
-    tj.x.resize(tj.l);
-    for (int i = 0; i < tj.l; i++) tj.x[i] = prob->x[tj.perm[i]];
-    std::vector<double> weighted_C(nr_class, param->C);
-    for (int i = 0; i < param->nr_weight; i++) {
-        int j;
-        for (j = 0; j < nr_class; j++)
-            if (param->weight_label[i] == tj.label[j]) break;
-        if (j == nr_class)
-            fprintf(stderr, "WARNING: class label %d specified in weight is not found\n", param->weight_label[i]);
-        else
-            weighted_C[j] *= param->weight[i];
-    }
-    auto id = [&](int g) { return row_id ? row_id[tj.perm[g]] : g; };   // grouped index -> uploaded row id
-    // the one-vs-one subproblems in pair order (class i rows +1, then class j
-    // rows -1), built in parallel: they are independent
-    std::vector<std::pair<int, int>> pairs;
-    for (int i = 0; i < nr_class; i++)
-        for (int j = i + 1; j < nr_class; j++) pairs.emplace_back(i, j);
-    const size_t first = tj.subs.size();
-    tj.subs.resize(first + pairs.size());
-    tj.subys.resize(first + pairs.size());
-#pragma omp parallel for schedule(dynamic, 1)
-    for (int q = 0; q < (int)pairs.size(); q++) {
-        const int i = pairs[q].first, j = pairs[q].second;
-        const int n = tj.count[i] + tj.count[j];
-        std::vector<int> r(n);
-        std::vector<signed char> y(n);
-        std::vector<double> yv(n);
-        for (int k = 0; k < tj.count[i]; k++) { r[k] = id(tj.start[i] + k); y[k] = +1; yv[k] = +1; }
-        for (int k = 0; k < tj.count[j]; k++) {
-            r[tj.count[i] + k] = id(tj.start[j] + k);
-            y[tj.count[i] + k] = -1;
-            yv[tj.count[i] + k] = -1;
-        }
-        tj.subs[first + q] = make_sub(r, y, param, weighted_C[i], weighted_C[j]);
-        tj.subys[first + q] = std::move(yv);
-    }
-    tj.own = make_solve_params(param);
-}
-
-// model assembly (reference svm.cpp:2297-2386) from the solutions res[first ..]
-svm_model *assemble_model(const TrainJob &tj, const std::vector<svmb::SolveResult> &res, size_t first)
-{
-    const svm_parameter *param = &tj.param;
-    const int l = tj.l, nr_class = tj.nr_class;
-    const std::vector<int> &start = tj.start, &count = tj.count;
-    std::vector<DecisionFunction> f(tj.subs.size());
-    // the pairs' decision functions in parallel; their messages, warnings and
-    // statistics then in pair order
-    std::vector<std::vector<std::string>> logs(tj.subs.size());
-    std::vector<svmb_solve_stats> sts(tj.subs.size());
-#pragma omp parallel for schedule(dynamic, 1)
-    for (int p = 0; p < (int)tj.subs.size(); p++)
-        f[p] = finish_solve(tj.subs[p], res[first + p], param, tj.subys[p].data(), logs[p], sts[p]);
-    for (size_t p = 0; p < tj.subs.size(); p++) {
-        // the solver's max_iter warning precedes its "optimization finished" line (svm.cpp:779-787)
-        if (res[first + p].out.status == 1) fprintf(stderr, "\nWARNING: reaching max number of iterations\n");
-        for (const std::string &line : logs[p]) (*svm_print_string)(line.c_str());
-        std::lock_guard<std::mutex> g(g_stats_mu);
-        g_last_stats.push_back(sts[p]);
-    }
-    svm_model *model = (svm_model *)malloc(sizeof(svm_model));
-    model->param = *param;
-    model->free_sv = 0;
-    model->nr_class = nr_class;
-    model->label = (int *)malloc(sizeof(int) * std::max(nr_class, 1));
-    for (int i = 0; i < nr_class; i++) model->label[i] = tj.label[i];
-    const int npair = nr_class * (nr_class - 1) / 2;
-    model->rho = (double *)malloc(sizeof(double) * std::max(npair, 1));
-    for (int i = 0; i < npair; i++) model->rho[i] = f[i].rho;
-    model->probA = NULL;
-    model->probB = NULL;
-    std::vector<char> nonzero(l, 0);
-    {
-        int p = 0;
-        for (int i = 0; i < nr_class; i++)
-            for (int j = i + 1; j < nr_class; j++) {
-                for (int k = 0; k < count[i]; k++)
-                    if (fabs(f[p].alpha[k]) > 0) nonzero[start[i] + k] = 1;
-                for (int k = 0; k < count[j]; k++)
-                    if (fabs(f[p].alpha[count[i] + k]) > 0) nonzero[start[j] + k] = 1;
-                ++p;
-            }
-    }
-    int total_sv = 0;
-    std::vector<int> nz_count(nr_class);
-    model->nSV = (int *)malloc(sizeof(int) * std::max(nr_class, 1));
-    for (int i = 0; i < nr_class; i++) {
-        int nSV = 0;
-        for (int j = 0; j < count[i]; j++)
-            if (nonzero[start[i] + j]) { ++nSV; ++total_sv; }
-        model->nSV[i] = nSV;
-        nz_count[i] = nSV;
-    }
-    info("Total nSV = %d\n", total_sv);
-    model->l = total_sv;
-    model->SV = (svm_node **)malloc(sizeof(svm_node *) * std::max(total_sv, 1));
-    model->sv_indices = (int *)malloc(sizeof(int) * std::max(total_sv, 1));
-    {
-        int p = 0;
-        for (int i = 0; i < l; i++)
-            if (nonzero[i]) {
-                model->SV[p] = tj.x[i];
-                model->sv_indices[p++] = tj.perm[i] + 1;
-            }
-    }
-    std::vector<int> nz_start(nr_class, 0);
-    for (int i = 1; i < nr_class; i++) nz_start[i] = nz_start[i - 1] + nz_count[i - 1];
-    model->sv_coef = (double **)malloc(sizeof(double *) * std::max(nr_class - 1, 1));
-    for (int i = 0; i < nr_class - 1; i++) model->sv_coef[i] = (double *)malloc(sizeof(double) * std::max(total_sv, 1));
-    {
-        int p = 0;
-        for (int i = 0; i < nr_class; i++)
-            for (int j = i + 1; j < nr_class; j++) {
-                int q = nz_start[i];
-                for (int k = 0; k < count[i]; k++)
-                    if (nonzero[start[i] + k]) model->sv_coef[j - 1][q++] = f[p].alpha[k];
-                q = nz_start[j];
-                for (int k = 0; k < count[j]; k++)
-                    if (nonzero[start[j] + k]) model->sv_coef[i][q++] = f[p].alpha[count[i] + k];
-                ++p;
-            }
-    }
-    return model;
+    std::lock_guard<std::mutex> g(g_stats_mu);
+    g_last_stats.insert(g_last_stats.end(), st.begin(), st.end());
 }
 
 // Stratified k-fold cross-validation (reference svm.cpp:2407-2525) over a grid
 // of (C, gamma) points: one fold assignment with the C library rand(), as the
-// reference draws it, then every point's and fold's one-vs-one subproblems are
-// solved in batched launches over the rows uploaded once.  target[p*l + i] is
-// the prediction of row i by the model of point p trained without i's fold.
+// reference draws it, then every point's and fold's training (with its
+// probability cross-validations, if asked for) is planned, all their binary
+// subproblems are solved in batched launches over the rows uploaded once, and
+// the models are assembled and evaluated point by point, fold by fold.
+// target[p*l + i] is the prediction of row i by the model of point p trained
+// without i's fold.
 int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, int nr_fold, int npoints,
                           const double *Cs, const double *gammas, double *target)
 {
@@ -413,45 +123,8 @@ int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, i
         g_last_stats.clear();
     }
     const int l = prob->l;
-    std::vector<int> perm(l);
-    if (nr_fold > l) {
-        nr_fold = l;
-        fprintf(stderr, "WARNING: # folds > # data. Will use # folds = # data instead (i.e., leave-one-out cross validation)\n");
-    }
-    std::vector<int> fold_start(nr_fold + 1);
-    if ((param->svm_type == C_SVC || param->svm_type == NU_SVC) && nr_fold < l) {
-        int nr_class;
-        std::vector<int> label, start, count;
-        group_classes(prob, &nr_class, label, start, count, perm);
-        std::vector<int> fold_count(nr_fold), index(perm);
-        // stratified shuffle with the C library rand(), as the reference (svm.cpp:2436-2442)
-        for (int c = 0; c < nr_class; c++)
-            for (int i = 0; i < count[c]; i++) {
-                const int j = i + rand() % (count[c] - i);
-                std::swap(index[start[c] + j], index[start[c] + i]);
-            }
-        for (int i = 0; i < nr_fold; i++) {
-            fold_count[i] = 0;
-            for (int c = 0; c < nr_class; c++) fold_count[i] += (i + 1) * count[c] / nr_fold - i * count[c] / nr_fold;
-        }
-        fold_start[0] = 0;
-        for (int i = 1; i <= nr_fold; i++) fold_start[i] = fold_start[i - 1] + fold_count[i - 1];
-        for (int c = 0; c < nr_class; c++)
-            for (int i = 0; i < nr_fold; i++) {
-                const int begin = start[c] + i * count[c] / nr_fold;
-                const int end = start[c] + (i + 1) * count[c] / nr_fold;
-                for (int j = begin; j < end; j++) perm[fold_start[i]++] = index[j];
-            }
-        fold_start[0] = 0;
-        for (int i = 1; i <= nr_fold; i++) fold_start[i] = fold_start[i - 1] + fold_count[i - 1];
-    } else {
-        for (int i = 0; i < l; i++) perm[i] = i;
-        for (int i = 0; i < l; i++) {
-            const int j = i + rand() % (l - i);
-            std::swap(perm[i], perm[j]);
-        }
-        for (int i = 0; i <= nr_fold; i++) fold_start[i] = i * l / nr_fold;
-    }
+    std::vector<int> perm, fold_start;
+    svmb::cv_folds(prob, param, nr_fold, perm, fold_start);
     for (long long k = 0; k < (long long)npoints * l; k++) target[k] = NAN;
     if (!train_supported(param)) return -1;
     const bool trace = getenv("SVMB_TRACE") && *getenv("SVMB_TRACE") == '1';
@@ -465,15 +138,14 @@ int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, i
         info("ERROR: %s\n", svmb::last_error());
         return -1;
     }
-    // the training set of every fold, its row ids, and one training per (point, fold)
+    // the training set of every fold and one training per (point, fold)
     std::vector<svm_problem> fold_prob(nr_fold);
     std::vector<std::vector<svm_node *>> fold_x(nr_fold);
     std::vector<std::vector<double>> fold_y(nr_fold);
     std::vector<std::vector<int>> fold_id(nr_fold);
     for (int i = 0; i < nr_fold; i++) {
-        const int begin = fold_start[i], end = fold_start[i + 1];
         for (int j = 0; j < l; j++) {
-            if (j >= begin && j < end) continue;
+            if (j >= fold_start[i] && j < fold_start[i + 1]) continue;
             fold_x[i].push_back(prob->x[perm[j]]);
             fold_y[i].push_back(prob->y[perm[j]]);
             fold_id[i].push_back(perm[j]);
@@ -483,46 +155,46 @@ int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, i
         fold_prob[i].y = fold_y[i].data();
     }
     std::vector<svm_parameter> pparam(npoints, *param);
-    std::vector<TrainJob> jobs((size_t)npoints * nr_fold);
+    std::vector<svmb::Training> jobs((size_t)npoints * nr_fold);
     std::vector<svmb::SubProblem> all;
-    std::vector<size_t> first(jobs.size());
     for (int q = 0; q < npoints; q++) {
         pparam[q].C = Cs[q];
         pparam[q].gamma = gammas[q];
-        for (int i = 0; i < nr_fold; i++) {
-            TrainJob &tj = jobs[(size_t)q * nr_fold + i];
-            setup_train(&fold_prob[i], &pparam[q], fold_id[i].data(), tj);
-        }
+        for (int i = 0; i < nr_fold; i++)
+            svmb::plan_training(&fold_prob[i], &pparam[q], fold_id[i].data(), make_solve_params(&pparam[q]),
+                                jobs[(size_t)q * nr_fold + i]);
     }
-    for (size_t k = 0; k < jobs.size(); k++) {
-        first[k] = all.size();
-        for (svmb::SubProblem &sp : jobs[k].subs) {
-            sp.own = &jobs[k].own;
-            all.push_back(sp);
-        }
-    }
+    for (svmb::Training &t : jobs) svmb::collect(t, all);
     std::vector<svmb::SolveResult> res;
-    {
-        std::lock_guard<std::mutex> g(g_stats_mu);
-        g_last_stats.clear();
-    }
     const double t_setup = since(c0);
     const auto c1 = std::chrono::steady_clock::now();
-    if (!all.empty() && svmb::solve_batch(rows, all, jobs[0].own, res, 0) != 0) {
+    if (!all.empty() && svmb::solve_batch(rows, all, jobs[0].solve, res, 0) != 0) {
         info("ERROR: %s\n", svmb::last_error());
         return -1;
     }
     const double t_solve = since(c1);
     const auto c2 = std::chrono::steady_clock::now();
+    const bool with_prob = param->probability && (param->svm_type == C_SVC || param->svm_type == NU_SVC);
     for (int q = 0; q < npoints; q++)
         for (int i = 0; i < nr_fold; i++) {
-            const size_t k = (size_t)q * nr_fold + i;
-            svm_model *m = assemble_model(jobs[k], res, first[k]);
+            std::vector<svmb_solve_stats> st;
+            svm_model *m = svmb::assemble(jobs[(size_t)q * nr_fold + i], res, st);
+            record_stats(st);
+            if (!m) continue;
             const int begin = fold_start[i], end = fold_start[i + 1];
             std::vector<const svm_node *> held;
             for (int j = begin; j < end; j++) held.push_back(prob->x[perm[j]]);
-            std::vector<double> lab(held.size());
-            if (held.empty() || svmb::predict_batch(m, held.data(), (int)held.size(), lab.data(), nullptr) == 0)
+            std::vector<double> lab(std::max<size_t>(held.size(), 1));
+            int rc = 0;
+            if (held.empty()) rc = 0;
+            else if (with_prob) {
+                // svm_predict_probability's label (svm.cpp:2500-2506)
+                std::vector<double> pe(held.size() * (size_t)std::max(m->nr_class, 1));
+                rc = svmb::predict_probability_batch(m, held.data(), (int)held.size(), lab.data(), pe.data());
+            } else {
+                rc = svmb::predict_batch(m, held.data(), (int)held.size(), lab.data(), nullptr);
+            }
+            if (rc == 0)
                 for (int j = begin; j < end; j++) target[(size_t)q * l + perm[j]] = lab[j - begin];
             svm_free_and_destroy_model(&m);
         }
@@ -531,7 +203,6 @@ int cross_validation_grid(const svm_problem *prob, const svm_parameter *param, i
                 nr_fold, all.size(), t_setup, t_solve, since(c2));
     return 0;
 }
-
 
 }  // namespace
 
@@ -582,23 +253,30 @@ struct svm_model *svm_train(const struct svm_problem *prob, const struct svm_par
     }
     if (!train_supported(param)) return NULL;
     const auto t0 = std::chrono::steady_clock::now();
-    TrainJob tj;
-    setup_train(prob, param, nullptr, tj);
+    svmb::Training t;
+    svmb::plan_training(prob, param, nullptr, make_solve_params(param), t);
+    std::vector<svmb::SubProblem> all;
+    svmb::collect(t, all);
     const auto t1 = std::chrono::steady_clock::now();
-    // rows are uploaded once, in grouped order; every pair addresses them by id
+    // rows are uploaded once, in the plan's order (grouped by class for the
+    // classifiers); every subproblem addresses them by id
     svmb::DeviceRows rows;
-    if (tj.l > 0 && svmb::upload_rows(tj.x.data(), tj.l, rows, svmb::api_force_layout(), 0, svmb::kAllocPooled) != 0) {
+    if (prob->l > 0 &&
+        svmb::upload_rows(t.x.data(), prob->l, rows, svmb::api_force_layout(), 0, svmb::kAllocPooled) != 0) {
         info("ERROR: %s\n", svmb::last_error());
         return NULL;
     }
     const auto t2 = std::chrono::steady_clock::now();
     std::vector<svmb::SolveResult> res;
-    if (!tj.subs.empty() && svmb::solve_batch(rows, tj.subs, make_solve_params(param), res, 0) != 0) {
+    if (!all.empty() && svmb::solve_batch(rows, all, t.solve, res, 0) != 0) {
         info("ERROR: %s\n", svmb::last_error());
         return NULL;
     }
     const auto t3 = std::chrono::steady_clock::now();
-    svm_model *model = assemble_model(tj, res, 0);
+    std::vector<svmb_solve_stats> st;
+    svm_model *model = svmb::assemble(t, res, st);
+    record_stats(st);
+    if (!model) info("ERROR: %s\n", svmb::last_error());
     if (getenv("SVMB_TRACE") && *getenv("SVMB_TRACE") == '1') {
         const auto t4 = std::chrono::steady_clock::now();
         auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
@@ -668,13 +346,36 @@ double svm_predict(const svm_model *model, const svm_node *x)
     return svm_predict_values(model, x, dec.data());
 }
 
-// Probability outputs need probA/probB, which this engine does not train
-// (svm_parameter.probability is accepted and ignored); as in the reference
-// (svm.cpp:2660-2697) such a model falls back to svm_predict.
+// Class probabilities by pairwise coupling of the pairs' sigmoid estimates
+// (reference svm.cpp:2660-2697); models without probA/probB fall back to
+// svm_predict, as there.
 double svm_predict_probability(const svm_model *model, const svm_node *x, double *prob_estimates)
 {
-    (void)prob_estimates;
+    if ((model->param.svm_type == C_SVC || model->param.svm_type == NU_SVC) && model->probA != NULL &&
+        model->probB != NULL) {
+        double lab = 0;
+        if (svmb::predict_probability_batch(model, &x, 1, &lab, prob_estimates) != 0) {
+            info("ERROR: %s\n", svmb::last_error());
+            return NAN;
+        }
+        return lab;
+    }
     return svm_predict(model, x);
+}
+
+int svmb_predict_probability_batch(const struct svm_model *model, const struct svm_node *const *rows, int n,
+                                   double *labels, double *prob_estimates)
+{
+    if (!model || (n > 0 && (!rows || !labels || !prob_estimates)) || n < 0) {
+        svmb::set_error("invalid arguments");
+        return -1;
+    }
+    if (!svm_check_probability_model(model) || model->param.svm_type == EPSILON_SVR ||
+        model->param.svm_type == NU_SVR) {
+        svmb::set_error("the model has no class probability information (train with probability = 1)");
+        return -1;
+    }
+    return svmb::predict_probability_batch(model, rows, n, labels, prob_estimates);
 }
 
 static const char *svm_type_table[] = {"c_svc", "nu_svc", "one_class", "epsilon_svr", "nu_svr", NULL};

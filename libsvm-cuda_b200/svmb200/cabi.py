@@ -127,6 +127,10 @@ def model_arrays(m: svm_model) -> dict:
         "labels": np.array([m.label[i] for i in range(k)], dtype=np.int64) if m.label else None,
         "nsv": np.array([m.nSV[i] for i in range(k)], dtype=np.int64) if m.nSV else None,
         "sv_indices": np.array([m.sv_indices[i] for i in range(m.l)], dtype=np.int64) if m.sv_indices else None,
+        "probA": np.array([m.probA[i] for i in range(max(npair, 1) if m.probA else 0)], dtype=np.float64)
+        if m.probA else None,
+        "probB": np.array([m.probB[i] for i in range(max(npair, 1) if m.probB else 0)], dtype=np.float64)
+        if m.probB else None,
     }
     coef = np.zeros((max(k - 1, 0), m.l), dtype=np.float64)
     for j in range(k - 1):

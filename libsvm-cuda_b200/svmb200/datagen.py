@@ -88,6 +88,42 @@ def _flip(rng, y, frac):
     return y
 
 
+def from_dense64(X: np.ndarray, y: np.ndarray) -> CSR:
+    """Dense float64 matrix -> CSR keeping the full double values (rows a
+    caller passes through svm.h need not be float32 numbers)."""
+    X = np.asarray(X, dtype=np.float64)
+    n, d = X.shape
+    mask = X != 0
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(mask.sum(axis=1), out=indptr[1:])
+    r, c = np.nonzero(mask)
+    return CSR(indptr, (c + 1).astype(np.int32), X[r, c].copy(), np.asarray(y, dtype=np.float64), d)
+
+
+def dense_gauss_f64(n: int, n_test: int, d: int, seed: int, flip: float = 0.05):
+    """dense_gauss with full-precision double features (not float32 numbers)."""
+    rng = np.random.default_rng(seed)
+    tot = n + n_test
+    y = np.where(np.arange(tot) % 2 == 0, 1.0, -1.0)
+    rng.shuffle(y)
+    X = rng.standard_normal((tot, d)) + 0.5 * y[:, None]
+    y = _flip(rng, y, flip)
+    return from_dense64(X[:n], y[:n]), from_dense64(X[n:], y[n:])
+
+
+def regression(n: int, n_test: int, d: int, seed: int, noise: float = 0.1):
+    """Regression targets y = sin(x.w) + 0.5 (x.v)^2 / d + noise over Gaussian
+    float32 features (epsilon-SVR / nu-SVR workloads)."""
+    rng = np.random.default_rng(seed)
+    tot = n + n_test
+    X = rng.standard_normal((tot, d)).astype(np.float32)
+    w = rng.standard_normal(d) / math.sqrt(d)
+    v = rng.standard_normal(d)
+    Xd = X.astype(np.float64)
+    y = np.sin(Xd @ w) + 0.5 * (Xd @ v) ** 2 / d + noise * rng.standard_normal(tot)
+    return from_dense(X[:n], y[:n]), from_dense(X[n:], y[n:])
+
+
 def dense_gauss(n: int = 4000, n_test: int = 1000, d: int = 64, seed: int = 1, flip: float = 0.05):
     """Two Gaussian classes with per-dimension means +0.5 / -0.5, std 1, balanced labels."""
     rng = np.random.default_rng(seed)

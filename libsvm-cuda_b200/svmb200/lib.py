@@ -40,7 +40,7 @@ class SvmbParams(C.Structure):
     _fields_ = [("svm_type", C.c_int), ("kernel_type", C.c_int), ("degree", C.c_int), ("shrinking", C.c_int),
                 ("gamma", C.c_double), ("coef0", C.c_double), ("C_pos", C.c_double), ("C_neg", C.c_double),
                 ("nu", C.c_double), ("eps", C.c_double), ("cache_mb", C.c_double), ("form", C.c_int),
-                ("blocks", C.c_int), ("prefetch", C.c_int), ("gbar_mode", C.c_int)]
+                ("blocks", C.c_int), ("prefetch", C.c_int), ("gbar_mode", C.c_int), ("p", C.c_double)]
 
 
 class ServerConfig(C.Structure):
@@ -59,13 +59,14 @@ class ServerStats(C.Structure):
 
 def make_params(svm_type=0, kernel_type=2, degree=3, gamma=0.0, coef0=0.0, C_pos=1.0, C_neg=None, nu=0.5,
                 eps=1e-3, cache_mb=100.0, shrinking=1, form=FORM_EXACT, blocks=0, prefetch=0,
-                gbar_mode=0) -> SvmbParams:
+                gbar_mode=0, eps_tube=0.1) -> SvmbParams:
     p = SvmbParams()
     p.svm_type, p.kernel_type, p.degree, p.shrinking = svm_type, kernel_type, degree, shrinking
     p.gamma, p.coef0, p.C_pos = gamma, coef0, C_pos
     p.C_neg = C_pos if C_neg is None else C_neg
     p.nu, p.eps, p.cache_mb, p.form, p.blocks, p.prefetch = nu, eps, cache_mb, form, blocks, prefetch
     p.gbar_mode = gbar_mode
+    p.p = eps_tube
     return p
 
 
@@ -95,6 +96,10 @@ def _load(path: str) -> C.CDLL:
     lib.svmb_set_option.argtypes = [C.c_char_p, C.c_longlong]
     lib.svmb_last_train_stats.argtypes = [_P(SolveStats), C.c_int]
     lib.svmb_predict_batch.argtypes = [_P(svm_model), C.c_void_p, C.c_int, _P(C.c_double), _P(C.c_double)]
+    lib.svmb_predict_probability_batch.argtypes = [_P(svm_model), C.c_void_p, C.c_int, _P(C.c_double),
+                                                   _P(C.c_double)]
+    lib.svm_predict_probability.restype = C.c_double
+    lib.svm_predict_probability.argtypes = [_P(svm_model), _P(cabi.svm_node), _P(C.c_double)]
     lib.svmb_solve_binary_csr.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           _P(SvmbParams), C.c_void_p, _P(SolveStats)]
     lib.svmb_solve_many_csr.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
@@ -234,6 +239,25 @@ class Engine:
                                          lab.ctypes.data_as(_P(C.c_double)), dec.ctypes.data_as(_P(C.c_double)))
         self._ok(rc, "svmb_predict_batch")
         return lab[:p.n], dec[:p.n, :k * (k - 1) // 2]
+
+    def predict_probability(self, model: Model, p: CSR) -> Tuple[np.ndarray, np.ndarray]:
+        """svmb_predict_probability_batch: labels and [n][nr_class] probabilities."""
+        rows = NodeRows(p)
+        k = model.contents.nr_class
+        lab = np.zeros(max(p.n, 1))
+        prob = np.zeros((max(p.n, 1), max(k, 1)))
+        rc = self.lib.svmb_predict_probability_batch(model.ptr, C.c_void_p(int(rows.addrs.ctypes.data)) if p.n else None,
+                                                     p.n, lab.ctypes.data_as(_P(C.c_double)),
+                                                     prob.ctypes.data_as(_P(C.c_double)))
+        self._ok(rc, "svmb_predict_probability_batch")
+        return lab[:p.n], prob[:p.n, :k]
+
+    def predict_probability_one(self, model: Model, p: CSR, i: int) -> Tuple[float, np.ndarray]:
+        rows = NodeRows(p)
+        k = model.contents.nr_class
+        prob = np.zeros(max(k, 1))
+        lab = self.lib.svm_predict_probability(model.ptr, rows.row(i), prob.ctypes.data_as(_P(C.c_double)))
+        return lab, prob[:k]
 
     def predict_one(self, model: Model, p: CSR, i: int) -> Tuple[float, np.ndarray]:
         rows = NodeRows(p)

@@ -164,6 +164,16 @@ static void dump_model(FILE *out, const struct svm_model *m)
     fprintf(out, "rho");
     for (int i = 0; i < npair; i++) fprintf(out, " %.17g", m->rho[i]);
     fprintf(out, "\n");
+    if (m->probA) {
+        fprintf(out, "probA");
+        for (int i = 0; i < npair; i++) fprintf(out, " %.17g", m->probA[i]);
+        fprintf(out, "\n");
+    }
+    if (m->probB) {
+        fprintf(out, "probB");
+        for (int i = 0; i < npair; i++) fprintf(out, " %.17g", m->probB[i]);
+        fprintf(out, "\n");
+    }
     fprintf(out, "sv_indices");
     for (int i = 0; i < m->l; i++) fprintf(out, " %d", m->sv_indices[i]);
     fprintf(out, "\n");

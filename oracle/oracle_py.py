@@ -109,7 +109,7 @@ def reference_lib():
 
 def parse_dump(text: str) -> dict:
     """Parse ref_dump / oracle_dump output into arrays."""
-    out = {"iter": [], "obj": [], "dec": [], "cv": [], "sv_coef": []}
+    out = {"iter": [], "obj": [], "dec": [], "cv": [], "sv_coef": [], "prob": []}
     for line in text.splitlines():
         parts = line.split()
         if not parts:
@@ -119,8 +119,10 @@ def parse_dump(text: str) -> dict:
             out[key] = int(parts[1])
         elif key in ("labels", "nsv", "sv_indices"):
             out[key] = np.array([int(v) for v in parts[1:]], dtype=np.int64)
-        elif key == "rho":
-            out["rho"] = np.array([float(v) for v in parts[1:]])
+        elif key in ("rho", "probA", "probB"):
+            out[key] = np.array([float(v) for v in parts[1:]])
+        elif key == "prob":
+            out["prob"].append([float(v) for v in parts[2:]])
         elif key == "sv_coef":
             out["sv_coef"].append(np.array([float(v) for v in parts[2:]]))
         elif key == "iter":
@@ -134,6 +136,10 @@ def parse_dump(text: str) -> dict:
         elif key == "error":
             out["error"] = " ".join(parts[1:])
     out["sv_coef"] = np.array(out["sv_coef"]) if out["sv_coef"] else np.zeros((0, 0))
+    if out["prob"]:
+        pr = np.array(out["prob"])
+        out["prob_pred"] = pr[:, 0]
+        out["prob"] = pr[:, 1:]
     if out["dec"]:
         d = np.array(out["dec"])
         out["pred"] = d[:, 0]

@@ -3,7 +3,8 @@
 // oracle/Makefile into oracle/_ref/) on one libsvm text file and dumps
 // everything the parity tests compare: the model (rho, sv_coef, sv_indices,
 // nSV, labels), the solver's #iter/obj per binary subproblem, decision values
-// and labels for an optional test file, or cross-validation targets.
+// and labels for an optional test file (and class probabilities of a model
+// trained with -b 1), or cross-validation targets.
 //
 // usage: ref_dump [svm-train options] train_file [test_file]
 //        ref_dump -v nfold [options] train_file      (cross validation)
@@ -49,6 +50,18 @@ int main(int argc, char **argv)
             printf("\n");
         }
         free(dec);
+        /* class probabilities (svm_predict_probability) of a model trained with -b 1 */
+        if (svm_check_probability_model(model) &&
+            (svm_get_svm_type(model) == C_SVC || svm_get_svm_type(model) == NU_SVC)) {
+            double *pe = (double *)malloc(sizeof(double) * (k > 0 ? k : 1));
+            for (int i = 0; i < te.l; i++) {
+                double lab = svm_predict_probability(model, te.x[i], pe);
+                printf("prob %d %.17g", i, lab);
+                for (int c = 0; c < k; c++) printf(" %.17g", pe[c]);
+                printf("\n");
+            }
+            free(pe);
+        }
     }
     svm_free_and_destroy_model(&model);
     return 0;

@@ -24,7 +24,11 @@ from svmb200.lib import FORM_BF16X3, FORM_FP16X3, FORM_FP32, ResidentRows, make_
 
 pytestmark = pytest.mark.gpu
 
-TRAIN_CASES = [k for k, v in cases.CASES.items() if v[2] == "train"]
+# every training case except the wide sparse rows (the tensor forms hold a
+# dense split copy of the rows), the probability cases (covered by the exact
+# form) and the double-valued one (its own test)
+TRAIN_CASES = [k for k, v in cases.CASES.items() if v[2] == "train" and not k.endswith("_wide")
+               and not k.startswith("prob_") and k not in cases.DOUBLE_VALUED]
 
 
 def _train_tensor(engine, tr, prm, form=FORM_FP16X3):
@@ -57,10 +61,14 @@ def test_tensor_form_against_fp64_oracle(engine, name):
             sel = np.where(np.asarray(arr["sv_indices"]) == idx)[0]
             if len(sel):
                 c = np.abs(arr["sv_coef"][:, sel[0]])
-                assert np.all((c <= 1e-6) | (np.abs(c - prm.C) <= 1e-6)), f"row {idx} differs in SV set"
+                bound = 1.0 if prm.svm_type == 2 else prm.C
+                assert np.all((c <= 1e-6) | (np.abs(c - bound) <= 1e-6)), f"row {idx} differs in SV set"
     if te is not None and te.n:
         lab, _ = engine.predict(model, te)
-        assert np.array_equal(lab, gold64["pred"])
+        if prm.svm_type in (3, 4):
+            np.testing.assert_allclose(lab, gold64["pred"], rtol=0, atol=1e-4)
+        else:
+            assert np.array_equal(lab, gold64["pred"])
     model.free()
 
 
