@@ -46,7 +46,18 @@ typedef struct svmb_solve_stats {
     long long prefetched;       /* rows evaluated ahead of need */
     long long prefetch_used;    /* of those, rows a later lookup hit */
     long long prof_cycles[8];   /* SM cycles per loop section (diagnostics) */
+    long long fill_targets;     /* target positions of all row-evaluation passes: each pass reads
+                                   every target row once, whatever the number of its source rows */
+    int fill_path;              /* SVMB_FILL_*: how the solve evaluated its kernel rows */
+    int reserved;
 } svmb_solve_stats;
+
+#define SVMB_FILL_DENSE          0  /* dense rows on CUDA cores, sources staged in shared memory */
+#define SVMB_FILL_SPARSE_SCATTER 1  /* sparse rows; sources scattered into dense shared-memory vectors */
+#define SVMB_FILL_SPARSE_TABLE   2  /* sparse rows too wide to scatter; sources in a column-keyed
+                                       shared-memory table probed by each target's nonzeros */
+#define SVMB_FILL_SPARSE_MERGE   3  /* sparse rows; merge walks of two index lists in global memory */
+#define SVMB_FILL_TENSOR         4  /* tensor cores on the split copy of the rows */
 
 /* Parameters of a binary solve (the subset of svm_parameter the solver reads). */
 typedef struct svmb_params {

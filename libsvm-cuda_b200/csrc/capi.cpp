@@ -112,6 +112,8 @@ void finish_instance(const svmb_params &p, const SubProblem &sp, const SolveResu
     st.prefetched = R.out.prefetched;
     st.prefetch_used = R.out.prefetch_used;
     for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
+    st.fill_path = R.fill_path;
+    st.fill_targets = R.out.fill_targets;
 }
 
 int solve_many(const DeviceRows &rows, int ninst, const int *inst_ptr, const int *inst_rows, const double *inst_y,

@@ -7,6 +7,7 @@
 // launch (smo_kernel.cu) and the host only uploads the problem and reads the
 // result back.
 #include "engine.hpp"
+#include "svm_b200.h"
 
 #include <algorithm>
 #include <chrono>
@@ -461,7 +462,7 @@ long long smem_budget()
 // shared-memory staging of one instance's rows: source rows staged in
 // float32 (CUDA-core forms) or the tensor-core operand stages
 struct StagePlan {
-    int stage_cap = 0, stage_lds = 0, tc_n = 0, tile_bufs = 2;
+    int stage_cap = 0, stage_lds = 0, tc_n = 0, tile_bufs = 2, hash_slots = 0;
     long long bytes = 0;        // staging + aux area
     long long chunk_max = 0;    // positions of state one block can hold
 };
@@ -486,6 +487,11 @@ StagePlan stage_plan(const DeviceRows &rows, int form, long long budget, int til
         // the exact form stages its source values as float64
         const long long elem = form == FORM_EXACT ? 8 : 4;
         p.bytes = (((long long)p.stage_cap * p.stage_lds * elem) + 15) & ~15LL;
+        if (!rows.dense && p.stage_cap == 0) {
+            // too wide to scatter: the sources go into a column-keyed table
+            p.hash_slots = kHashSlots;
+            p.bytes = hash_bytes(form);
+        }
     }
     p.bytes += aux_bytes(form, tile_bufs);   // transpose tiles / prefetch candidates / block-product partial sums
     p.chunk_max = (budget - p.bytes) / kChunkBytes;
@@ -617,6 +623,7 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
     }
     w.used = used;
     w.stage.resize(count);
+    w.fill_path.assign(count, 0);
     w.tile_bufs = count > 0 ? sp_all[0].tile_bufs : 2;
     long long dyn = 0;
     for (int k = 0; k < count; k++) {
@@ -626,6 +633,13 @@ int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const
         w.stage[k][1] = sp_all[k].stage_lds;
         w.stage[k][2] = sp_all[k].tc_n;
         w.stage[k][3] = (int)cap;
+        w.stage[k][4] = sp_all[k].hash_slots;
+        const bool dense = rows_of(subs[first + k], rows).dense;
+        w.fill_path[k] = is_tc_form(prm.form)           ? SVMB_FILL_TENSOR
+                         : dense                        ? SVMB_FILL_DENSE
+                         : sp_all[k].stage_cap > 0      ? SVMB_FILL_SPARSE_SCATTER
+                         : sp_all[k].hash_slots > 0     ? SVMB_FILL_SPARSE_TABLE
+                                                        : SVMB_FILL_SPARSE_MERGE;
         dyn = std::max(dyn, sp_all[k].bytes + cap * kChunkBytes);
     }
     w.dyn_smem = (size_t)dyn;
@@ -826,6 +840,7 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
         D.stage_lds = w.stage[k][1];
         D.tc_n = w.stage[k][2];
         D.chunk_cap = w.stage[k][3];
+        D.hash_slots = w.stage[k][4];
         D.done_flag = w.done_flags ? w.done_flags + k : nullptr;
         D.tile_bufs = w.tile_bufs;
         {
@@ -889,6 +904,7 @@ int wave_fetch(const Wave &w, int k, SolveResult &r, cudaStream_t s)
     if (l) CK(xfer_async(r.alpha.data(), w.dev + w.o_alocal + 8 * w.loff[k], 8 * l, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     r.seconds = 0;
+    r.fill_path = w.fill_path[k];
     if (r.out.status < 0) {
         set_error("solver group barrier timed out");
         return -1;
@@ -921,6 +937,7 @@ int wave_finish(Wave &w, std::vector<SolveResult> &res)
         R.alpha.assign(h_alocal + w.loff[k], h_alocal + w.loff[k] + l);
         R.out = h_out[k];
         R.seconds = ms * 1e-3;
+        R.fill_path = w.fill_path[k];
         if (R.out.status < 0) {
             set_error("solver group barrier timed out");
             rc = -1;

@@ -43,6 +43,14 @@ constexpr int kAuxBytesTc = ((kCandBytes > kRedBytes ? kCandBytes : kRedBytes) +
 // transpose tiles per warp in the CUDA-core fills: a ring of up to 4 column
 // slices, all but the one in use in flight
 constexpr int kMaxTileBufs = 4;
+// Sparse rows too wide to scatter into shared memory (fewer than two dense
+// source vectors fit) stage a fill pass's sources as one open-addressing
+// table keyed by column: kHashSlots int keys (-1 = empty) followed by
+// kHashSlots x kSrcBatch values (float64 in the exact form, float32 else).
+// A pass whose sources hold more than kHashSlots/2 nonzeros in total falls
+// back to merge walks in global memory.
+constexpr int kHashSlots = 1024;
+SVMB_HD constexpr int hash_bytes(int form) { return kHashSlots * 4 + kHashSlots * kSrcBatch * (form == 0 ? 8 : 4); }
 SVMB_HD constexpr int tile_aux_bytes(int bufs) { return ((bufs * kTileBytes > kCandBytes ? bufs * kTileBytes : kCandBytes) + 15) / 16 * 16; }
 SVMB_HD constexpr int aux_bytes(int form, int tile_bufs) { return (form == 2 || form == 3) ? kAuxBytesTc : tile_aux_bytes(tile_bufs); }
 
@@ -148,6 +156,7 @@ struct SolveOut {
     long long q_evals;
     long long lookups, hits;
     long long fills, prefetched, prefetch_used;   // fill passes, rows prefetched, prefetched rows later hit
+    long long fill_targets;     // target positions of all fill passes (each pass reads its targets' rows once)
     // SM cycles spent by block 0 in each section of the loop (kProf* below)
     long long prof[8];
 };
@@ -189,6 +198,7 @@ struct InstanceDesc {
     int tc_n;                   // FORM_BF16X3: sources per tensor-core pass (16, 32 or 64); 0 otherwise
     int *done_flag;             // host-mapped word set to 1 once the whole instance has written its results, or nullptr
     int tile_bufs;              // transpose tiles per warp in the CUDA-core fills (1 to kMaxTileBufs; same in every instance of a launch)
+    int hash_slots;             // sparse rows, stage_cap == 0: sources staged in a kHashSlots table (0: merge walks)
 };
 
 }  // namespace svmb

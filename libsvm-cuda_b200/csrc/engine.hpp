@@ -83,6 +83,7 @@ struct SolveParams {
 };
 
 struct SolveResult {
+    int fill_path = 0;              // SVMB_FILL_*: how the solve evaluated its kernel rows
     std::vector<double> alpha;      // by local index (unsigned)
     SolveOut out{};
     double seconds = 0;
@@ -94,7 +95,8 @@ struct SolveResult {
 struct Wave {
     int first = 0, count = 0, used = 0, form = 0;
     std::vector<int> nb;                      // blocks per instance
-    std::vector<std::array<int, 4>> stage;    // stage_cap, stage_lds, tc_n, chunk_cap per instance
+    std::vector<std::array<int, 5>> stage;    // stage_cap, stage_lds, tc_n, chunk_cap, hash_slots per instance
+    std::vector<int> fill_path;               // SVMB_FILL_* per instance
     size_t dyn_smem = 0;
     struct Layout { size_t G, Gb, A, P, QD, Al, Y, S, PL, PR, Sc, Out, Sync, Part, Tag, Ep, St, Data, bytes; int sets, ways; };
     std::vector<Layout> lay;

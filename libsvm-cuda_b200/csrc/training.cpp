@@ -241,6 +241,8 @@ void fill_stats(const Decision &f, const SolveResult &R, int l, svmb_solve_stats
     st.prefetched = R.out.prefetched;
     st.prefetch_used = R.out.prefetch_used;
     for (int q = 0; q < 8; q++) st.prof_cycles[q] = R.out.prof[q];
+    st.fill_path = R.fill_path;
+    st.fill_targets = R.out.fill_targets;
 }
 
 // the solver's messages of one subproblem: the max_iter warning first

@@ -28,7 +28,9 @@ class SolveStats(C.Structure):
                 ("active_size", C.c_int), ("launch", C.c_int), ("seconds", C.c_double),
                 ("sum_active", C.c_longlong), ("q_evals", C.c_longlong), ("lookups", C.c_longlong),
                 ("hits", C.c_longlong), ("fills", C.c_longlong), ("prefetched", C.c_longlong),
-                ("prefetch_used", C.c_longlong), ("prof_cycles", C.c_longlong * 8)]
+                ("prefetch_used", C.c_longlong), ("prof_cycles", C.c_longlong * 8),
+                ("fill_targets", C.c_longlong), ("fill_path", C.c_int),
+                ("reserved", C.c_int)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "prof_cycles"}

@@ -90,6 +90,8 @@ CASES = {
     # rows as wide as the sparse text workload (d = 20,000, about 40 nonzeros)
     "rbf_sparse_wide":      (lambda: _sparse(6000, 1000, 20000, 81), "-s 0 -t 2 -c 4 -g 0.5", "train"),
     "linear_sparse_wide":   (lambda: _sparse(6000, 1000, 20000, 82), "-s 0 -t 0 -c 4", "train"),
+    # the pixel workload's shape at a tenth of its rows (d = 784, C = 10, gamma = 1/784)
+    "rbf_pixels_10k":       (lambda: _pixels(10000, 2000, 784, 34), "-s 0 -t 2 -c 10 -g 0.0012755102040816326", "train"),
     # full-precision double features (not float32 numbers): the engine stores float32
     "rbf_double_values":    (lambda: _dense64(600, 200, 16, 91), "-s 0 -t 2 -c 1 -g 0.0625", "train"),
 }
@@ -103,7 +105,7 @@ REFERENCE_ONLY = [k for k in CASES if k.startswith(("one_class", "eps_svr", "nu_
 DOUBLE_VALUED = ["rbf_double_values"]
 
 # cases small enough to run in the default CPU suite in a second or two
-FAST = [k for k in CASES if k not in ("rbf_dense_c1", "rbf_sparse_wide", "linear_sparse_wide")]
+FAST = [k for k in CASES if k not in ("rbf_dense_c1", "rbf_sparse_wide", "linear_sparse_wide", "rbf_pixels_10k")]
 
 
 def materialise(name, outdir):

@@ -22,6 +22,7 @@ pytestmark = pytest.mark.gpu
 TRAIN_CASES = [k for k, v in cases.CASES.items() if v[2] == "train" and k not in cases.DOUBLE_VALUED]
 CV_CASES = [k for k, v in cases.CASES.items() if v[2].startswith("cv:")]
 SVR_TYPES = (3, 4)
+FILL_SPARSE_TABLE = 2   # SVMB_FILL_SPARSE_TABLE
 
 
 def _check_sv_set(diff, ours, gold, l, C_bound):
@@ -63,6 +64,10 @@ def test_train_and_predict_match_reference(engine, name):
     for s, it, obj in zip(stats, gold["iter"], gold["obj"]):
         assert abs(s["iters"] - it) <= max(1, 0.02 * it), (s["iters"], it)
         assert abs(s["obj"] - obj) <= max(1e-6 * abs(obj), 5.1e-7), (s["obj"], obj)
+    if name.endswith("_wide"):
+        # rows as wide as the sparse text workload (d = 20,000) are too wide to
+        # scatter into shared memory: the column-keyed table path must have run
+        assert all(s["fill_path"] == FILL_SPARSE_TABLE for s in stats), [s["fill_path"] for s in stats]
     diff = compare_models(ours, gold, tr.n)
     assert diff["max_rho_diff"] <= 1e-4, diff
     _check_sv_set(diff, ours, gold, tr.n, _bound(prm, stats))
