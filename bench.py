@@ -191,33 +191,62 @@ def run_reference(args, world, rank):
 # ----------------------------------------------------------------------------
 # our arm
 # ----------------------------------------------------------------------------
-def cpu_baseline_sample(p, rows, ys, budget_s=20.0):
+def reference_train(lib, prob_rows, prm):
+    """svm_train of the reference's CPU solver on one problem: seconds, and the
+    solver's statistics from its messages (#iter, obj) and model (rho, nSV)."""
+    log = []
+    hook = cabi.PRINT_FUNC(lambda s: log.append(s.decode()))
+    lib.svm_set_print_string_function(hook)
+    nodes = cabi.NodeRows(prob_rows)
+    t0 = time.perf_counter()
+    m = lib.svm_train(C.byref(nodes.prob), C.byref(prm))
+    dt = time.perf_counter() - t0
+    text = "".join(log)
+    iters = [int(t.split()[0].rstrip(",")) for t in text.split("#iter = ")[1:]]
+    objs = [float(t.split(",")[0]) for t in text.split("obj = ")[1:]]
+    out = {"seconds": dt, "iters": iters, "obj": objs, "rho": [m.contents.rho[0]], "nr_sv": m.contents.l, "model": m}
+    return out
+
+
+def cpu_baseline_sample(p, rows, ys, ours, budget_s=20.0):
     """The reference's CPU solver (single core) on a seeded random sample of the
-    45 subproblems, until ~budget_s of CPU work: solves/s of that sample."""
+    45 subproblems, until ~budget_s of CPU work: solves/s of that sample, and
+    each sampled subproblem checked against the engine's result of the same
+    subproblem in the timed step (iterations, dual objective, rho, nSV)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
     lib = oracle_py.reference_lib()
     if lib is None:
-        return None
-    quiet = cabi.PRINT_FUNC(lambda s: None)
-    lib.svm_set_print_string_function(quiet)
+        return None, None
+    lib.svm_free_and_destroy_model.argtypes = [C.POINTER(C.POINTER(cabi.svm_model))]
     order = np.random.default_rng(12345).permutation(len(rows))
     done, spent = 0, 0.0
+    worst = {"iters_rel": 0.0, "obj_rel": 0.0, "rho_abs": 0.0, "nsv_diff": 0}
     for k in order:
         sub = p.take(rows[k])
         sub.y = ys[k]
-        nodes = cabi.NodeRows(sub)
         prm = cabi.make_param(svm_type=0, kernel_type=2, gamma=GAMMA, C_=CVAL, cache_size=100.0, eps=1e-3,
                               shrinking=1, cuda_flag=0)
-        t0 = time.perf_counter()
-        m = lib.svm_train(C.byref(nodes.prob), C.byref(prm))
-        spent += time.perf_counter() - t0
-        lib.svm_free_and_destroy_model(C.byref(m))
+        r = reference_train(lib, sub, prm)
+        spent += r["seconds"]
+        lib.svm_free_and_destroy_model(C.byref(r["model"]))
+        o = ours[k]
+        worst["iters_rel"] = max(worst["iters_rel"], abs(o["iters"] - r["iters"][0]) / r["iters"][0])
+        # the reference prints obj with %f: compare to that precision too
+        worst["obj_rel"] = max(worst["obj_rel"], max(abs(o["obj"] - r["obj"][0]) - 5e-7, 0.0) / abs(r["obj"][0]))
+        worst["rho_abs"] = max(worst["rho_abs"], abs(o["rho"] - r["rho"][0]))
+        worst["nsv_diff"] = max(worst["nsv_diff"], abs(o["nr_sv"] - r["nr_sv"]))
         done += 1
         if spent >= budget_s:
             break
-    return {"value": done / spent, "unit": "solves/s", "cores": 1, "kind": "reference",
-            "sample": f"{done} of the 45 subproblems (seeded random order), reference svm_train on 1 core, {spent:.1f} s"}
+    lib.svm_set_print_string_function(cabi.PRINT_FUNC(lambda s: None))
+    cpu = {"value": done / spent, "unit": "solves/s", "cores": 1, "kind": "reference",
+           "sample": f"{done} of the 45 subproblems (seeded random order), reference svm_train on 1 core, {spent:.1f} s"}
+    parity = {"checked": done, "max_iters_rel": worst["iters_rel"], "max_obj_rel": worst["obj_rel"],
+              "max_rho_abs": worst["rho_abs"], "max_nsv_diff": worst["nsv_diff"],
+              "bar": "iterations within 2%, obj rel 1e-6, |rho| 1e-4 (per subproblem, vs the reference's solver)",
+              "pass": worst["iters_rel"] <= 0.02 and worst["obj_rel"] <= 1e-6 and worst["rho_abs"] <= 1e-4}
+    return cpu, parity
 
 
 # ----------------------------------------------------------------------------
@@ -257,13 +286,104 @@ def precision_form_extra(eng, ResidentRows, make_params):
             "precision_bar": "obj within 1e-6 and rho within 1e-4 of the FP64 oracle: tests/test_gpu_tensor_form.py"}
 
 
+def _reference_lib():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    lib = oracle_py.reference_lib()
+    if lib is not None:
+        lib.svm_free_and_destroy_model.argtypes = [C.POINTER(C.POINTER(cabi.svm_model))]
+        lib.svm_predict.restype = C.c_double
+        lib.svm_predict.argtypes = [C.POINTER(cabi.svm_model), C.POINTER(cabi.svm_node)]
+    return lib
+
+
+def _compare(ours_stats, ref):
+    return {"iters": [ours_stats["iters"], ref["iters"][0]], "obj": [ours_stats["obj"], ref["obj"][0]],
+            "rho": [ours_stats["rho"], ref["rho"][0]], "nr_sv": [ours_stats["nr_sv"], ref["nr_sv"]]}
+
+
+def dense_c1_extra(eng):
+    """Binary C-SVC, RBF, n=4000 train / 1000 test, d=64 (two Gaussians at
+    +-0.5, unit std, 5% flips), C=1, gamma=1/64, eps=1e-3, 100 MB cache,
+    shrinking on: svm_train through svm.h on the GPU (host wall seconds from
+    host rows, after one untimed call) against the reference's svm_train on
+    one host core with the same flags; solutions and held-out labels compared."""
+    tr, te = datagen.dense_gauss(n=4000, n_test=1000, d=64, seed=1)
+    prm = cabi.make_param(svm_type=0, kernel_type=2, gamma=1.0 / 64, C_=1.0, cache_size=100.0, eps=1e-3,
+                          shrinking=1)
+    eng.train(tr, prm).free()
+    t0 = time.perf_counter()
+    model = eng.train(tr, prm)
+    gpu_s = time.perf_counter() - t0
+    st = eng.last_stats()[0]
+    lab, _ = eng.predict(model, te)
+    model.free()
+    out = {"workload": "dense RBF C-SVC n=4000 d=64 (Gaussians +-0.5, 5% flips), C=1, gamma=1/64, eps=1e-3, "
+                       "100 MB cache, shrinking", "gpu_train_s": gpu_s, "gpu_solve_device_s": st["seconds"]}
+    lib = _reference_lib()
+    if lib is not None:
+        prm.cuda_flag = 0
+        r = reference_train(lib, tr, prm)
+        nodes = cabi.NodeRows(te)
+        ref_lab = np.array([lib.svm_predict(r["model"], nodes.row(i)) for i in range(te.n)])
+        lib.svm_free_and_destroy_model(C.byref(r["model"]))
+        lib.svm_set_print_string_function(cabi.PRINT_FUNC(lambda s: None))
+        out.update({"reference_train_s": r["seconds"], "reference_cores": 1, "speedup": r["seconds"] / gpu_s,
+                    "vs_reference": _compare(st, r), "heldout_labels_identical": bool(np.array_equal(lab, ref_lab))})
+    return out
+
+
+def sparse_c2_extra(eng, ResidentRows, make_params):
+    """Sparse binary C-SVC, n=50,000 rows over d=20,000 features (Poisson(40)
+    nonzeros per row, lognormal values, rows L2-normalised, sparse-hyperplane
+    labels, 10% flips), C=4, gamma=0.5, eps=1e-3, RBF and linear: device
+    seconds of the solve on resident CSR rows (the rows are too wide to
+    scatter, so the fill passes stage their sources in the column-keyed
+    table).  The reference's CPU solver runs on a bounded sample (the first
+    2,000 rows), and the engine on the same sample for a like-for-like time
+    and a solution check."""
+    tr, _ = datagen.sparse_text(n=50000, n_test=0)
+    rows = ResidentRows(eng, tr)
+    idx = [np.arange(tr.n, dtype=np.int32)]
+    y = [np.ascontiguousarray(tr.y, dtype=np.float64)]
+    out = {"workload": "sparse C-SVC n=50000 d=20000 nnz~Poisson(40), C=4, gamma=0.5, eps=1e-3, 100 MB cache",
+           "rows_layout": "dense" if rows.dense else "csr"}
+    lib = _reference_lib()
+    small = tr.take(np.arange(2000))
+    srows = ResidentRows(eng, small)
+    for name, kt in (("rbf", 2), ("linear", 0)):
+        prm = make_params(svm_type=0, kernel_type=kt, gamma=0.5, C_pos=4.0, cache_mb=100.0)
+        _, st = rows.solve_many(idx, y, [prm])
+        s = st[0]
+        row_bytes = rows.bytes / max(rows.n, 1)
+        abytes = 46.0 * s["sum_active"] + s["fill_targets"] * (row_bytes + 4.0)
+        rec = {"seconds": s["seconds"], "iters": s["iters"], "obj": s["obj"], "rho": s["rho"], "nr_sv": s["nr_sv"],
+               "fill_path": s["fill_path"], "fills": s["fills"], "us_per_iter": s["seconds"] / max(s["iters"], 1) * 1e6,
+               "algorithmic_gbs": abytes / s["seconds"] / 1e9}
+        _, st2 = srows.solve_many([np.arange(small.n, dtype=np.int32)], [small.y.astype(np.float64)], [prm])
+        rec["sample_2000"] = {"gpu_seconds": st2[0]["seconds"]}
+        if lib is not None:
+            cp = cabi.make_param(svm_type=0, kernel_type=kt, gamma=0.5, C_=4.0, cache_size=100.0, eps=1e-3,
+                                 shrinking=1, cuda_flag=0)
+            r = reference_train(lib, small, cp)
+            lib.svm_free_and_destroy_model(C.byref(r["model"]))
+            rec["sample_2000"].update({"reference_seconds": r["seconds"], "reference_cores": 1,
+                                       "vs_reference": _compare(st2[0], r)})
+        out[name] = rec
+    if lib is not None:
+        lib.svm_set_print_string_function(cabi.PRINT_FUNC(lambda s: None))
+    srows.free()
+    rows.free()
+    return out
+
+
 def cv_grid_extra(eng):
     """5-fold cross-validation over C in {0.5,1,2,4,8} x gamma in {1/256, 4/256}
-    on the one-vs-one workload's 10 classes (sizes scaled by 1/4): every
+    on the one-vs-one workload's 10 classes (its full size, 53,646 rows): every
     point's and fold's 45 subproblems in batched launches
     (svmb_cross_validation_grid), against one svm_cross_validation per point."""
     import ctypes
-    tr, _, sizes = datagen.multiclass_geo(n_classes=10, largest=12000, ratio=0.8, d=D, seed=4, scale=0.25)
+    tr, _, sizes = datagen.multiclass_geo(n_classes=10, largest=12000, ratio=0.8, d=D, seed=4)
     prm = cabi.make_param(svm_type=0, kernel_type=2, gamma=GAMMA, C_=CVAL, cache_size=100.0, eps=1e-3, shrinking=1)
     Cs = [c for c in (0.5, 1.0, 2.0, 4.0, 8.0) for g in (1 / 256, 4 / 256)]
     gs = [g for c in (0.5, 1.0, 2.0, 4.0, 8.0) for g in (1 / 256, 4 / 256)]
@@ -442,9 +562,11 @@ def main():
         # device time of the step's launches (instances of one launch share its time)
         kern_s.append(sum({s["launch"]: s["seconds"] for s in stats}.values()))
         # algorithmic bytes of the launch: per iteration 46 B per active position
-        # (WSS 22 B + update 24 B), per kernel value evaluated one stored row + 4 B
+        # (WSS 22 B + update 24 B); per fill pass (one per Q row a cache miss
+        # needed) one read of every target row and the needed row's 4 B values.
+        # Rows evaluated alongside, speculatively, read no further bytes.
         row_bytes = res.bytes / max(res.n, 1)
-        alg_bytes.append(sum(46.0 * s["sum_active"] + s["q_evals"] * (row_bytes + 4.0) for s in stats))
+        alg_bytes.append(sum(46.0 * s["sum_active"] + s["fill_targets"] * (row_bytes + 4.0) for s in stats))
         stats_all.append(stats)
     launches = eng.launches() - launches0
     clk = clocks.stop()
@@ -519,10 +641,12 @@ def main():
         abytes = sum(alg_bytes) / len(alg_bytes)
         achieved = abytes / kavg / 1e9
         iters = [s["iters"] for s in stats_all[-1]]
-        cpu = None if args.no_cpu_baseline else cpu_baseline_sample(p, rows, ys)
+        cpu, parity = (None, None) if args.no_cpu_baseline else cpu_baseline_sample(p, rows, ys, stats_all[-1])
         extras = {}
         if world == 1 and not args.no_extras:
             for name, fn in (("precision_form", lambda: precision_form_extra(eng, ResidentRows, make_params)),
+                             ("dense_c1", lambda: dense_c1_extra(eng)),
+                             ("sparse_c2", lambda: sparse_c2_extra(eng, ResidentRows, make_params)),
                              ("cv_grid", lambda: cv_grid_extra(eng)),
                              ("serving", lambda: serving_extra(eng, make_params))):
                 try:
@@ -544,10 +668,17 @@ def main():
                          "traffic": TRAFFIC_PER_LAUNCH if world == 1 else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one steady-state "
                                            "launch of this workload (profiles/smo_persistent_exact_ovo45_dram.txt)",
+                         "dram_frac": (TRAFFIC_PER_LAUNCH / kavg / 1e9) / peak if world == 1 else None,
+                         "limiter": "latency: the per-iteration chain of two group exchanges, cache decisions and "
+                                    "L2-resident row fills (barrier and long-scoreboard stalls lead; DRAM and L2 "
+                                    "far from their peaks), see profiles/",
                          "kernel": "smo_persistent<FORM_EXACT>",
                          "algorithmic_bytes_per_launch": abytes, "kernel_ms": kavg * 1e3,
+                         "numerator": "46 B per active position per iteration + per fill pass one read of each "
+                                      "target row and 4 B per target (fill_targets); speculative rows add nothing",
                          "peak_kind": f"{peak_kind} hbm_gbs"},
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clk,
             "gpu_launches": int(launches),
             "iters_total": int(sum(iters)), "iters_max": int(max(iters)), "solver_launches_per_step": launches_per_step,

@@ -49,7 +49,7 @@ constexpr int kGStageBytes = 2 * kGTileA + 2 * kGTileB; // A hi, A lo, B hi, B l
 constexpr int kGSmem = kGStages * kGStageBytes + 1024;  // + alignment slack
 
 struct GramArgs {
-    const uint16_t *xs;         // split rows [n][nchunk][128]
+    const uint16_t *xs;         // split rows [n][nchunk][128] of the tile rows (A)
     const double *xinv;         // per-row inverse scales (fp16 split) or nullptr
     long long rs;               // row stride in 16-bit elements (nchunk * 128)
     int nchunk;
@@ -58,9 +58,13 @@ struct GramArgs {
     const int *ib;
     int nb;
     KernelParams kp;
-    const double *xsq;          // norms by row id
-    double *out;                // [ma][ldo]
+    const double *xsq;          // norms by row id (A)
+    const uint16_t *xs_b;       // the tile columns' rows (B): the same layout and nchunk
+    const double *xinv_b;
+    const double *xsq_b;
+    double *out;                // [ma][ldo], or [nb][ldo] when `trans`
     long long ldo;
+    int trans;
     int *err;
 };
 
@@ -117,7 +121,7 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
                 const int rb = r - kGM;
                 const long long o = offB[rb];
                 tc::cp_async16(sa + 2 * kGTileA + (q >= 8 ? kGTileB : 0) + tc::sw128_offset(rb, q & 7),
-                               a.xs + (o < 0 ? 0 : o) + kc * 128 + q * 8, o < 0 ? 0u : 16u);
+                               a.xs_b + (o < 0 ? 0 : o) + kc * 128 + q * 8, o < 0 ? 0u : 16u);
             }
         }
     };
@@ -187,14 +191,16 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
         const int ra = a.ia ? a.ia[row] : row;
         const double xa = a.xsq[ra];
         const double sa_inv = a.xinv ? a.xinv[ra] : 1.0;
-        double *dst = a.out + (long long)row * a.ldo;
 #pragma unroll 4
         for (int k = 0; k < 32; k++) {
             const int col = n0 + ch * 32 + k;
             if (col < a.nb) {
                 const int rb = a.ib ? a.ib[col] : col;
-                const double sb_inv = a.xinv ? a.xinv[rb] : 1.0;
-                dst[col] = kernel_from_dot(a.kp, __dmul_rn(__dmul_rn(acc[k], sa_inv), sb_inv), xa, a.xsq[rb]);
+                const double sb_inv = a.xinv_b ? a.xinv_b[rb] : 1.0;
+                const double v = kernel_from_dot(a.kp, __dmul_rn(__dmul_rn(acc[k], sa_inv), sb_inv), xa, a.xsq_b[rb]);
+                // transposed: the lanes of a warp (consecutive rows) write consecutive words
+                if (a.trans) a.out[(long long)col * a.ldo + row] = v;
+                else a.out[(long long)row * a.ldo + col] = v;
             }
         }
     }
@@ -361,7 +367,11 @@ cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, 
         a.ia = d_ia; a.ma = ma; a.ib = d_ib; a.nb = nb;
         a.kp = kp;
         a.xsq = rows.xsq[FORM_EXACT];
+        a.xs_b = rows.Xs;
+        a.xinv_b = rows.xinv;
+        a.xsq_b = rows.xsq[FORM_EXACT];
         a.out = d_out; a.ldo = ldo;
+        a.trans = 0;
         a.err = d_err;
         dim3 grid((nb + kGN - 1) / kGN, (ma + kGM - 1) / kGM);
         if (bf16) gram_split_kernel<true><<<grid, kGThreads, kGSmem, s>>>(a);
@@ -373,6 +383,37 @@ cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, 
         else
             kblock_cuda_kernel<FORM_FP32><<<grid, block, 0, s>>>(rows.view(FORM_FP32), d_ia, ma, d_ib, nb, kp, d_out, ldo);
     }
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const KernelParams &kp, int form, int ma,
+                                 int nb, double *d_out_t, long long ldo, int *d_err, cudaStream_t s)
+{
+    if (ma <= 0 || nb <= 0) return cudaSuccess;
+    if (!is_tc_form(form) || A.split_form != form || B.split_form != form || A.nchunk != B.nchunk)
+        return cudaErrorInvalidValue;
+    const bool bf16 = form == FORM_BF16X3;
+    const void *fn = bf16 ? (const void *)gram_split_kernel<true> : (const void *)gram_split_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem);
+    if (e != cudaSuccess) return e;
+    GramArgs a;
+    a.xs = A.Xs;
+    a.xinv = A.xinv;
+    a.nchunk = A.nchunk;
+    a.rs = (long long)A.nchunk * 2 * kSplitChunk;
+    a.ia = nullptr; a.ma = ma; a.ib = nullptr; a.nb = nb;
+    a.kp = kp;
+    a.xsq = A.xsq[FORM_EXACT];
+    a.xs_b = B.Xs;
+    a.xinv_b = B.xinv;
+    a.xsq_b = B.xsq[FORM_EXACT];
+    a.out = d_out_t; a.ldo = ldo;
+    a.trans = 1;
+    a.err = d_err;
+    dim3 grid((nb + kGN - 1) / kGN, (ma + kGM - 1) / kGM);
+    if (bf16) gram_split_kernel<true><<<grid, kGThreads, kGSmem, s>>>(a);
+    else gram_split_kernel<false><<<grid, kGThreads, kGSmem, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }

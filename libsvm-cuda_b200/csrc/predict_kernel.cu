@@ -7,6 +7,14 @@
 // sum runs sequentially over the two classes' SVs in model order, exactly as
 // the reference, so decision values match it bit for bit on float inputs.
 // The file is compiled with -fmad=false.
+//
+// Kernel values are kept SV-major, kv[s][t] for the t-th test row of a chunk,
+// so that the pair sums (one thread per test row and pair, each walking the
+// SVs in model order) read consecutive words across a warp.  Dense rows take
+// a tiled kernel: a block computes 64 test rows x 64 SVs, 16 features at a
+// time staged as float64 in shared memory, 4 x 4 values per thread.  With a
+// tensor-core predict form the values come from the split-product kernel
+// block of the SVs' split copy (kept with the model) and the chunk's.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -107,58 +115,84 @@ __device__ double kval_csr(const KP &kp, const long long *rpa, const int *ca, co
     return tanh(__dadd_rn(__dmul_rn(kp.gamma, sum), kp.coef0));
 }
 
-constexpr int kTT = 8;   // test rows per block (dense path)
+constexpr int kPT = 64;   // test rows per tile (dense path)
+constexpr int kPS = 64;   // SVs per tile
+constexpr int kPK = 16;   // features per staged slice
 
-// dense path: block = kTT test rows (staged in smem) x 256 SVs (one per thread)
-__global__ void kvalue_dense(KP kp, const float *__restrict__ T, int nt, const float *__restrict__ S, int ns, int ld,
-                             double *__restrict__ out)
+__device__ __forceinline__ double kfinish(const KP &kp, double acc)
 {
-    extern __shared__ __align__(16) float tst[];
-    const int t0 = blockIdx.y * kTT;
-    const int tcount = min(kTT, nt - t0);
-    for (int k = threadIdx.x; k < kTT * ld; k += blockDim.x) {
-        const int tr = k / ld, c = k % ld;
-        tst[k] = tr < tcount ? T[(long long)(t0 + tr) * ld + c] : 0.0f;
-    }
-    __syncthreads();
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= ns) return;
-    const float *sv = S + (long long)s * ld;
-    double acc[kTT];
+    if (kp.type == 2) return exp(__dmul_rn(-kp.gamma, acc));
+    if (kp.type == 0) return acc;
+    if (kp.type == 1) return powi_p(__dadd_rn(__dmul_rn(kp.gamma, acc), kp.coef0), kp.degree);
+    return tanh(__dadd_rn(__dmul_rn(kp.gamma, acc), kp.coef0));
+}
+
+// dense path: a 64 x 64 tile of K(test, SV), out[s][t] (ldo = nt).  Thread
+// (ty, tx) of 16 x 16 owns test rows t0 + tx + 16i and SVs s0 + 4ty + j; every
+// value accumulates over the features in order, as the reference's walk does
+// (RBF: the squared difference; a feature zero in both adds nothing).
+__global__ void __launch_bounds__(256) kvalue_tile(KP kp, const float *__restrict__ T, int nt,
+                                                  const float *__restrict__ S, int ns, int ld,
+                                                  double *__restrict__ out)
+{
+    __shared__ double ta[kPK][kPT + 1];
+    __shared__ double sb[kPK][kPS + 1];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int t0 = blockIdx.y * kPT, s0 = blockIdx.x * kPS;
+    double acc[4][4];
 #pragma unroll
-    for (int k = 0; k < kTT; k++) acc[k] = 0.0;
-    for (int c = 0; c < ld; c += 4) {
-        const float4 w = __ldg(reinterpret_cast<const float4 *>(sv + c));
-        const float wv[4] = {w.x, w.y, w.z, w.w};
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+    // loader: 64 rows x 16 features = 256 float4 pieces per operand, one per thread
+    const int lr = tid >> 2, lc = (tid & 3) * 4;
+    for (int k0 = 0; k0 < ld; k0 += kPK) {
+        const int c = k0 + lc;
+        float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va;
+        if (t0 + lr < nt && c < ld) va = __ldg(reinterpret_cast<const float4 *>(T + (long long)(t0 + lr) * ld + c));
+        if (s0 + lr < ns && c < ld) vb = __ldg(reinterpret_cast<const float4 *>(S + (long long)(s0 + lr) * ld + c));
+        __syncthreads();
+        ta[lc][lr] = va.x; ta[lc + 1][lr] = va.y; ta[lc + 2][lr] = va.z; ta[lc + 3][lr] = va.w;
+        sb[lc][lr] = vb.x; sb[lc + 1][lr] = vb.y; sb[lc + 2][lr] = vb.z; sb[lc + 3][lr] = vb.w;
+        __syncthreads();
 #pragma unroll
-            for (int k = 0; k < kTT; k++) {
-                const float xv = tst[k * ld + c + q];
-                if (kp.type == 2) {
-                    const double d = __dsub_rn((double)xv, (double)wv[q]);
-                    acc[k] = __dadd_rn(acc[k], __dmul_rn(d, d));
-                } else {
-                    acc[k] = __dadd_rn(acc[k], __dmul_rn((double)xv, (double)wv[q]));
+        for (int kk = 0; kk < kPK; kk++) {
+            double av[4], bv[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) av[i] = ta[kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; j++) bv[j] = sb[kk][4 * ty + j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    if (kp.type == 2) {
+                        const double d = __dsub_rn(av[i], bv[j]);
+                        acc[i][j] = __dadd_rn(acc[i][j], __dmul_rn(d, d));
+                    } else {
+                        acc[i][j] = __dadd_rn(acc[i][j], __dmul_rn(av[i], bv[j]));
+                    }
                 }
-            }
         }
     }
-    for (int k = 0; k < tcount; k++) {
-        double v;
-        if (kp.type == 2) v = exp(__dmul_rn(-kp.gamma, acc[k]));
-        else if (kp.type == 0) v = acc[k];
-        else if (kp.type == 1) v = powi_p(__dadd_rn(__dmul_rn(kp.gamma, acc[k]), kp.coef0), kp.degree);
-        else v = tanh(__dadd_rn(__dmul_rn(kp.gamma, acc[k]), kp.coef0));
-        out[(long long)(t0 + k) * ns + s] = v;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int sv = s0 + 4 * ty + j;
+        if (sv >= ns) continue;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int t = t0 + tx + 16 * i;
+            if (t < nt) out[(long long)sv * nt + t] = kfinish(kp, acc[i][j]);
+        }
     }
 }
 
+// sparse path: out[s][t] = K(test t, SV s) by merge walks, consecutive threads on consecutive test rows
 __global__ void kvalue_csr(KP kp, Rows T, Rows S, double *__restrict__ out)
 {
     const long long total = (long long)T.n * S.n;
     for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total; id += (long long)gridDim.x * blockDim.x) {
-        const int t = (int)(id / S.n), s = (int)(id % S.n);
+        const int s = (int)(id / T.n), t = (int)(id % T.n);
         out[id] = kval_csr(kp, T.rowptr, T.col, T.val, t, S.rowptr, S.col, S.val, s);
     }
 }
@@ -171,19 +205,22 @@ __global__ void pair_sums(const double *__restrict__ kv, int nt, int ns, int nr_
     const int npair = nr_class * (nr_class - 1) / 2;
     const long long total = (long long)nt * npair;
     for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total; id += (long long)gridDim.x * blockDim.x) {
-        const int t = (int)(id / npair);
-        const int p = (int)(id % npair);
+        // consecutive threads on consecutive test rows of one pair
+        const int p = (int)(id / nt);
+        const int t = (int)(id % nt);
         // pair index -> (i,j)
         int i = 0, rem = p;
         while (rem >= nr_class - 1 - i) { rem -= nr_class - 1 - i; ++i; }
         const int j = i + 1 + rem;
-        const double *k = kv + (long long)t * ns;
+        const double *k = kv + t;                // kv[s][t]: SV s of test row t at s * nt
         const double *coef1 = coef + (long long)(j - 1) * ns;
         const double *coef2 = coef + (long long)i * ns;
         double sum = 0;
-        for (int q = 0; q < nsv[i]; q++) sum = __dadd_rn(sum, __dmul_rn(coef1[start[i] + q], k[start[i] + q]));
-        for (int q = 0; q < nsv[j]; q++) sum = __dadd_rn(sum, __dmul_rn(coef2[start[j] + q], k[start[j] + q]));
-        dec[id] = __dsub_rn(sum, rho[p]);
+        for (int q = 0; q < nsv[i]; q++)
+            sum = __dadd_rn(sum, __dmul_rn(coef1[start[i] + q], k[(long long)(start[i] + q) * nt]));
+        for (int q = 0; q < nsv[j]; q++)
+            sum = __dadd_rn(sum, __dmul_rn(coef2[start[j] + q], k[(long long)(start[j] + q) * nt]));
+        dec[(long long)t * npair + p] = __dsub_rn(sum, rho[p]);
     }
 }
 
@@ -196,6 +233,7 @@ struct Session {
     // device copy
     Rows sv;
     Rows sv_csr;                // CSR copy of dense SVs for the merge path (made on first need)
+    std::unique_ptr<DeviceRows> sv_tc;   // the SVs in a tensor predict form (split copy), made on first need
     int d = 0, base = 1;
     double *coef = nullptr, *rho = nullptr;
     int *start = nullptr, *nsv = nullptr;
@@ -203,6 +241,7 @@ struct Session {
     {
         sv.release();
         sv_csr.release();
+        sv_tc.reset();
         cudaFree(coef); cudaFree(rho); cudaFree(start); cudaFree(nsv);
         coef = rho = nullptr;
         start = nsv = nullptr;
@@ -319,47 +358,53 @@ Session *get_session(const svm_model *m)
     return raw;
 }
 
-// Tensor-core kernel values: the SVs and the test rows of a chunk go into one
-// row set (column = feature index), whose split copy feeds the block product
-// K(test, SV) on the tensor cores; RBF uses the float64 norms of both.
-int kvalue_tensor(const svm_model *m, const svm_node *const *rows, int tn, int form, double *kv)
+// rows as host CSR (0-based columns) of width d
+int rows_to_device(const svm_node *const *x, int n, int d, int form, DeviceRows &out)
 {
-    const int l = m->l;
-    const int n = l + tn;
     std::vector<long long> rp((size_t)n + 1, 0);
     std::vector<int> col;
     std::vector<float> val;
-    int maxi = 0;
     for (int r = 0; r < n; r++) {
-        const svm_node *x = r < l ? m->SV[r] : rows[r - l];
-        for (const svm_node *p = x; p->index != -1; ++p) {
+        for (const svm_node *p = x[r]; p->index != -1; ++p) {
             col.push_back(p->index);
             val.push_back((float)p->value);
-            maxi = std::max(maxi, p->index);
         }
         rp[r + 1] = (long long)col.size();
     }
     if (col.empty()) { col.push_back(0); val.push_back(0.0f); }
-    DeviceRows dr;
-    if (upload_csr(rp.data(), col.data(), val.data(), n, maxi + 1, dr, -1, 0) != 0) return -1;
-    if (dr.prepare_form(form, 0) != 0) return -1;
-    std::vector<int> ia(tn), ib(l);
-    for (int t = 0; t < tn; t++) ia[t] = l + t;
-    for (int s = 0; s < l; s++) ib[s] = s;
-    int *d_ia = nullptr, *d_ib = nullptr, *d_err = nullptr;
-    PK(cudaMalloc(&d_ia, sizeof(int) * (size_t)tn));
-    PK(cudaMalloc(&d_ib, sizeof(int) * (size_t)l));
+    if (upload_csr(rp.data(), col.data(), val.data(), n, d, out, -1, 0) != 0) return -1;
+    return out.prepare_form(form, 0);
+}
+
+// Tensor-core kernel values kv[s][t] of a chunk of test rows: the SVs' split
+// copy is made once per model (and form, and width), the chunk's rows are
+// split here, and the block product K(test, SV) runs on the tensor cores;
+// RBF uses the float64 norms of both.
+int kvalue_tensor(const svm_model *m, Session *s, const svm_node *const *rows, int tn, int form, double *kv)
+{
+    int maxi = s->d - 1;
+    for (int r = 0; r < tn; r++)
+        for (const svm_node *p = rows[r]; p->index != -1; ++p) maxi = std::max(maxi, p->index);
+    // both row sets need the same split width; test rows wider than the SVs
+    // widen it (their extra features still count in the RBF norms)
+    const int width = maxi + 1;
+    if (!s->sv_tc || s->sv_tc->split_form != form || s->sv_tc->d < width) {
+        s->sv_tc.reset(new DeviceRows());
+        if (rows_to_device(m->SV, m->l, width, form, *s->sv_tc) != 0) {
+            s->sv_tc.reset();
+            return -1;
+        }
+    }
+    DeviceRows T;
+    if (rows_to_device(rows, tn, s->sv_tc->d, form, T) != 0) return -1;
+    int *d_err = nullptr;
     PK(cudaMalloc(&d_err, sizeof(int)));
-    PK(xfer(d_ia, ia.data(), sizeof(int) * (size_t)tn, cudaMemcpyHostToDevice));
-    PK(xfer(d_ib, ib.data(), sizeof(int) * (size_t)l, cudaMemcpyHostToDevice));
     PK(cudaMemset(d_err, 0, sizeof(int)));
     KernelParams kp{m->param.kernel_type, m->param.degree, m->param.gamma, m->param.coef0};
-    cudaError_t e = launch_kernel_block(dr, kp, form, d_ia, tn, d_ib, l, kv, l, d_err, 0);
+    cudaError_t e = launch_kernel_block2(T, *s->sv_tc, kp, form, tn, m->l, kv, tn, d_err, 0);
     int herr = 0;
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = xfer(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(d_ia);
-    cudaFree(d_ib);
     cudaFree(d_err);
     if (e != cudaSuccess || herr) {
         set_error(e != cudaSuccess ? std::string("tensor-core kernel values: ") + cudaGetErrorString(e)
@@ -425,17 +470,11 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
                 for (const svm_node *p = rows[t0 + r]; p->index != -1; ++p) maxi = std::max(maxi, p->index);
             const bool wider = maxi + 1 > s->d;
             if (is_tc_form(g_predict_form)) {
-                if (kvalue_tensor(m, rows + t0, tn, g_predict_form, kv) != 0) return -1;
+                if (kvalue_tensor(m, s, rows + t0, tn, g_predict_form, kv) != 0) return -1;
             } else if (s->sv.dense && !wider) {
-                const size_t smem = (size_t)kTT * s->sv.ld * sizeof(float);
-                if (smem > 200 * 1024) {
-                    set_error("feature dimension too large for the dense prediction path");
-                    return -1;
-                }
                 if (upload_nodes(rows + t0, tn, s->d, s->base, true, T) != 0) return -1;
-                dim3 grid((m->l + 255) / 256, (tn + kTT - 1) / kTT);
-                cudaFuncSetAttribute(kvalue_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                kvalue_dense<<<grid, 256, smem>>>(kp, T.X, tn, s->sv.X, m->l, s->sv.ld, kv);
+                dim3 grid((m->l + kPS - 1) / kPS, (tn + kPT - 1) / kPT);
+                kvalue_tile<<<grid, 256>>>(kp, T.X, tn, s->sv.X, m->l, s->sv.ld, kv);
                 count_launch();
             } else {
                 if (s->sv.dense && !s->sv_csr.rowptr &&
@@ -443,7 +482,7 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
                     return -1;
                 const Rows &Sc = s->sv.dense ? s->sv_csr : s->sv;
                 if (upload_nodes(rows + t0, tn, maxi + 1, s->base, false, T) != 0) return -1;
-                kvalue_csr<<<std::min<long long>(((long long)tn * m->l + 255) / 256, 148 * 16), 256>>>(kp, T, Sc, kv);
+                kvalue_csr<<<(int)std::min<long long>(((long long)tn * m->l + 255) / 256, 148 * 16), 256>>>(kp, T, Sc, kv);
                 count_launch();
             }
             pair_sums<<<std::min<long long>(((long long)tn * npair + 127) / 128, 148 * 8), 128>>>(kv, tn, m->l, k, s->start, s->nsv, s->coef, s->rho, d_dec);
