@@ -260,7 +260,7 @@ def precision_form_extra(eng, ResidentRows, make_params):
     CUDA-core form (one row per cache miss, incremental G_bar) and the exact
     form (bit-identical to the reference's float-Q solver).  Device seconds of
     the solve launch."""
-    tr, _ = datagen.dense_pixels(n=100000, n_test=10)
+    tr, te = datagen.dense_pixels(n=100000, n_test=20000)
     rows = ResidentRows(eng, tr, layout=1)
     idx = [np.arange(tr.n, dtype=np.int32)]
     y = [np.ascontiguousarray(tr.y, dtype=np.float64)]
@@ -278,9 +278,11 @@ def precision_form_extra(eng, ResidentRows, make_params):
     for name in out:
         out[name]["obj_rel_diff_vs_exact"] = abs(out[name]["obj"] - ex["obj"]) / abs(ex["obj"])
         out[name]["rho_diff_vs_exact"] = abs(out[name]["rho"] - ex["rho"])
+    predict = decision_values_extra(eng, tr, te)
     return {"workload": "dense RBF C-SVC n=100000 d=784 (k/255, 70% zeros, tanh-teacher labels, 10% flips), C=10, "
                         "gamma=1/784, eps=1e-3, 4096 MB cache",
             "forms": out,
+            "decision_values": predict,
             "tensor_speedup_vs_fp32_plain": out["fp32_plain"]["seconds"] / out["fp16x3_tensor"]["seconds"],
             "tensor_speedup_vs_exact": out["exact"]["seconds"] / out["fp16x3_tensor"]["seconds"],
             "precision_bar": "obj within 1e-6 and rho within 1e-4 of the FP64 oracle: tests/test_gpu_tensor_form.py"}
@@ -374,6 +376,45 @@ def sparse_c2_extra(eng, ResidentRows, make_params):
         lib.svm_set_print_string_function(cabi.PRINT_FUNC(lambda s: None))
     srows.free()
     rows.free()
+    return out
+
+
+def decision_values_extra(eng, tr, te):
+    """The decision-value pass of the pixel workload: 20,000 held-out rows
+    against the model trained on the 100,000 rows (through svm_train, FP16X3
+    form), one svmb_predict_batch call each in the exact form (the reference's
+    k_function bit for bit: squared differences in float64 on CUDA cores) and
+    in the FP16X3 tensor form (split products on tcgen05, float64 norms).
+    Host wall seconds of the call from host rows (conversion, upload, kernel
+    values, pair sums, download), after a small untimed call that uploads the
+    SVs.  Algorithmic work: 2 * rows * SVs * d flops of dot products."""
+    prm = cabi.make_param(svm_type=0, kernel_type=2, gamma=1.0 / 784, C_=10.0, cache_size=4096.0, eps=1e-3,
+                          shrinking=1)
+    eng.set_option("form", 3)
+    try:
+        model = eng.train(tr, prm)
+    finally:
+        eng.set_option("form", 0)
+    nsv = model.contents.l
+    warm = te.take(np.arange(64))
+    out = {"rows": te.n, "svs": nsv, "d": 784}
+    res = {}
+    for name, form in (("exact", 0), ("fp16x3_tensor", 3)):
+        eng.set_option("predict_form", form)
+        try:
+            eng.predict(model, warm)
+            t0 = time.perf_counter()
+            lab, dec = eng.predict(model, te)
+            dt = time.perf_counter() - t0
+        finally:
+            eng.set_option("predict_form", 0)
+        flops = 2.0 * te.n * nsv * 784
+        out[name] = {"seconds": dt, "algorithmic_tflops": flops / dt / 1e12}
+        res[name] = (lab, dec)
+    out["labels_identical"] = bool(np.array_equal(res["exact"][0], res["fp16x3_tensor"][0]))
+    out["max_abs_dec_diff"] = float(np.max(np.abs(res["exact"][1] - res["fp16x3_tensor"][1])))
+    out["tensor_speedup"] = out["exact"]["seconds"] / out["fp16x3_tensor"]["seconds"]
+    model.free()
     return out
 
 

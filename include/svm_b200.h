@@ -120,7 +120,13 @@ void svmb_print_nothing(const char *s);
  *            instances in one launch); speed only, results never depend on it
  *   "predict_form" SVMB_FORM_EXACT (default: the reference's kernel values bit
  *            for bit) or a tensor-core form: svm_predict* and svmb_predict_batch
- *            then evaluate K(test rows, SVs) as block products on the tensor cores */
+ *            then evaluate K(test rows, SVs) as block products on the tensor cores
+ *   "wait_limit_ms" bound of every wait of a solver block for the other blocks
+ *            of its group (0 = the default, 30 s); a wait that runs out makes
+ *            the whole group return and the call report an error
+ *   "test_drop_block" 1: the next solver launch leaves out its last thread
+ *            block (one shot), so that its group's waits run out; for testing
+ *            the timeout path (the instance must have two or more blocks) */
 int svmb_set_option(const char *name, long long value);
 
 /* The autotuner's configuration of the last batched solve of this process:

@@ -26,6 +26,15 @@
 
 namespace svmb {
 
+// bound of the solver groups' cross-block waits (ns, 0: the kernel's default)
+// and the one-shot test hook that launches a wave without its last block
+static std::atomic<long long> g_wait_ns{0};
+void set_wait_limit_ms(long long ms) { g_wait_ns = ms > 0 ? ms * 1000000LL : 0; }
+
+static std::atomic<int> g_drop_block{0};
+void arm_drop_block() { g_drop_block = 1; }
+
+
 static thread_local std::string g_last_error;
 void set_error(const std::string &msg) { g_last_error = msg; }
 const char *last_error() { return g_last_error.c_str(); }
@@ -703,7 +712,8 @@ static cudaError_t wave_issue(Wave &w, InstanceDesc *d_desc, int *d_block_inst, 
     if (e == cudaSuccess) e = cudaMemsetAsync(dev + w.o_zero, 0, w.zero_bytes, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(dev + w.o_tag, 0xff, w.tag_bytes, s);
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.ev0, s, rec);
-    if (e == cudaSuccess) e = launch_smo(w.form, d_desc, d_block_inst, w.used, w.dyn_smem, w.cooperative, s);
+    if (e == cudaSuccess)
+        e = launch_smo(w.form, d_desc, d_block_inst, w.used - (w.drop_last_block ? 1 : 0), w.dyn_smem, w.cooperative, s);
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.ev1, s, rec);
     if (e == cudaSuccess) e = xfer_async(host + w.up_bytes, dev + w.o_out, w.down_bytes, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(w.done, s, rec);
@@ -841,6 +851,7 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
         D.tc_n = w.stage[k][2];
         D.chunk_cap = w.stage[k][3];
         D.hash_slots = w.stage[k][4];
+        D.wait_ns = g_wait_ns.load();
         D.done_flag = w.done_flags ? w.done_flags + k : nullptr;
         D.tile_bufs = w.tile_bufs;
         {
@@ -879,6 +890,10 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
         memcpy(h_p + w.loff[k], sp.p.data(), sizeof(double) * l);
         memcpy(h_row + w.loff[k], sp.rows.data(), sizeof(int) * l);
         memcpy(h_y + w.loff[k], sp.y.data(), (size_t)l);
+    }
+    if (g_drop_block.exchange(0)) {
+        w.drop_last_block = true;
+        w.use_graph = false;
     }
     if (w.use_graph) return wave_issue_graph(w, d_desc, d_block_inst, s);
     CK(cudaEventCreate(&w.ev0));
@@ -1054,6 +1069,7 @@ void autotune_last(int *prefetch, int *rows_per_block, int *exploring)
 
 static int g_graphs_on = 1;
 void set_graphs(int on) { g_graphs_on = on ? 1 : 0; }
+
 
 static int g_fill_depth = 2;
 int set_fill_depth(int bufs)

@@ -199,6 +199,7 @@ struct InstanceDesc {
     int *done_flag;             // host-mapped word set to 1 once the whole instance has written its results, or nullptr
     int tile_bufs;              // transpose tiles per warp in the CUDA-core fills (1 to kMaxTileBufs; same in every instance of a launch)
     int hash_slots;             // sparse rows, stage_cap == 0: sources staged in a kHashSlots table (0: merge walks)
+    long long wait_ns;          // bound of every cross-block wait, in ns of %globaltimer (0: 30 s)
 };
 
 }  // namespace svmb

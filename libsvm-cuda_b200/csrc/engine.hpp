@@ -108,6 +108,7 @@ struct Wave {
     cudaStream_t stream = nullptr;
     bool cooperative = true;   // false: plain launch (the caller guarantees the blocks are co-resident)
     bool use_graph = false;    // replay a captured graph of the stream work when the layout repeats
+    bool drop_last_block = false;   // test hook: launch without the last block (its group's waits run out)
     bool own_events = true;    // the events belong to this wave (not to a cached graph)
     int tune_prefetch = 0;     // autotuner: rows per fill pass for every instance (0: the instances' own)
     int tune_rows_per_block = 500;   // autotuner: positions per block a solve aims at (caps its blocks)
@@ -148,6 +149,13 @@ void count_launch(long long n = 1);
 void count_transfer(long long h2d, long long d2h);
 // CUDA graphs of repeated waves in solve_batch (on by default)
 void set_graphs(int on);
+// bound of every cross-block wait of later launches, in ms (0: the default 30 s)
+void set_wait_limit_ms(long long ms);
+// Test hook, one shot: the next launch leaves out its last thread block, so
+// the group of the launch's last instance never completes an exchange; its
+// waits run out after the wait bound, the group returns with an error and
+// the call reports it.  The instance must have two or more blocks.
+void arm_drop_block();
 // deepest ring of transpose tiles per warp the CUDA-core fills may use (1 to
 // kMaxTileBufs, default 2: deeper rings measured no faster on B200, the rows
 // being L2-resident); a launch takes the deepest that still fits its

@@ -185,11 +185,15 @@ void Server::reap(Slot &slot)
     const std::string err = rc ? std::string(last_error()) : std::string();
     cudaFreeAsync(slot.dev, slot.stream);
     slot.dev = nullptr;
+    // each request by its own outcome: one instance whose group timed out
+    // fails alone; a launch that failed leaves every result unfilled
+    std::vector<char> ok(slot.jobs.size(), 0);
     for (size_t k = 0; k < slot.jobs.size(); k++) {
         Job *j = slot.jobs[k];
         if (slot.delivered[k]) continue;
         j->rows->release_async(slot.stream);
-        if (rc == 0) {
+        ok[k] = res[k].alpha.size() == j->sub.rows.size() && res[k].out.status >= 0;
+        if (ok[k]) {
             j->alpha.assign(j->n, 0.0);
             capi::finish_instance(j->params, j->sub, res[k], j->y.data(), j->n, j->alpha.data(), &j->stats);
         }
@@ -198,7 +202,7 @@ void Server::reap(Slot &slot)
     for (size_t k = 0; k < slot.jobs.size(); k++) {
         if (slot.delivered[k]) continue;
         slot.jobs[k]->rows.reset();
-        complete_locked(slot.jobs[k], rc == 0, err);
+        complete_locked(slot.jobs[k], ok[k] != 0, ok[k] ? std::string() : (err.empty() ? "solve failed" : err));
     }
     mem_used -= slot.mem;
     blocks_used -= slot.blocks;

@@ -34,8 +34,9 @@
 // reference's operand order; the file is compiled with -fmad=false so that no
 // multiply-add is contracted.
 //
-// Every wait is bounded: a poll that exceeds kWaitTimeout cycles sets the
-// group's error flag and every block of the group returns.
+// Every wait is bounded: a poll that exceeds the instance's wait bound (30 s
+// unless the host sets another) sets the group's error flag and every block
+// of the group returns.
 //
 // The kernel template smo_persistent<FORM> is instantiated once per
 // arithmetic form, each in its own translation unit (smo_form_*.cu), so the
@@ -56,7 +57,7 @@ namespace {
 
 #define SVMB_INF __longlong_as_double(0x7ff0000000000000ULL)
 constexpr double kTau = 1e-12;                     // reference svm.cpp:42
-constexpr long long kWaitTimeout = 60000000000LL;  // ~30 s of SM clock
+constexpr long long kWaitTimeoutNs = 30000000000LL;  // default bound of a cross-block wait: 30 s
 // positions a thread takes at a time in the chunk scans that read Q rows from
 // global memory: their loads are issued together
 constexpr int kScanGroup = 8;
@@ -854,14 +855,15 @@ __device__ bool exchange(Ctx &c, Shared &sh)
         // barrier above, the whole block's before the record is seen
         if (threadIdx.x == 0) st_release_i32(&mine->seq, want);
         const Partial *all = c.D->partials + (long long)(c.phase & 1) * c.nb;
+        const long long limit = c.D->wait_ns > 0 ? c.D->wait_ns : kWaitTimeoutNs;
         for (int b = threadIdx.x; b < c.nb; b += blockDim.x) {
-            const long long t0 = clock64();
+            const long long t0 = (long long)tc::global_ns();
             long long spins = 0;
             // spin with relaxed loads; one acquire load of the awaited value
             // then synchronizes with the record's release store
             while (ld_relaxed_i32(&all[b].seq) != want) {
                 if ((++spins & 63) == 0) {
-                    if (ld_relaxed_i32(&c.D->sync->error) != 0 || clock64() - t0 > kWaitTimeout) {
+                    if (ld_relaxed_i32(&c.D->sync->error) != 0 || (long long)tc::global_ns() - t0 > limit) {
                         atomicExch(&c.D->sync->error, 1);
                         ok = 0;
                         break;

@@ -224,6 +224,12 @@ int api_set_option(const char *name, long long value)
         if (set_fill_depth((int)value) != 0) return -1;
     } else if (!strcmp(name, "predict_form")) {
         if (predict_set_form((int)value) != 0) return -1;
+    } else if (!strcmp(name, "wait_limit_ms")) {
+        if (value < 0) return -1;
+        set_wait_limit_ms(value);
+    } else if (!strcmp(name, "test_drop_block")) {
+        if (value != 1) return -1;
+        arm_drop_block();
     } else if (!strcmp(name, "prefetch")) {
         if (value < 0 || value > kPrefetchMax) return -1;
         g_opt.prefetch = (int)value;
