@@ -255,24 +255,36 @@ def cpu_baseline_sample(p, rows, ys, ours, budget_s=20.0):
 # ----------------------------------------------------------------------------
 def precision_form_extra(eng, ResidentRows, make_params):
     """Dense RBF training at n=100,000, d=784 (pixel-like rows, 70% zeros, C=10,
-    gamma=1/784, 4 GB Q-row cache): the tensor-core form (scaled fp16 split,
-    fp32 TMEM accumulation, fp64 G/alpha/step/rho) against the plain fp32
-    CUDA-core form (one row per cache miss, incremental G_bar) and the exact
-    form (bit-identical to the reference's float-Q solver).  Device seconds of
-    the solve launch."""
+    gamma=1/784, 4 GB Q-row cache): the tensor-core forms (scaled fp16 split,
+    bf16 split, tf32; fp32 TMEM accumulation, fp64 G/alpha/step/rho) against
+    the plain fp32 CUDA-core form (one row per cache miss, incremental G_bar)
+    and the exact form (bit-identical to the reference's float-Q solver).
+    Device seconds of the solve launch."""
     tr, te = datagen.dense_pixels(n=100000, n_test=20000)
     rows = ResidentRows(eng, tr, layout=1)
     idx = [np.arange(tr.n, dtype=np.int32)]
     y = [np.ascontiguousarray(tr.y, dtype=np.float64)]
     common = dict(svm_type=0, kernel_type=2, gamma=1.0 / 784, C_pos=10.0, cache_mb=4096.0)
     forms = {"fp16x3_tensor": make_params(form=3, **common),
+             "bf16x3_tensor": make_params(form=2, **common),
+             "tf32_tensor": make_params(form=4, **common),
              "fp32_plain": make_params(form=1, prefetch=1, gbar_mode=1, **common),
              "exact": make_params(form=0, **common)}
     out = {}
     for name, prm in forms.items():
         _, st = rows.solve_many(idx, y, [prm])
         s = st[0]
-        out[name] = {"seconds": s["seconds"], "iters": s["iters"], "obj": s["obj"], "rho": s["rho"], "nr_sv": s["nr_sv"]}
+        prof = s["prof_cycles"]
+        tot = max(prof[7], 1)
+        out[name] = {"seconds": s["seconds"], "iters": s["iters"], "obj": s["obj"], "rho": s["rho"], "nr_sv": s["nr_sv"],
+                     "us_per_iter": s["seconds"] / max(s["iters"], 1) * 1e6,
+                     "fill_passes": s["fills"], "fill_passes_per_iter": s["fills"] / max(s["iters"], 1),
+                     "prefetched": s["prefetched"], "prefetch_used": s["prefetch_used"],
+                     "cache_hit_rate": s["hits"] / max(s["lookups"], 1),
+                     "target_gb_read": s["fill_targets"] * 784 * 4 / 1e9,
+                     # block 0's SM cycles per loop section, as shares of its total
+                     "section_share": {k: prof[q] / tot for q, k in enumerate(
+                         ["a_reduce", "a_fill", "a_scan", "b_reduce", "b_fill", "b_update", "shrink"])}}
     rows.free()
     ex = out["exact"]
     for name in out:
@@ -284,6 +296,7 @@ def precision_form_extra(eng, ResidentRows, make_params):
             "forms": out,
             "decision_values": predict,
             "tensor_speedup_vs_fp32_plain": out["fp32_plain"]["seconds"] / out["fp16x3_tensor"]["seconds"],
+            "speedup_vs_fp32_plain": {k: out["fp32_plain"]["seconds"] / v["seconds"] for k, v in out.items()},
             "tensor_speedup_vs_exact": out["exact"]["seconds"] / out["fp16x3_tensor"]["seconds"],
             "precision_bar": "obj within 1e-6 and rho within 1e-4 of the FP64 oracle: tests/test_gpu_tensor_form.py"}
 

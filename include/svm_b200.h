@@ -91,6 +91,8 @@ typedef struct svmb_params {
                                the split copy holds every row densely */
 #define SVMB_FORM_FP16X3 3  /* tensor cores: each row scaled by a power of two and split x*2^e = hi + lo
                                (fp16), same three products in fp32 (about 22 significant bits) */
+#define SVMB_FORM_TF32   4  /* tensor cores: features rounded to tf32, one product per pair
+                               (kind::tf32, about 11 significant bits), fp32 accumulation */
 
 const char *svmb_last_error(void);
 /* Number of device kernels this library has launched in this process. */
@@ -105,7 +107,7 @@ int svmb_device_available(void);                /* 1 if a CUDA device can be use
 void svmb_print_nothing(const char *s);
 
 /* Process-wide engine options used by svm_train / svm_cross_validation:
- *   "form"   SVMB_FORM_EXACT (default), SVMB_FORM_FP32, SVMB_FORM_BF16X3 or SVMB_FORM_FP16X3
+ *   "form"   SVMB_FORM_EXACT (default), SVMB_FORM_FP32, SVMB_FORM_BF16X3, SVMB_FORM_FP16X3 or SVMB_FORM_TF32
  *   "blocks" thread blocks per solve (0 = automatic)
  *   "layout" -1 automatic, 0 CSR, 1 dense device layout of the rows
  *   "prefetch" kernel rows per cache-miss pass (1 = none, 0 = automatic)

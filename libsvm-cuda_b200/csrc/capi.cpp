@@ -43,8 +43,7 @@ int check_params(const svmb_params *p)
         return -1;
     }
     if (p->svm_type == EPSILON_SVR && p->p < 0) { svmb::set_error("p < 0"); return -1; }
-    if (p->form != SVMB_FORM_EXACT && p->form != SVMB_FORM_FP32 && p->form != SVMB_FORM_BF16X3 &&
-        p->form != SVMB_FORM_FP16X3) { svmb::set_error("unknown form"); return -1; }
+    if (p->form < SVMB_FORM_EXACT || p->form > SVMB_FORM_TF32) { svmb::set_error("unknown form"); return -1; }
     if (p->gbar_mode < SVMB_GBAR_AUTO || p->gbar_mode > SVMB_GBAR_RECOMPUTE) { svmb::set_error("unknown gbar_mode"); return -1; }
     return 0;
 }
@@ -237,7 +236,7 @@ int svmb_rows_kernel_block(const svmb_rows *rows, const svmb_params *params, int
         return -1;
     }
     if (params->kernel_type < LINEAR || params->kernel_type > SIGMOID) { svmb::set_error("kernel_type must be LINEAR, POLY, RBF or SIGMOID"); return -1; }
-    if (params->form < SVMB_FORM_EXACT || params->form > SVMB_FORM_FP16X3) { svmb::set_error("unknown form"); return -1; }
+    if (params->form < SVMB_FORM_EXACT || params->form > SVMB_FORM_TF32) { svmb::set_error("unknown form"); return -1; }
     const int n = rows->dev.n;
     for (int i = 0; i < ma; i++)
         if (ia[i] < 0 || ia[i] >= n) { svmb::set_error("row index out of range"); return -1; }

@@ -52,7 +52,7 @@ constexpr int kMaxTileBufs = 4;
 constexpr int kHashSlots = 1024;
 SVMB_HD constexpr int hash_bytes(int form) { return kHashSlots * 4 + kHashSlots * kSrcBatch * (form == 0 ? 8 : 4); }
 SVMB_HD constexpr int tile_aux_bytes(int bufs) { return ((bufs * kTileBytes > kCandBytes ? bufs * kTileBytes : kCandBytes) + 15) / 16 * 16; }
-SVMB_HD constexpr int aux_bytes(int form, int tile_bufs) { return (form == 2 || form == 3) ? kAuxBytesTc : tile_aux_bytes(tile_bufs); }
+SVMB_HD constexpr int aux_bytes(int form, int tile_bufs) { return (form == 2 || form == 3 || form == 4) ? kAuxBytesTc : tile_aux_bytes(tile_bufs); }
 
 // tensor-core (FORM_BF16X3) block products inside the solver
 constexpr int kTcM = 128;               // targets per tile (MMA M); rows are TMEM lanes
@@ -71,10 +71,12 @@ enum RowForm : int {
     FORM_FP32 = 1,    // fp32 X, fp32 accumulation (the plain CUDA-core form)
     FORM_BF16X3 = 2,  // tensor cores: x = hi + lo in bf16, dot = hi.hi + hi.lo + lo.hi, fp32 accumulation
     FORM_FP16X3 = 3,  // tensor cores: x*2^e = hi + lo in fp16 (power-of-2 scale per row), same three products
+    FORM_TF32 = 4,    // tensor cores: x rounded to tf32 (10-bit mantissa), one product, fp32 accumulation
 };
-constexpr int kNumForms = 4;
-SVMB_HD constexpr bool is_tc_form(int f) { return f == FORM_BF16X3 || f == FORM_FP16X3; }
-constexpr int kSplitChunk = 64;         // bf16 features per K-chunk of the split rows (hi 64 then lo 64)
+constexpr int kNumForms = 5;
+SVMB_HD constexpr bool is_tc_form(int f) { return f == FORM_BF16X3 || f == FORM_FP16X3 || f == FORM_TF32; }
+constexpr int kSplitChunk = 64;         // features per K-chunk of the split rows: hi 64 then lo 64 (16-bit
+                                        // values), or in FORM_TF32 the chunk's 64 tf32 values (the same 256 bytes)
 
 struct KernelParams {
     int type;         // LINEAR, POLY, RBF, SIGMOID

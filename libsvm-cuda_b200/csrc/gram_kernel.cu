@@ -14,7 +14,12 @@
 //   FORM_FP16X3  tensor cores, the same three products over an fp16 split of
 //                each row scaled by a power of two (max |x| 2^e in [2^14, 2^15)):
 //                x 2^e = hi + lo, about 2^-22 of each product; the dot is
-//                multiplied back by 2^-e_a 2^-e_b (exact).
+//                multiplied back by 2^-e_a 2^-e_b (exact);
+//   FORM_TF32    tensor cores, one product of the features rounded to tf32
+//                (10 explicit mantissa bits, about 2^-11 of each product),
+//                kind::tf32.  The tf32 copy has the same 256 bytes per
+//                64-feature chunk as the split copy: two 128-byte halves of
+//                32 features each, staged exactly like hi and lo.
 // The split copy is dense (CSR rows are scattered into it), d padded to a
 // multiple of 64.  RBF distances use the float64 row norms.
 // The kernel value itself is always formed in float64 from the dot product.
@@ -73,7 +78,7 @@ struct GramArgs {
 // (two, alternating); while the next chunk's MMAs run, the 8 warps add the
 // finished chunk into float64 registers (warp w: lanes 32(w%4).., columns
 // 32(w/4)..+31), so the tensor core's float32 accumulation spans 64 features.
-template <bool BF16>
+template <int SF>   // the split form: FORM_BF16X3, FORM_FP16X3 or FORM_TF32
 __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
 {
     extern __shared__ uint8_t g_smem_raw[];
@@ -126,7 +131,7 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
         }
     };
 
-    const uint32_t idesc = tc::idesc_f16_f32(kGM, kGN, BF16);
+    const uint32_t idesc = SF == FORM_TF32 ? tc::idesc_tf32_f32(kGM, kGN) : tc::idesc_f16_f32(kGM, kGN, SF == FORM_BF16X3);
     const int nk = a.nchunk;
     double acc[32];
 #pragma unroll
@@ -161,14 +166,23 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
             tc::tc_fence_after();
             const uint32_t sa = base + s * kGStageBytes;
             const uint32_t dst = tmem + (uint32_t)((kc & 1) * kGN);
+            if (SF == FORM_TF32) {
 #pragma unroll
-            for (int kk = 0; kk < 4; kk++) {
-                const uint64_t ahi = tc::sw128_desc(sa + kk * 32), alo = tc::sw128_desc(sa + kGTileA + kk * 32);
-                const uint64_t bhi = tc::sw128_desc(sa + 2 * kGTileA + kk * 32);
-                const uint64_t blo = tc::sw128_desc(sa + 2 * kGTileA + kGTileB + kk * 32);
-                tc::mma_bf16(dst, ahi, blo, idesc, kk > 0);
-                tc::mma_bf16(dst, alo, bhi, idesc, true);
-                tc::mma_bf16(dst, ahi, bhi, idesc, true);
+                for (int h = 0; h < 2; h++)
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++)
+                        tc::mma_tf32(dst, tc::sw128_desc(sa + h * kGTileA + kk * 32),
+                                     tc::sw128_desc(sa + 2 * kGTileA + h * kGTileB + kk * 32), idesc, h > 0 || kk > 0);
+            } else {
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) {
+                    const uint64_t ahi = tc::sw128_desc(sa + kk * 32), alo = tc::sw128_desc(sa + kGTileA + kk * 32);
+                    const uint64_t bhi = tc::sw128_desc(sa + 2 * kGTileA + kk * 32);
+                    const uint64_t blo = tc::sw128_desc(sa + 2 * kGTileA + kGTileB + kk * 32);
+                    tc::mma_bf16(dst, ahi, blo, idesc, kk > 0);
+                    tc::mma_bf16(dst, alo, bhi, idesc, true);
+                    tc::mma_bf16(dst, ahi, bhi, idesc, true);
+                }
             }
             tc::mma_commit(&bars[s]);
         }
@@ -271,6 +285,42 @@ __global__ void row_scale_kernel(DevX x, int n, double *__restrict__ xinv)
     }
 }
 
+// feature k of a row in the tf32 copy: the chunk's 64 values as 32-bit words,
+// rounded to tf32 (nearest, ties away: cvt.rna.tf32.f32)
+__device__ __forceinline__ void tf32_store(float v, uint16_t *row, int k)
+{
+    uint32_t t;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(v));
+    reinterpret_cast<uint32_t *>(row)[(k / kSplitChunk) * kSplitChunk + (k % kSplitChunk)] = t;
+}
+
+__global__ void tf32_dense_kernel(const float *__restrict__ X, int n, int ld, int d, int nchunk, uint16_t *__restrict__ Xs)
+{
+    const long long rs = (long long)nchunk * 2 * kSplitChunk;
+    const long long total = (long long)n * d;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long r = idx / d;
+        const int k = (int)(idx - r * d);
+        tf32_store(X[r * ld + k], Xs + r * rs, k);
+    }
+}
+
+__global__ void tf32_csr_kernel(const long long *__restrict__ rowptr, const int *__restrict__ col,
+                                const float *__restrict__ val, int n, int nchunk, uint16_t *__restrict__ Xs)
+{
+    const long long nnz = rowptr[n];
+    const long long rs = (long long)nchunk * 2 * kSplitChunk;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+        int a = 0, b = n;
+        while (b - a > 1) {
+            const int m = (a + b) >> 1;
+            if (rowptr[m] <= e) a = m; else b = m;
+        }
+        tf32_store(val[e], Xs + a * rs, col[e]);
+    }
+}
+
 template <bool BF16>
 __device__ __forceinline__ void split_store(float v, float s, uint16_t *dst)
 {
@@ -324,6 +374,20 @@ __global__ void split_csr_kernel(const long long *__restrict__ rowptr, const int
     }
 }
 
+const void *gram_fn(int form)
+{
+    if (form == FORM_BF16X3) return (const void *)gram_split_kernel<FORM_BF16X3>;
+    if (form == FORM_TF32) return (const void *)gram_split_kernel<FORM_TF32>;
+    return (const void *)gram_split_kernel<FORM_FP16X3>;
+}
+
+void launch_gram(int form, dim3 grid, const GramArgs &a, cudaStream_t s)
+{
+    if (form == FORM_BF16X3) gram_split_kernel<FORM_BF16X3><<<grid, kGThreads, kGSmem, s>>>(a);
+    else if (form == FORM_TF32) gram_split_kernel<FORM_TF32><<<grid, kGThreads, kGSmem, s>>>(a);
+    else gram_split_kernel<FORM_FP16X3><<<grid, kGThreads, kGSmem, s>>>(a);
+}
+
 }  // namespace
 
 cudaError_t launch_split(const DeviceRows &rows, int form, int nchunk, uint16_t *Xs, double *xinv, cudaStream_t s)
@@ -332,6 +396,18 @@ cudaError_t launch_split(const DeviceRows &rows, int form, int nchunk, uint16_t 
     if (n <= 0) return cudaSuccess;
     const bool bf16 = form == FORM_BF16X3;
     const DevX x = rows.view(FORM_EXACT);
+    if (form == FORM_TF32) {
+        if (rows.dense) {
+            const long long total = (long long)n * rows.d;
+            const int blocks = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32));
+            tf32_dense_kernel<<<blocks, 256, 0, s>>>(rows.X, n, rows.ld, rows.d, nchunk, Xs);
+        } else {
+            const int blocks = (int)std::max<long long>(1, std::min<long long>((rows.nnz + 255) / 256, 148LL * 32));
+            tf32_csr_kernel<<<blocks, 256, 0, s>>>(rows.rowptr, rows.col, rows.val, n, nchunk, Xs);
+        }
+        count_launch();
+        return cudaGetLastError();
+    }
     if (!bf16) {
         row_scale_kernel<<<(int)std::min<long long>(((long long)n * 32 + 255) / 256, 148LL * 32), 256, 0, s>>>(x, n, xinv);
         count_launch();
@@ -355,8 +431,7 @@ cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, 
 {
     if (ma <= 0 || nb <= 0) return cudaSuccess;
     if (is_tc_form(form)) {
-        const bool bf16 = form == FORM_BF16X3;
-        const void *fn = bf16 ? (const void *)gram_split_kernel<true> : (const void *)gram_split_kernel<false>;
+        const void *fn = gram_fn(form);
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem);
         if (e != cudaSuccess) return e;
         GramArgs a;
@@ -374,8 +449,7 @@ cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, 
         a.trans = 0;
         a.err = d_err;
         dim3 grid((nb + kGN - 1) / kGN, (ma + kGM - 1) / kGM);
-        if (bf16) gram_split_kernel<true><<<grid, kGThreads, kGSmem, s>>>(a);
-        else gram_split_kernel<false><<<grid, kGThreads, kGSmem, s>>>(a);
+        launch_gram(form, grid, a, s);
     } else {
         dim3 grid((nb + 15) / 16, (ma + 15) / 16), block(16, 16);
         if (form == FORM_EXACT)
@@ -393,8 +467,7 @@ cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const
     if (ma <= 0 || nb <= 0) return cudaSuccess;
     if (!is_tc_form(form) || A.split_form != form || B.split_form != form || A.nchunk != B.nchunk)
         return cudaErrorInvalidValue;
-    const bool bf16 = form == FORM_BF16X3;
-    const void *fn = bf16 ? (const void *)gram_split_kernel<true> : (const void *)gram_split_kernel<false>;
+    const void *fn = gram_fn(form);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem);
     if (e != cudaSuccess) return e;
     GramArgs a;
@@ -412,8 +485,7 @@ cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const
     a.trans = 1;
     a.err = d_err;
     dim3 grid((nb + kGN - 1) / kGN, (ma + kGM - 1) / kGM);
-    if (bf16) gram_split_kernel<true><<<grid, kGThreads, kGSmem, s>>>(a);
-    else gram_split_kernel<false><<<grid, kGThreads, kGSmem, s>>>(a);
+    launch_gram(form, grid, a, s);
     count_launch();
     return cudaGetLastError();
 }

@@ -405,7 +405,7 @@ int svmb_server_create(const svmb_server_config *cfg, svmb_server **out)
     std::unique_ptr<svmb_server> h(new svmb_server());
     Server &S = h->s;
     if (cfg) S.cfg = *cfg;
-    if (S.cfg.form < SVMB_FORM_EXACT || S.cfg.form > SVMB_FORM_FP16X3) { svmb::set_error("unknown form"); return -1; }
+    if (S.cfg.form < SVMB_FORM_EXACT || S.cfg.form > SVMB_FORM_TF32) { svmb::set_error("unknown form"); return -1; }
     cudaGetDevice(&S.device);
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);

@@ -12,6 +12,7 @@ const void *smo_entry_exact();
 const void *smo_entry_fp32();
 const void *smo_entry_bf16x3();
 const void *smo_entry_fp16x3();
+const void *smo_entry_tf32();
 
 // ---------------------------------------------------------------------------
 // setup kernels
@@ -84,6 +85,7 @@ static const void *smo_fn(int form)
     if (form == FORM_EXACT) return smo_entry_exact();
     if (form == FORM_FP32) return smo_entry_fp32();
     if (form == FORM_BF16X3) return smo_entry_bf16x3();
+    if (form == FORM_TF32) return smo_entry_tf32();
     return smo_entry_fp16x3();
 }
 

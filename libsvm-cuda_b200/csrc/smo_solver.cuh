@@ -1040,7 +1040,7 @@ __device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool glob
     const int total = ntiles * NK;
     if (total <= 0 || ns <= 0) return true;
     const int N = (ns + 15) & ~15;                      // MMA N for M = 128: multiple of 16
-    const uint32_t idesc = tc::idesc_f16_f32(kTcM, N, D.form == FORM_BF16X3);
+    const uint32_t idesc = D.form == FORM_TF32 ? tc::idesc_tf32_f32(kTcM, N) : tc::idesc_f16_f32(kTcM, N, D.form == FORM_BF16X3);
     const uint32_t sbytes = (uint32_t)tc_stage_bytes(D.tc_n);
     const uint32_t a_lo = kTcM * 128u;                  // target lo tile
     const uint32_t b_hi = 2u * kTcM * 128u;             // source hi tile
@@ -1113,13 +1113,23 @@ __device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool glob
             tc::tc_fence_after();
             const uint32_t sa = c.tcbase + (uint32_t)(G % kTcStages) * sbytes;
             const uint32_t dst = sh.tmem + (uint32_t)((G & 1) * kTcMaxN);
+            if (D.form == FORM_TF32) {
+                // the two 128-byte halves hold features 0..31 and 32..63 of the chunk
 #pragma unroll
-            for (int kk = 0; kk < 4; kk++) {
-                const uint64_t ah = tc::sw128_desc(sa + kk * 32), al = tc::sw128_desc(sa + a_lo + kk * 32);
-                const uint64_t bh = tc::sw128_desc(sa + b_hi + kk * 32), bl = tc::sw128_desc(sa + b_lo + kk * 32);
-                tc::mma_bf16(dst, ah, bl, idesc, kk > 0);
-                tc::mma_bf16(dst, al, bh, idesc, true);
-                tc::mma_bf16(dst, ah, bh, idesc, true);
+                for (int h = 0; h < 2; h++)
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++)
+                        tc::mma_tf32(dst, tc::sw128_desc(sa + (h ? a_lo : 0u) + kk * 32),
+                                     tc::sw128_desc(sa + (h ? b_lo : b_hi) + kk * 32), idesc, h > 0 || kk > 0);
+            } else {
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) {
+                    const uint64_t ah = tc::sw128_desc(sa + kk * 32), al = tc::sw128_desc(sa + a_lo + kk * 32);
+                    const uint64_t bh = tc::sw128_desc(sa + b_hi + kk * 32), bl = tc::sw128_desc(sa + b_lo + kk * 32);
+                    tc::mma_bf16(dst, ah, bl, idesc, kk > 0);
+                    tc::mma_bf16(dst, al, bh, idesc, true);
+                    tc::mma_bf16(dst, ah, bh, idesc, true);
+                }
             }
             tc::mma_commit(&sh.tbar[G % kTcStages]);
         }

@@ -210,7 +210,7 @@ namespace svmb {
 int api_set_option(const char *name, long long value)
 {
     if (!strcmp(name, "form")) {
-        if (value != FORM_EXACT && value != FORM_FP32 && value != FORM_BF16X3 && value != FORM_FP16X3) return -1;
+        if (value < FORM_EXACT || value > FORM_TF32) return -1;
         g_opt.form = (int)value;
     } else if (!strcmp(name, "blocks")) {
         g_opt.blocks = (int)value;

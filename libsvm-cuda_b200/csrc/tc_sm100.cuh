@@ -137,6 +137,11 @@ __host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N, bool bf16)
            | ((uint32_t)(M >> 4) << 24);       // M / 16
 }
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) { return idesc_f16_f32(M, N, true); }
+// kind::tf32 instruction descriptor: A and B tf32 (format 2), f32 accumulator, both K-major
+__host__ __device__ constexpr uint32_t idesc_tf32_f32(int M, int N)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
 
 // D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, bool accumulate)
@@ -145,6 +150,17 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"((uint32_t)accumulate)
+        : "memory");
+}
+
+// the same with tf32 operands (K = 8 per instruction: 32 bytes of a 128-byte row, as for 16-bit types)
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, bool accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
         ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"((uint32_t)accumulate)
         : "memory");
 }

@@ -15,7 +15,7 @@ PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_DIR, "libsvm_b200.so")
 CLI_PATH = os.path.join(PKG_DIR, "svm-train")
 
-FORM_EXACT, FORM_FP32, FORM_BF16X3, FORM_FP16X3 = 0, 1, 2, 3
+FORM_EXACT, FORM_FP32, FORM_BF16X3, FORM_FP16X3, FORM_TF32 = 0, 1, 2, 3, 4
 
 
 class EngineError(RuntimeError):

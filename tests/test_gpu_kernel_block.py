@@ -7,12 +7,13 @@ Tolerances, per output, with S = sum_k |a_k b_k| and u = 2^-24:
   fp32    |d dot| <= d u S                     sequential float32 accumulation
   bf16x3  |d dot| <= (2^-14 + 2 d u) S         bf16 split products (~2^-16 each), float32 accumulation
   fp16x3  |d dot| <= (2^-19 + 2 d u) M         scaled fp16 split (~2^-22 of the row maxima), M = d max|a| max|b|
+  tf32    |d dot| <= (2^-10 + 2 d u) S         inputs rounded to tf32 (2^-11 each), float32 accumulation
 RBF values are held to |dK| <= K * gamma * 2 * (dot bound + norm bound)."""
 import numpy as np
 import pytest
 
 from svmb200 import datagen
-from svmb200.lib import FORM_BF16X3, FORM_EXACT, FORM_FP16X3, FORM_FP32, ResidentRows, make_params
+from svmb200.lib import FORM_BF16X3, FORM_EXACT, FORM_FP16X3, FORM_FP32, FORM_TF32, ResidentRows, make_params
 
 pytestmark = pytest.mark.gpu
 
@@ -41,7 +42,7 @@ def test_linear_block_forms(engine, n, d, ma, nb):
     want = A @ B.T
     S = np.abs(A) @ np.abs(B).T
     u = 2.0 ** -24
-    forms = (FORM_EXACT, FORM_FP32, FORM_BF16X3, FORM_FP16X3)
+    forms = (FORM_EXACT, FORM_FP32, FORM_BF16X3, FORM_FP16X3, FORM_TF32)
     got = {f: rows.kernel_block(ia, ib, make_params(kernel_type=0, form=f)) for f in forms}
     rel = {f: float((np.abs(got[f] - want) / S).max()) for f in got}
     M = d * np.abs(A).max(1)[:, None] * np.abs(B).max(1)[None, :]
@@ -49,8 +50,11 @@ def test_linear_block_forms(engine, n, d, ma, nb):
     assert np.all(np.abs(got[FORM_EXACT] - want) <= 1e-12 * (1 + np.abs(want))), rel
     assert np.all(np.abs(got[FORM_FP32] - want) <= d * u * S + 1e-30), rel
     assert np.all(np.abs(got[FORM_BF16X3] - want) <= (2.0 ** -14 + 2 * d * u) * S + 1e-30), rel
+    assert np.all(np.abs(got[FORM_TF32] - want) <= (2.0 ** -10 + 2 * d * u) * S + 1e-30), rel
     # the split form is far more accurate than a single bf16 product (2^-8)
     assert rel[FORM_BF16X3] < 2.0 ** -12, rel
+    # and a single tf32 product is less accurate than either split form
+    assert rel[FORM_TF32] > rel[FORM_BF16X3], rel
 
 
 def test_rbf_block_tensor_form(engine):
@@ -92,5 +96,7 @@ def test_tensor_form_on_csr_rows(engine):
     got16 = rows.kernel_block(ia, ib, make_params(kernel_type=0, form=FORM_FP16X3))
     M = 5000 * np.abs(X[ia]).max(1)[:, None] * np.abs(X[ib]).max(1)[None, :]
     assert np.all(np.abs(got16 - want) <= (2.0 ** -19 + 2 * 5000 * 2.0 ** -24) * M + 1e-30)
+    got32 = rows.kernel_block(ia, ib, make_params(kernel_type=0, form=FORM_TF32))
+    assert np.all(np.abs(got32 - want) <= (2.0 ** -10 + 2 * 5000 * 2.0 ** -24) * S + 1e-30)
     ex = rows.kernel_block(ia, ib, make_params(kernel_type=0, form=FORM_EXACT))
     assert np.all(np.abs(ex - want) <= 1e-12 * (1 + np.abs(want)))
