@@ -123,6 +123,8 @@ void svmb_print_nothing(const char *s);
  *   "predict_form" SVMB_FORM_EXACT (default: the reference's kernel values bit
  *            for bit) or a tensor-core form: svm_predict* and svmb_predict_batch
  *            then evaluate K(test rows, SVs) as block products on the tensor cores
+ *   "blocks_per_sm" 1 (default) to 4: solver blocks one SM may hold; each gets
+ *            that share of the SM's shared memory (speed only)
  *   "wait_limit_ms" bound of every wait of a solver block for the other blocks
  *            of its group (0 = the default, 30 s); a wait that runs out makes
  *            the whole group return and the call report an error

@@ -32,6 +32,15 @@ static std::atomic<long long> g_wait_ns{0};
 void set_wait_limit_ms(long long ms) { g_wait_ns = ms > 0 ? ms * 1000000LL : 0; }
 
 static std::atomic<int> g_drop_block{0};
+
+// solver blocks a launch may place on one SM (their shared memory is split)
+static int g_blocks_per_sm = 1;
+int set_blocks_per_sm(int b)
+{
+    if (b < 1 || b > 4) return -1;
+    g_blocks_per_sm = b;
+    return 0;
+}
 void arm_drop_block() { g_drop_block = 1; }
 
 
@@ -462,10 +471,14 @@ constexpr int kChunkBytes = 3 * 8 + 2 * 4 + 2;     // per position: G, alpha, QD
 // dynamic shared memory a solver block can use beside its static part
 long long smem_budget()
 {
-    int smem_total = 0, dev = 0;
+    int smem_total = 0, smem_sm = 0, dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&smem_total, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return -1;
-    return (long long)smem_total - smo_static_smem() - 1024;
+    if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) return -1;
+    // with several solver blocks per SM each gets its share of the SM's
+    // shared memory (less the 1 KB the runtime reserves per block)
+    const long long per_block = std::min<long long>(smem_total, smem_sm / g_blocks_per_sm - 1024);
+    return per_block - smo_static_smem() - 1024;
 }
 
 // shared-memory staging of one instance's rows: source rows staged in

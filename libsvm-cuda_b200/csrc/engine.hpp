@@ -156,6 +156,10 @@ void set_wait_limit_ms(long long ms);
 // waits run out after the wait bound, the group returns with an error and
 // the call reports it.  The instance must have two or more blocks.
 void arm_drop_block();
+// solver blocks placed on one SM (1 to 4, default 1): the shared memory a
+// block may use is the SM's divided among them; a launch then holds up to
+// that many blocks per SM where registers allow it.  Speed only.
+int set_blocks_per_sm(int b);
 // deepest ring of transpose tiles per warp the CUDA-core fills may use (1 to
 // kMaxTileBufs, default 2: deeper rings measured no faster on B200, the rows
 // being L2-resident); a launch takes the deepest that still fits its

@@ -106,7 +106,8 @@ struct StageSlots {
     int *hkeys;
     void *hvals;
 };
-static_assert(kHashSlots / 2 <= kThreads, "one staged nonzero per thread");
+// staged nonzeros a thread handles at most (a pass holds up to kHashSlots / 2)
+constexpr int kHashPer = (kHashSlots / 2 + kThreads - 1) / kThreads;
 
 __device__ __forceinline__ int hash_home(int col) { return (int)(((unsigned)col * 2654435761u) >> 22) & (kHashSlots - 1); }
 
@@ -169,8 +170,8 @@ __device__ void stage_sources(const InstanceDesc &D, float *stage, StageSlots &s
         }
     } else if (D.hash_slots > 0) {
         // wide sparse sources: every nonzero (column c of source k) goes to the
-        // slot of c in the table, one nonzero per thread; a slot shared by
-        // several sources holds each one's value, the others stay zero
+        // slot of c in the table; a slot shared by several sources holds each
+        // one's value, the others stay zero
         if (threadIdx.x == 0) {
             int tot = 0;
             ss.hoff[0] = 0;
@@ -184,8 +185,7 @@ __device__ void stage_sources(const InstanceDesc &D, float *stage, StageSlots &s
             ss.dbl = D.form == FORM_EXACT ? 1 : 0;
         }
         __syncthreads();
-        const int t = threadIdx.x;
-        if (ss.hash && t < ss.hoff[ns]) {
+        for (int t = threadIdx.x; ss.hash && t < ss.hoff[ns]; t += blockDim.x) {
             const int k = hash_owner(ss, t);
             const long long e = x.rowptr[rows[k]] + (t - ss.hoff[k]);
             const int col = x.col[e];
@@ -225,17 +225,24 @@ __device__ void unstage_sources(const InstanceDesc &D, float *stage, StageSlots 
         // every slot this pass filled goes back to empty with zero values: the
         // slots are found first and cleared after a barrier, so that no
         // lookup meets a chain with a hole
-        const int t = threadIdx.x;
-        int h = -1, k = 0;
-        if (ss.hash && t < ss.hoff[ss.ns]) {
-            k = hash_owner(ss, t);
-            h = hash_find(ss.hkeys, x.col[x.rowptr[ss.rows[k]] + (t - ss.hoff[k])]);
+        int h[kHashPer], k[kHashPer];
+#pragma unroll
+        for (int u = 0; u < kHashPer; u++) {
+            const int t = threadIdx.x + u * (int)blockDim.x;
+            h[u] = -1;
+            k[u] = 0;
+            if (ss.hash && t < ss.hoff[ss.ns]) {
+                k[u] = hash_owner(ss, t);
+                h[u] = hash_find(ss.hkeys, x.col[x.rowptr[ss.rows[k[u]]] + (t - ss.hoff[k[u]])]);
+            }
         }
         __syncthreads();
-        if (h >= 0) {
-            ss.hkeys[h] = -1;
-            if (ss.dbl) reinterpret_cast<double *>(ss.hvals)[h * kSrcBatch + k] = 0.0;
-            else reinterpret_cast<float *>(ss.hvals)[h * kSrcBatch + k] = 0.0f;
+#pragma unroll
+        for (int u = 0; u < kHashPer; u++) {
+            if (h[u] < 0) continue;
+            ss.hkeys[h[u]] = -1;
+            if (ss.dbl) reinterpret_cast<double *>(ss.hvals)[h[u] * kSrcBatch + k[u]] = 0.0;
+            else reinterpret_cast<float *>(ss.hvals)[h[u] * kSrcBatch + k[u]] = 0.0f;
         }
     } else if (!x.X && D.stage_cap > 0) {
         for (int k = 0; k < ss.ns; k++) {

@@ -224,6 +224,8 @@ int api_set_option(const char *name, long long value)
         if (set_fill_depth((int)value) != 0) return -1;
     } else if (!strcmp(name, "predict_form")) {
         if (predict_set_form((int)value) != 0) return -1;
+    } else if (!strcmp(name, "blocks_per_sm")) {
+        if (set_blocks_per_sm((int)value) != 0) return -1;
     } else if (!strcmp(name, "wait_limit_ms")) {
         if (value < 0) return -1;
         set_wait_limit_ms(value);
