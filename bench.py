@@ -518,7 +518,9 @@ def profile_case(name):
     """One solver launch for an ncu capture (autotuner and graphs off, so that
     the launch is a plain kernel launch):
       ovo45_half     the one-vs-one workload at half size, exact form, 45 solves
-      pixels8k_fp16  dense pixel rows n=8000 d=784, one solve in the fp16x3 tensor form"""
+      pixels8k_fp16  dense pixel rows n=8000 d=784, one solve in the fp16x3 tensor form
+      gram_fp16x3    one kernel block K(4096 rows, 8192 rows) of dense pixel rows, d=784,
+                     in the fp16x3 tensor form (gram_split_kernel)"""
     from svmb200 import Engine
     from svmb200.lib import ResidentRows, make_params
     eng = Engine()
@@ -535,6 +537,18 @@ def profile_case(name):
         ys = [tr.y.astype(np.float64)]
         prm = [make_params(svm_type=0, kernel_type=2, gamma=1.0 / 784, C_pos=10.0, cache_mb=400.0, form=3)]
         res = ResidentRows(eng, tr, layout=1)
+    elif name == "gram_fp16x3":
+        tr, _ = datagen.dense_pixels(n=12288, n_test=0)
+        res = ResidentRows(eng, tr, layout=1)
+        ia = np.arange(4096, dtype=np.int32)
+        ib = np.arange(4096, 12288, dtype=np.int32)
+        prm = make_params(kernel_type=2, gamma=1.0 / 784, form=3)
+        res.kernel_block(ia[:128], ib[:64], prm)          # split copy made here, before the captured launch
+        t0 = time.perf_counter()
+        res.kernel_block(ia, ib, prm)
+        print(json.dumps({"profile_case": name, "block": [4096, 8192, 784],
+                          "host_ms": (time.perf_counter() - t0) * 1e3}), flush=True)
+        return 0
     else:
         raise SystemExit(f"unknown profile case {name}")
     _, st = res.solve_many(rows, ys, prm)

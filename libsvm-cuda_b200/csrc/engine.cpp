@@ -1138,18 +1138,41 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
     }
     const int capacity = per_sm * sms;
     clk.mark("setup");
-    // More instances than one launch holds: launch them largest first, so that
-    // each launch holds instances of similar size (a launch lasts as long as
-    // its longest solve, and its other SMs idle meanwhile).  Results do not
-    // depend on which instances share a launch.
+    // More instances than one launch holds: launch instances of the same
+    // parameters together (kernel, C: a grid point's solves take similar
+    // numbers of iterations, other points' may take ten times as many), and
+    // within those the largest first, so that each launch holds instances of
+    // similar length (a launch lasts as long as its longest solve, and its
+    // other SMs idle meanwhile).  Results do not depend on which instances
+    // share a launch.
     std::vector<SubProblem> sorted_subs;
     std::vector<int> order;
     const std::vector<SubProblem> *plan = &subs;
     if (ninst > capacity) {
         order.resize(ninst);
         for (int k = 0; k < ninst; k++) order[k] = k;
-        std::stable_sort(order.begin(), order.end(),
-                         [&](int a, int b) { return subs[a].rows.size() > subs[b].rows.size(); });
+        // group of an instance: index of the first instance with the same parameters
+        std::vector<int> group(ninst, 0);
+        {
+            std::vector<std::pair<std::array<double, 6>, int>> keys;
+            for (int k = 0; k < ninst; k++) {
+                const SolveParams &p = params_of(subs[k], prm);
+                const std::array<double, 6> key{(double)p.kp.type, (double)p.kp.degree, p.kp.gamma, p.kp.coef0,
+                                                subs[k].Cp, subs[k].Cn};
+                int g = -1;
+                for (const auto &e : keys)
+                    if (e.first == key) { g = e.second; break; }
+                if (g < 0) {
+                    g = (int)keys.size();
+                    keys.emplace_back(key, g);
+                }
+                group[k] = g;
+            }
+        }
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            if (group[a] != group[b]) return group[a] < group[b];
+            return subs[a].rows.size() > subs[b].rows.size();
+        });
         sorted_subs.reserve(ninst);
         for (int k : order) sorted_subs.push_back(subs[k]);
         plan = &sorted_subs;

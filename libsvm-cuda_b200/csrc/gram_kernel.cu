@@ -461,8 +461,8 @@ cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const KernelParams &kp, int form, int ma,
-                                 int nb, double *d_out_t, long long ldo, int *d_err, cudaStream_t s)
+cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const KernelParams &kp, int form, int a0,
+                                 int ma, int nb, double *d_out_t, long long ldo, int *d_err, cudaStream_t s)
 {
     if (ma <= 0 || nb <= 0) return cudaSuccess;
     if (!is_tc_form(form) || A.split_form != form || B.split_form != form || A.nchunk != B.nchunk)
@@ -471,13 +471,14 @@ cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem);
     if (e != cudaSuccess) return e;
     GramArgs a;
-    a.xs = A.Xs;
-    a.xinv = A.xinv;
-    a.nchunk = A.nchunk;
+    // rows a0 .. a0+ma of A: the row pointers, scales and norms start there
     a.rs = (long long)A.nchunk * 2 * kSplitChunk;
+    a.xs = A.Xs + (long long)a0 * a.rs;
+    a.xinv = A.xinv ? A.xinv + a0 : nullptr;
+    a.nchunk = A.nchunk;
     a.ia = nullptr; a.ma = ma; a.ib = nullptr; a.nb = nb;
     a.kp = kp;
-    a.xsq = A.xsq[FORM_EXACT];
+    a.xsq = A.xsq[FORM_EXACT] + a0;
     a.xs_b = B.Xs;
     a.xinv_b = B.xinv;
     a.xsq_b = B.xsq[FORM_EXACT];

@@ -5,20 +5,23 @@
 // (Kernel::k_function, svm.cpp:327-384: RBF walks the squared difference over
 // the union of nonzero features in index order, no norm trick).  Each pair's
 // sum runs sequentially over the two classes' SVs in model order, exactly as
-// the reference, so decision values match it bit for bit on float inputs.
+// the reference, so decision values match it bit for bit (rows and SVs are
+// kept as the doubles the caller's svm_node lists hold).
 // The file is compiled with -fmad=false.
 //
 // Kernel values are kept SV-major, kv[s][t] for the t-th test row of a chunk,
 // so that the pair sums (one thread per test row and pair, each walking the
 // SVs in model order) read consecutive words across a warp.  Dense rows take
 // a tiled kernel: a block computes 64 test rows x 64 SVs, 16 features at a
-// time staged as float64 in shared memory, 4 x 4 values per thread.  With a
+// time staged in shared memory, 4 x 4 values per thread.  With a
 // tensor-core predict form the values come from the split-product kernel
 // block of the SVs' split copy (kept with the model) and the chunk's.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -33,12 +36,14 @@ namespace svmb {
 namespace {
 
 struct Rows {
-    // dense [n][ld] or CSR; each array grows on demand and is reused by later
-    // uploads into the same Rows (capacities in bytes)
-    float *X = nullptr;
+    // dense [n][ld] or CSR, values in float64: a model's SVs (read from a
+    // model file, say) and the caller's rows are doubles, and the exact form
+    // evaluates the reference's kernel on exactly those values.  Each array
+    // grows on demand and is reused by later uploads (capacities in bytes)
+    double *X = nullptr;
     long long *rowptr = nullptr;
     int *col = nullptr;
-    float *val = nullptr;
+    double *val = nullptr;
     size_t capX = 0, capRp = 0, capCol = 0, capVal = 0;
     int n = 0, ld = 0;
     bool dense = true;
@@ -80,8 +85,8 @@ struct KP {
 };
 
 // kvalue for rows given as CSR in global memory (merge walks, svm.cpp:305-384)
-__device__ double kval_csr(const KP &kp, const long long *rpa, const int *ca, const float *va, int a,
-                           const long long *rpb, const int *cb, const float *vb, int b)
+__device__ double kval_csr(const KP &kp, const long long *rpa, const int *ca, const double *va, int a,
+                           const long long *rpb, const int *cb, const double *vb, int b)
 {
     long long e = rpa[a], ee = rpa[a + 1], f = rpb[b], ff = rpb[b + 1];
     double sum = 0.0;
@@ -89,24 +94,24 @@ __device__ double kval_csr(const KP &kp, const long long *rpa, const int *ca, co
         while (e < ee && f < ff) {
             const int x = ca[e], y = cb[f];
             if (x == y) {
-                const double d = __dsub_rn((double)va[e], (double)vb[f]);
+                const double d = __dsub_rn(va[e], vb[f]);
                 sum = __dadd_rn(sum, __dmul_rn(d, d));
                 ++e; ++f;
             } else if (x > y) {
-                sum = __dadd_rn(sum, __dmul_rn((double)vb[f], (double)vb[f]));
+                sum = __dadd_rn(sum, __dmul_rn(vb[f], vb[f]));
                 ++f;
             } else {
-                sum = __dadd_rn(sum, __dmul_rn((double)va[e], (double)va[e]));
+                sum = __dadd_rn(sum, __dmul_rn(va[e], va[e]));
                 ++e;
             }
         }
-        for (; e < ee; ++e) sum = __dadd_rn(sum, __dmul_rn((double)va[e], (double)va[e]));
-        for (; f < ff; ++f) sum = __dadd_rn(sum, __dmul_rn((double)vb[f], (double)vb[f]));
+        for (; e < ee; ++e) sum = __dadd_rn(sum, __dmul_rn(va[e], va[e]));
+        for (; f < ff; ++f) sum = __dadd_rn(sum, __dmul_rn(vb[f], vb[f]));
         return exp(__dmul_rn(-kp.gamma, sum));
     }
     while (e < ee && f < ff) {
         const int x = ca[e], y = cb[f];
-        if (x == y) { sum = __dadd_rn(sum, __dmul_rn((double)va[e], (double)vb[f])); ++e; ++f; }
+        if (x == y) { sum = __dadd_rn(sum, __dmul_rn(va[e], vb[f])); ++e; ++f; }
         else if (x > y) ++f;
         else ++e;
     }
@@ -131,8 +136,8 @@ __device__ __forceinline__ double kfinish(const KP &kp, double acc)
 // (ty, tx) of 16 x 16 owns test rows t0 + tx + 16i and SVs s0 + 4ty + j; every
 // value accumulates over the features in order, as the reference's walk does
 // (RBF: the squared difference; a feature zero in both adds nothing).
-__global__ void __launch_bounds__(256) kvalue_tile(KP kp, const float *__restrict__ T, int nt,
-                                                  const float *__restrict__ S, int ns, int ld,
+__global__ void __launch_bounds__(256) kvalue_tile(KP kp, const double *__restrict__ T, int nt,
+                                                  const double *__restrict__ S, int ns, int ld,
                                                   double *__restrict__ out)
 {
     __shared__ double ta[kPK][kPT + 1];
@@ -144,16 +149,24 @@ __global__ void __launch_bounds__(256) kvalue_tile(KP kp, const float *__restric
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-    // loader: 64 rows x 16 features = 256 float4 pieces per operand, one per thread
+    // loader: 64 rows x 16 features = 256 pieces of 4 doubles per operand, one per thread
     const int lr = tid >> 2, lc = (tid & 3) * 4;
     for (int k0 = 0; k0 < ld; k0 += kPK) {
         const int c = k0 + lc;
-        float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va;
-        if (t0 + lr < nt && c < ld) va = __ldg(reinterpret_cast<const float4 *>(T + (long long)(t0 + lr) * ld + c));
-        if (s0 + lr < ns && c < ld) vb = __ldg(reinterpret_cast<const float4 *>(S + (long long)(s0 + lr) * ld + c));
+        double2 a0 = make_double2(0.0, 0.0), a1 = a0, b0 = a0, b1 = a0;
+        if (t0 + lr < nt && c < ld) {
+            const double2 *p = reinterpret_cast<const double2 *>(T + (long long)(t0 + lr) * ld + c);
+            a0 = __ldg(p);
+            a1 = __ldg(p + 1);
+        }
+        if (s0 + lr < ns && c < ld) {
+            const double2 *p = reinterpret_cast<const double2 *>(S + (long long)(s0 + lr) * ld + c);
+            b0 = __ldg(p);
+            b1 = __ldg(p + 1);
+        }
         __syncthreads();
-        ta[lc][lr] = va.x; ta[lc + 1][lr] = va.y; ta[lc + 2][lr] = va.z; ta[lc + 3][lr] = va.w;
-        sb[lc][lr] = vb.x; sb[lc + 1][lr] = vb.y; sb[lc + 2][lr] = vb.z; sb[lc + 3][lr] = vb.w;
+        ta[lc][lr] = a0.x; ta[lc + 1][lr] = a0.y; ta[lc + 2][lr] = a1.x; ta[lc + 3][lr] = a1.y;
+        sb[lc][lr] = b0.x; sb[lc + 1][lr] = b0.y; sb[lc + 2][lr] = b1.x; sb[lc + 3][lr] = b1.y;
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < kPK; kk++) {
@@ -256,7 +269,8 @@ int g_predict_form = FORM_EXACT;
 // single-row svm_predict calls allocates nothing after its first call).
 struct Workspace {
     double *kv = nullptr, *dec = nullptr;
-    size_t cap_kv = 0, cap_dec = 0;
+    int *err = nullptr;
+    size_t cap_kv = 0, cap_dec = 0, cap_err = 0;
     Rows T;                     // test rows of the current chunk
 } g_ws;
 
@@ -276,33 +290,33 @@ int upload_nodes(const svm_node *const *x, int n, int d, int base, bool dense, R
     out.ld = (d + 3) & ~3;
     if (out.ld == 0) out.ld = 4;
     if (dense) {
-        std::vector<float> h((size_t)std::max(n, 1) * out.ld, 0.0f);
+        std::vector<double> h((size_t)std::max(n, 1) * out.ld, 0.0);
         for (int r = 0; r < n; r++)
             for (const svm_node *p = x[r]; p->index != -1; ++p) {
                 const int c = p->index - base;
-                if (c >= 0 && c < out.ld) h[(size_t)r * out.ld + c] = (float)p->value;
+                if (c >= 0 && c < out.ld) h[(size_t)r * out.ld + c] = p->value;
             }
-        PK(grow(out.X, out.capX, h.size() * sizeof(float)));
-        PK(xfer(out.X, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+        PK(grow(out.X, out.capX, h.size() * sizeof(double)));
+        PK(xfer(out.X, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
     } else {
         std::vector<long long> rp(n + 1, 0);
         std::vector<int> col;
-        std::vector<float> val;
+        std::vector<double> val;
         for (int r = 0; r < n; r++) {
             rp[r] = (long long)col.size();
             for (const svm_node *p = x[r]; p->index != -1; ++p) {
                 col.push_back(p->index - base);
-                val.push_back((float)p->value);
+                val.push_back(p->value);
             }
         }
         rp[n] = (long long)col.size();
         if (col.empty()) { col.push_back(0); val.push_back(0); }
         PK(grow(out.rowptr, out.capRp, rp.size() * sizeof(long long)));
         PK(grow(out.col, out.capCol, col.size() * sizeof(int)));
-        PK(grow(out.val, out.capVal, val.size() * sizeof(float)));
+        PK(grow(out.val, out.capVal, val.size() * sizeof(double)));
         PK(xfer(out.rowptr, rp.data(), rp.size() * sizeof(long long), cudaMemcpyHostToDevice));
         PK(xfer(out.col, col.data(), col.size() * sizeof(int), cudaMemcpyHostToDevice));
-        PK(xfer(out.val, val.data(), val.size() * sizeof(float), cudaMemcpyHostToDevice));
+        PK(xfer(out.val, val.data(), val.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
     return 0;
 }
@@ -376,39 +390,17 @@ int rows_to_device(const svm_node *const *x, int n, int d, int form, DeviceRows 
     return out.prepare_form(form, 0);
 }
 
-// Tensor-core kernel values kv[s][t] of a chunk of test rows: the SVs' split
-// copy is made once per model (and form, and width), the chunk's rows are
-// split here, and the block product K(test, SV) runs on the tensor cores;
-// RBF uses the float64 norms of both.
-int kvalue_tensor(const svm_model *m, Session *s, const svm_node *const *rows, int tn, int form, double *kv)
+// The SVs' split (or tf32) copy for tensor-core kernel values, made once per
+// model, form and width: both row sets of the block product need the same
+// split width, and test rows wider than the SVs widen it (their extra
+// features still count in the RBF norms).
+int prepare_tensor_svs(const svm_model *m, Session *s, int width, int form)
 {
-    int maxi = s->d - 1;
-    for (int r = 0; r < tn; r++)
-        for (const svm_node *p = rows[r]; p->index != -1; ++p) maxi = std::max(maxi, p->index);
-    // both row sets need the same split width; test rows wider than the SVs
-    // widen it (their extra features still count in the RBF norms)
-    const int width = maxi + 1;
-    if (!s->sv_tc || s->sv_tc->split_form != form || s->sv_tc->d < width) {
-        s->sv_tc.reset(new DeviceRows());
-        if (rows_to_device(m->SV, m->l, width, form, *s->sv_tc) != 0) {
-            s->sv_tc.reset();
-            return -1;
-        }
-    }
-    DeviceRows T;
-    if (rows_to_device(rows, tn, s->sv_tc->d, form, T) != 0) return -1;
-    int *d_err = nullptr;
-    PK(cudaMalloc(&d_err, sizeof(int)));
-    PK(cudaMemset(d_err, 0, sizeof(int)));
-    KernelParams kp{m->param.kernel_type, m->param.degree, m->param.gamma, m->param.coef0};
-    cudaError_t e = launch_kernel_block2(T, *s->sv_tc, kp, form, tn, m->l, kv, tn, d_err, 0);
-    int herr = 0;
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    if (e == cudaSuccess) e = xfer(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(d_err);
-    if (e != cudaSuccess || herr) {
-        set_error(e != cudaSuccess ? std::string("tensor-core kernel values: ") + cudaGetErrorString(e)
-                                   : std::string("tensor-core kernel values: a wait timed out"));
+    width = std::max(width, s->d);
+    if (s->sv_tc && s->sv_tc->split_form == form && s->sv_tc->d >= width) return 0;
+    s->sv_tc.reset(new DeviceRows());
+    if (rows_to_device(m->SV, m->l, width, form, *s->sv_tc) != 0) {
+        s->sv_tc.reset();
         return -1;
     }
     return 0;
@@ -454,35 +446,61 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
     KP kp{m->param.kernel_type, m->param.degree, m->param.gamma, m->param.coef0};
     std::vector<double> dec((size_t)n * std::max(npair, 1), 0.0);
     if (npair > 0 && m->l > 0) {
-        // chunk test rows so that the kvalue block stays below ~1 GB
+        // the test rows go to the device once; kernel values are made in
+        // chunks of rows whose value block stays below a quarter of the free
+        // device memory (at most 4 GB)
+        const bool trace = getenv("SVMB_TRACE") && *getenv("SVMB_TRACE") == '1';
+        const auto c0 = std::chrono::steady_clock::now();
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 1ull << 32;
         const long long per_row = (long long)m->l * 8;
-        const int chunk = (int)std::max<long long>(1, std::min<long long>(n, (1LL << 30) / per_row));
+        const long long budget = std::min<long long>(4LL << 30, std::max<long long>((long long)free_b / 4, 64LL << 20));
+        const int chunk = (int)std::max<long long>(1, std::min<long long>(n, budget / per_row));
         PK(grow(g_ws.kv, g_ws.cap_kv, (size_t)chunk * per_row));
         PK(grow(g_ws.dec, g_ws.cap_dec, (size_t)chunk * npair * 8));
         double *kv = g_ws.kv, *d_dec = g_ws.dec;
+        // test rows: features beyond the SVs' width cannot meet an SV feature in a
+        // dot product but still count in the RBF distance, so widen to cover them
+        int maxi = s->d - 1;
+        for (int r = 0; r < n; r++)
+            for (const svm_node *p = rows[r]; p->index != -1; ++p) maxi = std::max(maxi, p->index);
+        const bool wider = maxi + 1 > s->d;
+        const bool tensor = is_tc_form(g_predict_form);
+        const bool dense = !tensor && s->sv.dense && !wider;
         Rows &T = g_ws.T;
+        DeviceRows Ttc;
+        if (tensor) {
+            if (prepare_tensor_svs(m, s, maxi + 1, g_predict_form) != 0) return -1;
+            if (rows_to_device(rows, n, s->sv_tc->d, g_predict_form, Ttc) != 0) return -1;
+        } else if (dense) {
+            if (upload_nodes(rows, n, s->d, s->base, true, T) != 0) return -1;
+        } else {
+            if (s->sv.dense && !s->sv_csr.rowptr && upload_nodes(m->SV, m->l, s->d, s->base, false, s->sv_csr) != 0)
+                return -1;
+            if (upload_nodes(rows, n, maxi + 1, s->base, false, T) != 0) return -1;
+        }
+        int *d_err = nullptr;
+        if (tensor) {
+            PK(grow(g_ws.err, g_ws.cap_err, sizeof(int)));
+            d_err = g_ws.err;
+            PK(cudaMemset(d_err, 0, sizeof(int)));
+        }
+        const auto c1 = std::chrono::steady_clock::now();
+        KernelParams kpk{m->param.kernel_type, m->param.degree, m->param.gamma, m->param.coef0};
         for (int t0 = 0; t0 < n; t0 += chunk) {
             const int tn = std::min(chunk, n - t0);
-            // test rows: features beyond the SVs' width cannot meet an SV feature in a
-            // dot product but still count in the RBF distance, so widen to cover them
-            int maxi = s->d - 1;
-            for (int r = 0; r < tn; r++)
-                for (const svm_node *p = rows[t0 + r]; p->index != -1; ++p) maxi = std::max(maxi, p->index);
-            const bool wider = maxi + 1 > s->d;
-            if (is_tc_form(g_predict_form)) {
-                if (kvalue_tensor(m, s, rows + t0, tn, g_predict_form, kv) != 0) return -1;
-            } else if (s->sv.dense && !wider) {
-                if (upload_nodes(rows + t0, tn, s->d, s->base, true, T) != 0) return -1;
+            if (tensor) {
+                PK(launch_kernel_block2(Ttc, *s->sv_tc, kpk, g_predict_form, t0, tn, m->l, kv, tn, d_err, 0));
+            } else if (dense) {
                 dim3 grid((m->l + kPS - 1) / kPS, (tn + kPT - 1) / kPT);
-                kvalue_tile<<<grid, 256>>>(kp, T.X, tn, s->sv.X, m->l, s->sv.ld, kv);
+                kvalue_tile<<<grid, 256>>>(kp, T.X + (long long)t0 * T.ld, tn, s->sv.X, m->l, s->sv.ld, kv);
                 count_launch();
             } else {
-                if (s->sv.dense && !s->sv_csr.rowptr &&
-                    upload_nodes(m->SV, m->l, s->d, s->base, false, s->sv_csr) != 0)
-                    return -1;
                 const Rows &Sc = s->sv.dense ? s->sv_csr : s->sv;
-                if (upload_nodes(rows + t0, tn, maxi + 1, s->base, false, T) != 0) return -1;
-                kvalue_csr<<<(int)std::min<long long>(((long long)tn * m->l + 255) / 256, 148 * 16), 256>>>(kp, T, Sc, kv);
+                Rows Tc = T;               // a view of rows t0 .. t0+tn (row pointers stay absolute)
+                Tc.rowptr = T.rowptr + t0;
+                Tc.n = tn;
+                kvalue_csr<<<(int)std::min<long long>(((long long)tn * m->l + 255) / 256, 148 * 16), 256>>>(kp, Tc, Sc, kv);
                 count_launch();
             }
             pair_sums<<<std::min<long long>(((long long)tn * npair + 127) / 128, 148 * 8), 128>>>(kv, tn, m->l, k, s->start, s->nsv, s->coef, s->rho, d_dec);
@@ -493,6 +511,22 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
                 return -1;
             }
             PK(xfer(dec.data() + (size_t)t0 * npair, d_dec, (size_t)tn * npair * 8, cudaMemcpyDeviceToHost));
+        }
+        if (tensor) {
+            int herr = 0;
+            PK(xfer(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+            if (herr) {
+                set_error("tensor-core kernel values: a wait timed out");
+                return -1;
+            }
+        }
+        if (trace) {
+            const auto c2 = std::chrono::steady_clock::now();
+            auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+                return std::chrono::duration<double, std::milli>(b - a).count();
+            };
+            fprintf(stderr, "[svmb] predict rows=%d svs=%d chunks=%d rows_to_device=%.2fms values+sums=%.2fms\n", n,
+                    m->l, (n + chunk - 1) / chunk, ms(c0, c1), ms(c1, c2));
         }
     } else if (npair > 0) {
         for (int t = 0; t < n; t++)

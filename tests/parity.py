@@ -17,7 +17,8 @@ def compare_models(ours: dict, gold: dict, l: int) -> dict:
     b = coef_matrix(gold["sv_indices"], gold["sv_coef"], l)
     sv_a, sv_b = set(ours["sv_indices"].tolist()), set(gold["sv_indices"].tolist())
     return {
-        "same_classes": ours["nr_class"] == gold["nr_class"] and np.array_equal(ours["labels"], gold["labels"]),
+        "same_classes": ours["nr_class"] == gold["nr_class"] and (
+            np.array_equal(ours["labels"], gold["labels"]) if "labels" in gold else ours["labels"] is None),
         "sv_sym_diff": sorted(sv_a ^ sv_b),
         "max_coef_diff": float(np.max(np.abs(a - b))) if a.size else 0.0,
         "coef_bit_equal": bool(np.array_equal(a, b)),
