@@ -431,6 +431,59 @@ def decision_values_extra(eng, tr, te):
     return out
 
 
+def ovo45_tensor_extra(res, rows, ys, make_params):
+    """The headline one-vs-one step in the FP16X3 tensor form (the form that
+    meets the 1e-6 objective bar): device ms of the batched launch and of the
+    largest subproblem alone, after the autotuner settles."""
+    params = [make_params(svm_type=0, kernel_type=2, gamma=GAMMA, C_pos=CVAL, form=3) for _ in rows]
+    for _ in range(12):
+        _, st = res.solve_many(rows, ys, params)
+    ks = []
+    for _ in range(3):
+        _, st = res.solve_many(rows, ys, params)
+        ks.append(sum({s["launch"]: s["seconds"] for s in st}.values()))
+    big = int(np.argmax([len(r) for r in rows]))
+    alone = min(res.solve_many([rows[big]], [ys[big]], [params[big]])[1][0]["seconds"] for _ in range(3))
+    return {"form": "fp16x3", "batched_ms": min(ks) * 1e3, "largest_alone_ms": alone * 1e3,
+            "batched_over_largest": min(ks) / alone, "solves_per_s": len(rows) / min(ks)}
+
+
+def text_input_extra(eng):
+    """Parsing libsvm text: the sparse workload's 50,000 training rows
+    (d = 20,000, ~40 nonzeros) and the pixel workload's 100,000 rows (d = 784,
+    ~235 nonzeros), written to a temporary file, read by svmb_read_problem
+    (all host threads) and by the reference's own svm-train (its serial
+    read_problem; the run stops at the parameter check right after reading,
+    so the time is the read plus process start)."""
+    import ctypes
+    lib = eng.lib
+    lib.svmb_read_problem.argtypes = [C.c_char_p, C.POINTER(cabi.svm_problem), C.POINTER(C.POINTER(cabi.svm_node)),
+                                      C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+    lib.svmb_free_problem.argtypes = [C.POINTER(cabi.svm_problem), C.POINTER(cabi.svm_node)]
+    ref = os.path.join(ROOT, "oracle", "_ref", "svm-train")
+    out = {"threads": os.cpu_count()}
+    with tempfile.TemporaryDirectory() as td:
+        for name, make in (("sparse_50k", lambda: datagen.sparse_text(n=50000, n_test=0)[0]),
+                           ("pixels_100k", lambda: datagen.dense_pixels(n=100000, n_test=0)[0])):
+            path = os.path.join(td, name + ".txt")
+            datagen.write_libsvm(path, make())
+            prob = cabi.svm_problem()
+            space = C.POINTER(cabi.svm_node)()
+            maxi, bad = C.c_int(), C.c_longlong()
+            t0 = time.perf_counter()
+            rc = lib.svmb_read_problem(path.encode(), C.byref(prob), C.byref(space), C.byref(maxi), C.byref(bad))
+            ours = time.perf_counter() - t0
+            rec = {"mb": os.path.getsize(path) / 1e6, "rows": prob.l, "ours_s": ours, "rc": rc}
+            lib.svmb_free_problem(C.byref(prob), space)
+            if os.path.exists(ref):
+                t0 = time.perf_counter()
+                subprocess.run([ref, "-s", "1", "-n", "2", path, os.path.join(td, "m")], capture_output=True)
+                rec["reference_s"] = time.perf_counter() - t0
+                rec["speedup"] = rec["reference_s"] / ours
+            out[name] = rec
+    return out
+
+
 def cv_grid_extra(eng):
     """5-fold cross-validation over C in {0.5,1,2,4,8} x gamma in {1/256, 4/256}
     on the one-vs-one workload's 10 classes (its full size, 53,646 rows): every
@@ -713,7 +766,9 @@ def main():
         extras = {}
         if world == 1 and not args.no_extras:
             for name, fn in (("precision_form", lambda: precision_form_extra(eng, ResidentRows, make_params)),
+                             ("ovo45_fp16x3", lambda: ovo45_tensor_extra(res, rows, ys, make_params)),
                              ("dense_c1", lambda: dense_c1_extra(eng)),
+                             ("text_input", lambda: text_input_extra(eng)),
                              ("sparse_c2", lambda: sparse_c2_extra(eng, ResidentRows, make_params)),
                              ("cv_grid", lambda: cv_grid_extra(eng)),
                              ("serving", lambda: serving_extra(eng, make_params))):
