@@ -572,6 +572,8 @@ def profile_case(name):
     the launch is a plain kernel launch):
       ovo45_half     the one-vs-one workload at half size, exact form, 45 solves
       pixels8k_fp16  dense pixel rows n=8000 d=784, one solve in the fp16x3 tensor form
+      sparse_table   sparse rows n=4000 over d=20000 (~40 nonzeros), one exact-form RBF solve on
+                     the column-keyed table path
       gram_fp16x3    one kernel block K(4096 rows, 8192 rows) of dense pixel rows, d=784,
                      in the fp16x3 tensor form (gram_split_kernel)"""
     from svmb200 import Engine
@@ -590,6 +592,12 @@ def profile_case(name):
         ys = [tr.y.astype(np.float64)]
         prm = [make_params(svm_type=0, kernel_type=2, gamma=1.0 / 784, C_pos=10.0, cache_mb=400.0, form=3)]
         res = ResidentRows(eng, tr, layout=1)
+    elif name == "sparse_table":
+        tr, _ = datagen.sparse_text(n=4000, n_test=0)
+        rows = [np.arange(tr.n, dtype=np.int32)]
+        ys = [tr.y.astype(np.float64)]
+        prm = [make_params(svm_type=0, kernel_type=2, gamma=0.5, C_pos=4.0)]
+        res = ResidentRows(eng, tr)
     elif name == "gram_fp16x3":
         tr, _ = datagen.dense_pixels(n=12288, n_test=0)
         res = ResidentRows(eng, tr, layout=1)

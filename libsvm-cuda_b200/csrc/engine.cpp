@@ -1154,23 +1154,21 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
     if (ninst > capacity) {
         order.resize(ninst);
         for (int k = 0; k < ninst; k++) order[k] = k;
-        // group of an instance: index of the first instance with the same parameters
+        // group of an instance: the rank of its parameters in numeric order
+        // (kernel, gamma, ..., C), so that neighbouring groups -- which share
+        // a launch at their boundary -- are alike too
         std::vector<int> group(ninst, 0);
         {
-            std::vector<std::pair<std::array<double, 6>, int>> keys;
+            std::vector<std::array<double, 6>> key(ninst);
             for (int k = 0; k < ninst; k++) {
                 const SolveParams &p = params_of(subs[k], prm);
-                const std::array<double, 6> key{(double)p.kp.type, (double)p.kp.degree, p.kp.gamma, p.kp.coef0,
-                                                subs[k].Cp, subs[k].Cn};
-                int g = -1;
-                for (const auto &e : keys)
-                    if (e.first == key) { g = e.second; break; }
-                if (g < 0) {
-                    g = (int)keys.size();
-                    keys.emplace_back(key, g);
-                }
-                group[k] = g;
+                key[k] = {(double)p.kp.type, (double)p.kp.degree, p.kp.gamma, p.kp.coef0, subs[k].Cp, subs[k].Cn};
             }
+            std::vector<std::array<double, 6>> uniq(key);
+            std::sort(uniq.begin(), uniq.end());
+            uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+            for (int k = 0; k < ninst; k++)
+                group[k] = (int)(std::lower_bound(uniq.begin(), uniq.end(), key[k]) - uniq.begin());
         }
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
             if (group[a] != group[b]) return group[a] < group[b];

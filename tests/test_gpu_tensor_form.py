@@ -78,7 +78,11 @@ def test_tensor_form_against_fp64_oracle(engine, name):
     if te is not None and te.n:
         lab, _ = engine.predict(model, te)
         if prm.svm_type in (3, 4):
-            np.testing.assert_allclose(lab, gold64["pred"], rtol=0, atol=1e-4)
+            # regression values: the reference's own float-Q and double-Q
+            # builds differ by up to ~1e-3 here; hold the tensor form to twice
+            # that spread (at least 1e-4)
+            spread = float(np.max(np.abs(gold["pred"] - gold64["pred"])))
+            np.testing.assert_allclose(lab, gold64["pred"], rtol=0, atol=max(1e-4, 2 * spread))
         else:
             assert np.array_equal(lab, gold64["pred"])
     model.free()
