@@ -182,9 +182,10 @@ cudaError_t launch_split(const DeviceRows &rows, int form, int nchunk, uint16_t 
 cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, int form, const int *d_ia, int ma,
                                 const int *d_ib, int nb, double *d_out, long long ldo, int *d_err, cudaStream_t s);
 // K(A rows a0 .. a0+ma, B rows 0 .. nb) of two row sets in the same tensor
-// form (equal split widths), written transposed: out[j * ldo + i] = K(a_{a0+i}, b_j)
+// form (equal split widths): out[i * ldo + j] = K(a_{a0+i}, b_j), or with
+// `trans` out[j * ldo + i]
 cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const KernelParams &kp, int form, int a0,
-                                 int ma, int nb, double *d_out_t, long long ldo, int *d_err, cudaStream_t s);
+                                 int ma, int nb, double *d_out, long long ldo, int trans, int *d_err, cudaStream_t s);
 cudaError_t launch_smo(int form, const InstanceDesc *d_insts, const int *d_block_inst, int nblocks,
                        size_t dyn_smem, bool cooperative, cudaStream_t s);
 cudaError_t smo_max_blocks(int form, size_t dyn_smem, int *blocks_per_sm);

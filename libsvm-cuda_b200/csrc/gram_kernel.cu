@@ -462,7 +462,7 @@ cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, 
 }
 
 cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const KernelParams &kp, int form, int a0,
-                                 int ma, int nb, double *d_out_t, long long ldo, int *d_err, cudaStream_t s)
+                                 int ma, int nb, double *d_out, long long ldo, int trans, int *d_err, cudaStream_t s)
 {
     if (ma <= 0 || nb <= 0) return cudaSuccess;
     if (!is_tc_form(form) || A.split_form != form || B.split_form != form || A.nchunk != B.nchunk)
@@ -482,8 +482,8 @@ cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const
     a.xs_b = B.Xs;
     a.xinv_b = B.xinv;
     a.xsq_b = B.xsq[FORM_EXACT];
-    a.out = d_out_t; a.ldo = ldo;
-    a.trans = 1;
+    a.out = d_out; a.ldo = ldo;
+    a.trans = trans;
     a.err = d_err;
     dim3 grid((nb + kGN - 1) / kGN, (ma + kGM - 1) / kGM);
     launch_gram(form, grid, a, s);

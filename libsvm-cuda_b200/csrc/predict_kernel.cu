@@ -237,6 +237,35 @@ __global__ void pair_sums(const double *__restrict__ kv, int nt, int ns, int nr_
     }
 }
 
+// Tensor forms: kv[t][s] row-major; one warp per (test row, pair), the lanes
+// summing every 32nd SV of each class in model order and the lane sums
+// combined by a fixed shuffle tree (the order is the same on every run; the
+// exact form keeps the reference's sequential sums in pair_sums)
+__global__ void pair_sums_rows(const double *__restrict__ kv, int nt, int ns, int nr_class, const int *__restrict__ start,
+                               const int *__restrict__ nsv, const double *__restrict__ coef, const double *__restrict__ rho,
+                               double *__restrict__ dec)
+{
+    const int npair = nr_class * (nr_class - 1) / 2;
+    const long long total = (long long)nt * npair;
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long id = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; id < total; id += warps) {
+        const int t = (int)(id / npair), p = (int)(id % npair);
+        int i = 0, rem = p;
+        while (rem >= nr_class - 1 - i) { rem -= nr_class - 1 - i; ++i; }
+        const int j = i + 1 + rem;
+        const double *k = kv + (long long)t * ns;
+        const double *coef1 = coef + (long long)(j - 1) * ns;
+        const double *coef2 = coef + (long long)i * ns;
+        double sum = 0;
+        for (int q = lane; q < nsv[i]; q += 32) sum = __dadd_rn(sum, __dmul_rn(coef1[start[i] + q], k[start[i] + q]));
+        for (int q = lane; q < nsv[j]; q += 32) sum = __dadd_rn(sum, __dmul_rn(coef2[start[j] + q], k[start[j] + q]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum = __dadd_rn(sum, __shfl_xor_sync(0xffffffffu, sum, o));
+        if (lane == 0) dec[(long long)t * npair + p] = __dsub_rn(sum, rho[p]);
+    }
+}
+
 struct Session {
     // fingerprint
     const svm_node *const *SV = nullptr;
@@ -490,7 +519,7 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
         for (int t0 = 0; t0 < n; t0 += chunk) {
             const int tn = std::min(chunk, n - t0);
             if (tensor) {
-                PK(launch_kernel_block2(Ttc, *s->sv_tc, kpk, g_predict_form, t0, tn, m->l, kv, tn, d_err, 0));
+                PK(launch_kernel_block2(Ttc, *s->sv_tc, kpk, g_predict_form, t0, tn, m->l, kv, m->l, 0, d_err, 0));
             } else if (dense) {
                 dim3 grid((m->l + kPS - 1) / kPS, (tn + kPT - 1) / kPT);
                 kvalue_tile<<<grid, 256>>>(kp, T.X + (long long)t0 * T.ld, tn, s->sv.X, m->l, s->sv.ld, kv);
@@ -503,7 +532,11 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
                 kvalue_csr<<<(int)std::min<long long>(((long long)tn * m->l + 255) / 256, 148 * 16), 256>>>(kp, Tc, Sc, kv);
                 count_launch();
             }
-            pair_sums<<<std::min<long long>(((long long)tn * npair + 127) / 128, 148 * 8), 128>>>(kv, tn, m->l, k, s->start, s->nsv, s->coef, s->rho, d_dec);
+            if (tensor)
+                pair_sums_rows<<<(int)std::min<long long>(((long long)tn * npair * 32 + 255) / 256, 148 * 16), 256>>>(
+                    kv, tn, m->l, k, s->start, s->nsv, s->coef, s->rho, d_dec);
+            else
+                pair_sums<<<std::min<long long>(((long long)tn * npair + 127) / 128, 148 * 8), 128>>>(kv, tn, m->l, k, s->start, s->nsv, s->coef, s->rho, d_dec);
             count_launch();
             cudaError_t e = cudaDeviceSynchronize();
             if (e != cudaSuccess) {
