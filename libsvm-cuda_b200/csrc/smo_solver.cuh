@@ -1802,78 +1802,6 @@ __device__ bool fill(Ctx &c, Shared &sh, int ns, const int *src_row, const int *
     }
 }
 
-// Speculative rows for a fill pass: the highest-priority candidates of the
-// group's table c.pt (warp 0 picks them by argmax rounds: the largest
-// priority, the lowest table index on ties; lane L owns entries L + 32j),
-// except positions g0, g1, g2, go to the fill list (sh.frow / fy / fslot,
-// sh.nfill) until it holds `limit` rows, each with its cache slot (stamped
-// clk; ways stamped at or after `protect` are never evicted), unless the row
-// is already valid for the active set.  This only fills the cache; it never
-// changes which pair is chosen.  Called by every thread; returns the rows
-// added (thread 0).
-__device__ int add_prefetch(Ctx &c, Shared &sh, int limit, int g0, int g1, int g2, unsigned long long clk,
-                            unsigned long long protect, int whole)
-{
-    const InstanceDesc &D = *c.D;
-    const int ncand = c.nb * kPrefetchCand;
-    const int want = limit - sh.nfill;
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        unsigned taken = 0;
-        int got = 0;
-        for (; got < want; got++) {
-            double bv = -SVMB_INF;
-            int be = 0x7fffffff;
-            for (int e = lane, j = 0; e < ncand; e += 32, j++) {
-                if ((taken >> j) & 1u) continue;
-                const int pos = c.pt->pos[e];
-                const double v = c.pt->v[e];
-                if (pos < 0 || pos == g0 || pos == g1 || pos == g2 || !(v > -SVMB_INF)) continue;
-                if (v > bv) { bv = v; be = e; }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                const int oe = __shfl_xor_sync(0xffffffffu, be, o);
-                if (ov > bv || (ov == bv && oe < be)) { bv = ov; be = oe; }
-            }
-            if (be == 0x7fffffff) break;
-            if ((be & 31) == lane) taken |= 1u << (be >> 5);
-            if (lane == 0) sh.pick[got] = be;
-        }
-        if (lane == 0) sh.npick = got;
-    }
-    __syncthreads();
-    // the picks' cache sets, read by one thread per way in a single round trip
-    for (int e = threadIdx.x; e < sh.npick * kMaxWays; e += blockDim.x) {
-        const int t = e / kMaxWays, w = e % kMaxWays;
-        const int set = c.pt->loc[sh.pick[t]] % D.cache.nsets;
-        if (w == 0) sh.sset[t].set = set;
-        if (w < D.cache.nways) {
-            const long long s = (long long)set * D.cache.nways + w;
-            sh.sset[t].tag[w] = __ldcg(&D.cache.tag[s]);
-            sh.sset[t].ep[w] = __ldcg(&D.cache.epoch[s]);
-            sh.sset[t].st[w] = __ldcg(&D.cache.stamp[s]);
-        }
-    }
-    __syncthreads();
-    int added = 0;
-    if (threadIdx.x == 0) {
-        for (int t = 0; t < sh.npick && sh.nfill < limit; t++) {
-            const int e = sh.pick[t];
-            Lookup L = cache_lookup(sh.cs, D.cache, c.pt->loc[e], c.epoch, clk, whole, protect, 1, &sh.sset[t]);
-            if (L.slot >= 0 && !L.valid_active) {
-                sh.frow[sh.nfill] = c.pt->row[e];
-                sh.fy[sh.nfill] = c.pt->y[e];
-                sh.fslot[sh.nfill] = L.slot;
-                sh.nfill++;
-                added++;
-            }
-        }
-    }
-    __syncthreads();
-    return added;
-}
-
 // position of the phase-A winner of track k (excluded from prefetching)
 __device__ __forceinline__ int i0_prev_guard(const Shared &sh, int k) { return sh.bi[4 * k]; }
 
@@ -2072,9 +2000,71 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                 // speculative prefetch: a missing row is evaluated together with
                 // the rows of the group's most violating positions (this only
                 // fills the cache; it never changes which pair is chosen)
-                if (sh.nfill > 0 && D.prefetch > sh.nfill)
-                    cnt_pf += add_prefetch(c, sh, D.prefetch, i0_prev_guard(sh, 0), i0_prev_guard(sh, 1), -1, clkA, clkA,
-                                           c.A == l);
+                if (sh.nfill > 0 && D.prefetch > sh.nfill) {
+                    // the `want` highest-priority candidates, chosen by warp 0: every
+                    // lane keeps its own best few, then the lanes' heads are merged
+                    // (the order of prefetched rows affects only what is cached)
+                    const int ncand = c.nb * kPrefetchCand;
+                    const int want = D.prefetch - sh.nfill;
+                    if (threadIdx.x < 32) {
+                        // `want` rounds of a warp argmax over the candidates
+                        // (largest priority, the lowest table index on ties); lane
+                        // L owns entries L + 32j and marks the ones taken in a mask
+                        const int lane = threadIdx.x;
+                        const int g0 = i0_prev_guard(sh, 0), g1 = i0_prev_guard(sh, 1);
+                        unsigned taken = 0;
+                        int got = 0;
+                        for (; got < want; got++) {
+                            double bv = -SVMB_INF;
+                            int be = 0x7fffffff;
+                            for (int e = lane, j = 0; e < ncand; e += 32, j++) {
+                                if ((taken >> j) & 1u) continue;
+                                const int pos = c.pt->pos[e];
+                                const double v = c.pt->v[e];
+                                if (pos < 0 || pos == g0 || pos == g1 || !(v > -SVMB_INF)) continue;
+                                if (v > bv) { bv = v; be = e; }
+                            }
+                            for (int o = 16; o > 0; o >>= 1) {
+                                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                                const int oe = __shfl_xor_sync(0xffffffffu, be, o);
+                                if (ov > bv || (ov == bv && oe < be)) { bv = ov; be = oe; }
+                            }
+                            if (be == 0x7fffffff) break;
+                            if ((be & 31) == lane) taken |= 1u << (be >> 5);
+                            if (lane == 0) sh.pick[got] = be;
+                        }
+                        if (lane == 0) sh.npick = got;
+                    }
+                    __syncthreads();
+                    // the picks' cache sets, read by one thread per way in a single round trip
+                    for (int e = threadIdx.x; e < sh.npick * kMaxWays; e += blockDim.x) {
+                        const int t = e / kMaxWays, w = e % kMaxWays;
+                        const int set = c.pt->loc[sh.pick[t]] % D.cache.nsets;
+                        if (w == 0) sh.sset[t].set = set;
+                        if (w < D.cache.nways) {
+                            const long long s = (long long)set * D.cache.nways + w;
+                            sh.sset[t].tag[w] = __ldcg(&D.cache.tag[s]);
+                            sh.sset[t].ep[w] = __ldcg(&D.cache.epoch[s]);
+                            sh.sset[t].st[w] = __ldcg(&D.cache.stamp[s]);
+                        }
+                    }
+                    __syncthreads();
+                    if (threadIdx.x == 0) {
+                        const int whole = c.A == l;
+                        for (int t = 0; t < sh.npick && sh.nfill < D.prefetch; t++) {
+                            const int e = sh.pick[t];
+                            Lookup L = cache_lookup(sh.cs, D.cache, c.pt->loc[e], c.epoch, clkA, whole, clkA, 1, &sh.sset[t]);
+                            if (L.slot >= 0 && !L.valid_active) {
+                                sh.frow[sh.nfill] = c.pt->row[e];
+                                sh.fy[sh.nfill] = c.pt->y[e];
+                                sh.fslot[sh.nfill] = L.slot;
+                                sh.nfill++;
+                                cnt_pf++;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
             }
             Gmax0 = sh.bd[0];
             Gmax1 = sh.bd[3];
@@ -2242,23 +2232,11 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
             SVMB_PROF(kProfBReduce);
             const long long slot_j = sh.bl[2];
             if (!sh.bi[16]) {
-                if (threadIdx.x == 0) {
-                    sh.frow[0] = row_j;
-                    sh.fy[0] = yj;
-                    sh.fslot[0] = slot_j;
-                    sh.nfill = 1;
-                }
-                __syncthreads();
-                // tensor forms: the pass also evaluates speculative rows (the
-                // candidate table of phase A is intact: their fills do not use
-                // the aux area); a pass reads its targets once whatever its sources
-                if constexpr (is_tc_form(FORM)) {
-                    if (D.prefetch > 1)
-                        cnt_pf += add_prefetch(c, sh, D.prefetch, i0, i1, j, clkB, clkA, c.A == l);
-                }
-                const int ns = sh.nfill;
-                if (!fill<FORM>(c, sh, ns, sh.frow, sh.fy, sh.fslot, 0)) goto fail;
-                cnt_q += (long long)ns * c.A;
+                const int srow[1] = {row_j};
+                const int sy[1] = {yj};
+                const long long ss[1] = {slot_j};
+                if (!fill<FORM>(c, sh, 1, srow, sy, ss, 0)) goto fail;
+                cnt_q += c.A;
                 cnt_tgt += c.A;
                 cnt_fill++;
             }
