@@ -868,10 +868,7 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
         D.done_flag = w.done_flags ? w.done_flags + k : nullptr;
         D.tile_bufs = w.tile_bufs;
         {
-            // tensor forms: up to the MMA N rows per pass; CUDA cores: the staged rows
-            const int limit = is_tc_form(prm.form) ? D.tc_n
-                              : D.stage_cap > 0   ? std::min(kPrefetchMax, D.stage_cap)
-                                                  : kPrefetchMax;
+            const int limit = D.stage_cap > 0 ? std::min(kPrefetchMax, D.stage_cap) : kPrefetchMax;
             const int pf = w.tune_prefetch > 0 ? w.tune_prefetch : p.prefetch;
             D.prefetch = pf > 0 ? std::min(pf, limit) : limit;
             D.lazy_gbar = p.lazy_gbar < 0 ? (is_tc_form(prm.form) ? 1 : 0) : p.lazy_gbar;

@@ -59,10 +59,6 @@ constexpr int kTcM = 128;               // targets per tile (MMA M); rows are TM
 constexpr int kTcStages = 3;            // operand stages of the cp.async -> MMA pipeline
 constexpr int kTcMaxN = 4 * (kThreads / 32) < 64 ? 4 * (kThreads / 32) : 64;   // sources per block-product pass
                                         // (MMA N; the epilogue reads 16 columns per group of 4 warps)
-// rows a fill pass may evaluate: up to kPrefetchMax on CUDA cores, up to the
-// MMA N in the tensor forms (a pass reads its targets' rows once, whatever
-// the number of its sources)
-constexpr int kPassMax = kTcMaxN > kPrefetchMax ? kTcMaxN : kPrefetchMax;
 // bytes of one operand stage: target tile (128 rows x 64 bf16, hi and lo) + n source rows (hi and lo)
 SVMB_HD constexpr int tc_stage_bytes(int n) { return 2 * kTcM * 128 + n * 256; }
 SVMB_HD constexpr int tc_area_bytes(int n) { return 1024 + kTcStages * tc_stage_bytes(n); }
@@ -196,7 +192,7 @@ struct InstanceDesc {
     int stage_cap;              // rows staged at once (1..kSrcBatch); 0: read sources from global memory
     int stage_lds;              // floats per staged row (dense: ld; sparse: d)
     int chunk_cap;              // positions of per-block state held in shared memory (>= ceil(l/nblocks))
-    int prefetch;               // rows evaluated per fill pass (1 = no prefetch), <= kPrefetchMax (tensor forms: <= tc_n)
+    int prefetch;               // rows evaluated per fill pass (1 = no prefetch), <= kPrefetchMax
     // 0: G_bar maintained on every bound change, as the reference does (svm.cpp:744-769);
     // 1: no G_bar -- reconstruction recomputes G = p + sum over alpha>0 of alpha*Q on the
     //    inactive positions as one block product (no full-length rows during the loop)

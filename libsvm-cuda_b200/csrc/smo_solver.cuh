@@ -564,11 +564,8 @@ struct CacheRec {
     unsigned long long stamp;
 };
 
-// decisions of one phase: the rows of a fill pass (up to kPassMax), the two
-// working rows and their completion marks
-constexpr int kPhaseRecs = kPassMax + 8;
 struct CacheState {
-    CacheRec prev[kPhaseRecs], cur[kPhaseRecs];
+    CacheRec prev[16], cur[16];
     int nprev, ncur;
 };
 
@@ -747,18 +744,16 @@ struct Shared {
     double cand_v[kWarps];
     int cand_p[kWarps];
     // rows of the current fill pass: row id, label, slot
-    int frow[kPassMax], fy[kPassMax];
-    long long fslot[kPassMax];
-    // per source of the fill pass running now: norm, label, destination row,
-    // inverse split scale (tensor forms)
-    double fsx[kPassMax];
-    int fsy[kPassMax];
-    float *fsd[kPassMax];
-    double fsi[kPassMax];
+    int frow[kPrefetchMax], fy[kPrefetchMax];
+    long long fslot[kPrefetchMax];
+    // per source of the fill pass running now: norm, label, destination row
+    double fsx[kPrefetchMax];
+    int fsy[kPrefetchMax];
+    float *fsd[kPrefetchMax];
     int nfill;
-    int pick[kPassMax];
+    int pick[kPrefetchMax];
     int npick;
-    SetStage sset[kPassMax];        // cache sets of the prefetch picks, read in one round trip
+    SetStage sset[kPrefetchMax];    // cache sets of the prefetch picks, read in one round trip
     // tensor-core block products (FORM_BF16X3, FORM_FP16X3): sources of the current pass
     // (row id, position, alpha, norm, C, inverse scale, label, status), the
     // pipeline's mbarriers (one per operand stage) and the TMEM base address
@@ -1185,41 +1180,41 @@ __device__ bool fill_rows_tc(Ctx &c, Shared &sh, int ns, const int *src_row, con
 {
     const InstanceDesc &D = *c.D;
     if (ns == 0) return true;
-    // per-source constants of the pass in shared memory (up to the MMA N sources)
-    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
-        const int r = src_row[k];
-        sh.tsrow[k] = r;
-        sh.fsx[k] = D.x.xsq[r];
-        sh.fsi[k] = D.x.xinv ? D.x.xinv[r] : 1.0;
-        sh.fsd[k] = D.cache.data + slot[k] * D.cache.stride;
-        sh.fsy[k] = src_y[k];
+    if (threadIdx.x < ns) sh.tsrow[threadIdx.x] = src_row[threadIdx.x];
+    double xs[kPrefetchMax], is[kPrefetchMax];
+    float *dst[kPrefetchMax];
+    int sy[kPrefetchMax];
+#pragma unroll
+    for (int k = 0; k < kPrefetchMax; k++) {
+        const int kk = k < ns ? k : 0;
+        xs[k] = D.x.xsq[src_row[kk]];
+        is[k] = D.x.xinv ? D.x.xinv[src_row[kk]] : 1.0;
+        dst[k] = D.cache.data + slot[kk] * D.cache.stride;
+        sy[k] = src_y[kk];
     }
     __syncthreads();
     const int lo = tail ? c.t0 : 0, hi = tail ? c.t1 : c.a1 - c.a0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int lg = warp & 3, cg = warp >> 2;
-    // warp (lg, cg) holds the dots of targets 32 lg + lane and sources 16 cg .. 16 cg + 15
     return tc_product(c, sh, ns, lo, hi, tail != 0, [&](int tlo, const double *acc) {
-        if (cg * 16 >= ns) return;
-        const int t = tlo + lg * 32 + lane;
-        if (t >= hi) return;
-        int r, yp, col;
-        if (tail) {
-            r = D.pos_row[t];
-            yp = D.y[t];
-            col = D.pos_local[t];
-        } else {
-            r = c.sRow[t];
-            yp = c.sY[t];
-            col = c.sCol[t];
-        }
-        const double xe = D.x.xsq[r];
-        const double ie = D.x.xinv ? D.x.xinv[r] : 1.0;
+        if (warp < 4) {
+            const int t = tlo + warp * 32 + lane;
+            if (t < hi) {
+                int r, yp, col;
+                if (tail) {
+                    r = D.pos_row[t];
+                    yp = D.y[t];
+                    col = D.pos_local[t];
+                } else {
+                    r = c.sRow[t];
+                    yp = c.sY[t];
+                    col = c.sCol[t];
+                }
+                const double xe = D.x.xsq[r];
+                const double ie = D.x.xinv ? D.x.xinv[r] : 1.0;
 #pragma unroll
-        for (int k = 0; k < 16; k++) {
-            const int s2 = cg * 16 + k;
-            if (s2 < ns)
-                sh.fsd[s2][col] = q_value(D.kp, sh.fsy[s2] * yp, __dmul_rn(__dmul_rn(acc[k], ie), sh.fsi[s2]), sh.fsx[s2], xe);
+                for (int k = 0; k < kPrefetchMax; k++)
+                    if (k < ns) dst[k][col] = q_value(D.kp, sy[k] * yp, __dmul_rn(__dmul_rn(acc[k], ie), is[k]), xs[k], xe);
+            }
         }
     });
 }
@@ -2037,8 +2032,8 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                     }
                     __syncthreads();
                     // the picks' cache sets, read by one thread per way in a single round trip
-                    for (int e = threadIdx.x; e < sh.npick * kMaxWays; e += blockDim.x) {
-                        const int t = e / kMaxWays, w = e % kMaxWays;
+                    if (threadIdx.x < sh.npick * kMaxWays) {
+                        const int t = threadIdx.x / kMaxWays, w = threadIdx.x % kMaxWays;
                         const int set = c.pt->loc[sh.pick[t]] % D.cache.nsets;
                         if (w == 0) sh.sset[t].set = set;
                         if (w < D.cache.nways) {

@@ -233,7 +233,7 @@ int api_set_option(const char *name, long long value)
         if (value != 1) return -1;
         arm_drop_block();
     } else if (!strcmp(name, "prefetch")) {
-        if (value < 0 || value > kPassMax) return -1;
+        if (value < 0 || value > kPrefetchMax) return -1;
         g_opt.prefetch = (int)value;
     } else {
         return -1;
