@@ -175,14 +175,19 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
                                      tc::sw128_desc(sa + 2 * kGTileA + h * kGTileB + kk * 32), idesc, h > 0 || kk > 0);
             } else {
 #pragma unroll
+                // the small cross terms of the whole chunk first, then hi.hi: the
+                // tensor core's fp32 accumulation rounds toward zero, and only the
+                // four hi.hi additions then land on a large partial sum
                 for (int kk = 0; kk < 4; kk++) {
                     const uint64_t ahi = tc::sw128_desc(sa + kk * 32), alo = tc::sw128_desc(sa + kGTileA + kk * 32);
                     const uint64_t bhi = tc::sw128_desc(sa + 2 * kGTileA + kk * 32);
                     const uint64_t blo = tc::sw128_desc(sa + 2 * kGTileA + kGTileB + kk * 32);
                     tc::mma_bf16(dst, ahi, blo, idesc, kk > 0);
                     tc::mma_bf16(dst, alo, bhi, idesc, true);
-                    tc::mma_bf16(dst, ahi, bhi, idesc, true);
                 }
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++)
+                    tc::mma_bf16(dst, tc::sw128_desc(sa + kk * 32), tc::sw128_desc(sa + 2 * kGTileA + kk * 32), idesc, true);
             }
             tc::mma_commit(&bars[s]);
         }

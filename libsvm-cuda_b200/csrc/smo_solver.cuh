@@ -1130,13 +1130,18 @@ __device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool glob
                                      tc::sw128_desc(sa + (h ? b_lo : b_hi) + kk * 32), idesc, h > 0 || kk > 0);
             } else {
 #pragma unroll
+                // the small cross terms of the whole chunk first, then hi.hi (the
+                // tensor core's fp32 accumulation rounds toward zero; see the
+                // kernel-block kernel): dots measured 2x less biased this way
                 for (int kk = 0; kk < 4; kk++) {
                     const uint64_t ah = tc::sw128_desc(sa + kk * 32), al = tc::sw128_desc(sa + a_lo + kk * 32);
                     const uint64_t bh = tc::sw128_desc(sa + b_hi + kk * 32), bl = tc::sw128_desc(sa + b_lo + kk * 32);
                     tc::mma_bf16(dst, ah, bl, idesc, kk > 0);
                     tc::mma_bf16(dst, al, bh, idesc, true);
-                    tc::mma_bf16(dst, ah, bh, idesc, true);
                 }
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++)
+                    tc::mma_bf16(dst, tc::sw128_desc(sa + kk * 32), tc::sw128_desc(sa + b_hi + kk * 32), idesc, true);
             }
             tc::mma_commit(&sh.tbar[G % kTcStages]);
         }
