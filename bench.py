@@ -626,6 +626,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--clocks-dir", default=None, help="where to keep the nvidia-smi clock samples (default: temp dir)")
     ap.add_argument("--no-extras", action="store_true", help="skip the precision-form, CV-grid and serving workloads")
+    ap.add_argument("--extras", default=None, help="run only these extra workloads (comma-separated names)")
     ap.add_argument("--profile-case", default=None, help="run one solver launch for a profiler capture and exit")
     args = ap.parse_args()
     if args.profile_case:
@@ -780,6 +781,8 @@ def main():
                              ("sparse_c2", lambda: sparse_c2_extra(eng, ResidentRows, make_params)),
                              ("cv_grid", lambda: cv_grid_extra(eng)),
                              ("serving", lambda: serving_extra(eng, make_params))):
+                if args.extras is not None and name not in args.extras.split(","):
+                    continue
                 try:
                     extras[name] = fn()
                 except Exception as e:          # an extra never hides the headline line
