@@ -62,6 +62,22 @@ constexpr int kTcMaxN = 4 * (kThreads / 32) < 64 ? 4 * (kThreads / 32) : 64;   /
 // bytes of one operand stage: target tile (128 rows x 64 bf16, hi and lo) + n source rows (hi and lo)
 SVMB_HD constexpr int tc_stage_bytes(int n) { return 2 * kTcM * 128 + n * 256; }
 SVMB_HD constexpr int tc_area_bytes(int n) { return 1024 + kTcStages * tc_stage_bytes(n); }
+// the Q-row fill pipeline of the tensor forms reuses that area: stages of one
+// target tile + kFillN source rows; warps 0-3 read the accumulators, warp 4
+// issues the MMAs, warps kFillLoad0.. load the operands
+constexpr int kFillN = 16;              // MMA N of a fill pass (>= kPrefetchMax sources)
+constexpr int kFillStagesMax = 4;
+constexpr int kFillAcc = 4;             // TMEM accumulators of kFillN columns, used in turn
+constexpr int kFillLoad0 = 5;
+SVMB_HD constexpr int fill_stage_bytes() { return 2 * kTcM * 128 + kFillN * 256; }
+SVMB_HD constexpr int fill_stages(int tc_n)
+{
+    return (tc_area_bytes(tc_n) - 1024) / fill_stage_bytes() < kFillStagesMax
+               ? (tc_area_bytes(tc_n) - 1024) / fill_stage_bytes()
+               : kFillStagesMax;
+}
+static_assert(fill_stages(16) >= 3, "the fill pipeline needs three operand stages");
+static_assert(kThreads / 32 > kFillLoad0, "the fill pipeline needs loader warps");
 
 enum : uint8_t { ST_LOWER = 0, ST_UPPER = 1, ST_FREE = 2 };   // reference svm.cpp:425
 

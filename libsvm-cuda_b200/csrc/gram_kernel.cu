@@ -24,12 +24,15 @@
 // multiple of 64.  RBF distances use the float64 row norms.
 // The kernel value itself is always formed in float64 from the dot product.
 //
-// Tensor-core tiling: one CTA computes a 128 x 64 tile of dots; K runs in
-// chunks of 64 features (the split rows store, per chunk, 64 hi then 64 lo
-// 16-bit values = 256 contiguous bytes), staged by cp.async into 128B-swizzled
-// K-major shared-memory tiles, three stages deep; thread 0 issues the 12 MMAs
-// of a chunk (4 K-steps x 3 products, M=128 N=64 K=16) and commits them to
-// the stage's mbarrier, which releases the stage and the chunk's accumulator.
+// Tensor-core tiling: a persistent CTA per SM walks 128 x 64 tiles of dots;
+// K runs in chunks of 64 features (the split rows store, per chunk, 64 hi then
+// 64 lo 16-bit values = 256 contiguous bytes), staged by cp.async into
+// 128B-swizzled K-major shared-memory tiles, four stages deep.  The warps are
+// specialised and meet only at mbarriers: loader warps fill free stages (and
+// run on into the next tile), one thread issues the 12 MMAs of a chunk (4
+// K-steps x 3 products, M=128 N=64 K=16) into one of four TMEM accumulators,
+// and eight reader warps add each finished chunk into float64 registers and
+// write the tile's kernel values while the next tile's chunks are loaded.
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -46,12 +49,19 @@ namespace {
 
 constexpr int kGM = 128;                                // rows of a tile (TMEM lanes)
 constexpr int kGN = 64;                                 // columns of a tile
-constexpr int kGThreads = 256;                          // 8 warps: 4 lane quarters x 2 column halves
-constexpr int kGStages = 3;
+constexpr int kGReaders = 8;                            // warps 0-7: 4 lane quarters x 2 column halves
+constexpr int kGIssuer = 8;                             // warp 8 issues the MMAs
+constexpr int kGLoad0 = 9;                              // warps 9-15 load the operands
+constexpr int kGThreads = 512;
+constexpr int kGLoaders = kGThreads - kGLoad0 * 32;
+constexpr int kGStages = 4;
+constexpr int kGAcc = 4;                                // TMEM accumulators of kGN columns, used in turn
 constexpr int kGTileA = kGM * 128;                      // bytes of a 128-row x 64-bf16 operand tile
 constexpr int kGTileB = kGN * 128;                      // bytes of a 64-row x 64-bf16 operand tile
 constexpr int kGStageBytes = 2 * kGTileA + 2 * kGTileB; // A hi, A lo, B hi, B lo
 constexpr int kGSmem = kGStages * kGStageBytes + 1024;  // + alignment slack
+constexpr int kGPieces = ((kGM + kGN) * 16 + kGLoaders - 1) / kGLoaders;   // 16-byte pieces per loader and step
+static_assert(kGSmem <= 227 * 1024, "stages exceed the shared memory of a CTA");
 
 struct GramArgs {
     const uint16_t *xs;         // split rows [n][nchunk][128] of the tile rows (A)
@@ -73,39 +83,40 @@ struct GramArgs {
     int *err;
 };
 
-// One CTA: a 128 x 64 tile of dots.  Each 64-feature chunk's 12 MMAs (4
-// K-steps x hi.lo, lo.hi, hi.hi) start a fresh float32 accumulator in TMEM
-// (two, alternating); while the next chunk's MMAs run, the 8 warps add the
-// finished chunk into float64 registers (warp w: lanes 32(w%4).., columns
-// 32(w/4)..+31), so the tensor core's float32 accumulation spans 64 features.
+// Persistent CTA: tiles blockIdx.x, blockIdx.x + gridDim.x, ... of the
+// ceil(ma/128) x ceil(nb/64) tiles, tile t = (t / ntn, t % ntn).  Each 64-feature
+// chunk's 12 MMAs start a fresh float32 accumulator, so the tensor core's
+// float32 accumulation spans 64 features; reader warp w adds it into float64
+// registers (lanes 32(w%4).., columns 32(w/4)..+31).  Every wait is bounded; a
+// role whose wait runs out sets `abort`, which ends the other roles' waits,
+// and the launch reports the failure through a.err.
 template <int SF>   // the split form: FORM_BF16X3, FORM_FP16X3 or FORM_TF32
 __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
 {
     extern __shared__ uint8_t g_smem_raw[];
-    __shared__ uint64_t bars[kGStages];
+    __shared__ uint64_t full[kGStages], empty[kGStages], accf[kGAcc], acce[kGAcc];
     __shared__ uint32_t tmem_base;
-    __shared__ long long offA[kGM], offB[kGN];
+    __shared__ int abort_flag;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int lq = warp & 3, ch = warp >> 2;
-    const int m0 = blockIdx.y * kGM, n0 = blockIdx.x * kGN;
     const uint32_t raw = tc::smem_addr(g_smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
+    volatile int *abort = &abort_flag;
 
-    if (tid < kGM) {
-        const int r = m0 + tid;
-        offA[tid] = r < a.ma ? (long long)(a.ia ? a.ia[r] : r) * a.rs : -1;
-    }
-    if (tid < kGN) {
-        const int c = n0 + tid;
-        offB[tid] = c < a.nb ? (long long)(a.ib ? a.ib[c] : c) * a.rs : -1;
-    }
     if (tid == 0) {
-        for (int s = 0; s < kGStages; s++) tc::mbar_init(&bars[s], 1);
+        for (int s = 0; s < kGStages; s++) {
+            tc::mbar_init(&full[s], kGLoaders);
+            tc::mbar_init(&empty[s], 1);
+        }
+        for (int s = 0; s < kGAcc; s++) {
+            tc::mbar_init(&accf[s], 1);
+            tc::mbar_init(&acce[s], kGReaders * 32);
+        }
+        abort_flag = 0;
         tc::mbar_init_fence();
     }
     if (warp == 0) {
-        tc::tmem_alloc(&tmem_base, 2 * kGN);
+        tc::tmem_alloc(&tmem_base, kGAcc * kGN);
         tc::tmem_relinquish();
     }
     tc::tc_fence_before();
@@ -113,119 +124,191 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
     tc::tc_fence_after();
     const uint32_t tmem = tmem_base;
 
-    // stage s <- chunk kc of the 128 A rows and 64 B rows (16 pieces of 16 B per row)
-    auto load = [&](int s, int kc) {
-        const uint32_t sa = base + s * kGStageBytes;
-        for (int idx = tid; idx < (kGM + kGN) * 16; idx += kGThreads) {
-            const int r = idx >> 4, q = idx & 15;
-            if (r < kGM) {
-                const long long o = offA[r];
-                tc::cp_async16(sa + (q >= 8 ? kGTileA : 0) + tc::sw128_offset(r, q & 7),
-                               a.xs + (o < 0 ? 0 : o) + kc * 128 + q * 8, o < 0 ? 0u : 16u);
-            } else {
-                const int rb = r - kGM;
-                const long long o = offB[rb];
-                tc::cp_async16(sa + 2 * kGTileA + (q >= 8 ? kGTileB : 0) + tc::sw128_offset(rb, q & 7),
-                               a.xs_b + (o < 0 ? 0 : o) + kc * 128 + q * 8, o < 0 ? 0u : 16u);
-            }
-        }
-    };
-
-    const uint32_t idesc = SF == FORM_TF32 ? tc::idesc_tf32_f32(kGM, kGN) : tc::idesc_f16_f32(kGM, kGN, SF == FORM_BF16X3);
     const int nk = a.nchunk;
-    double acc[32];
+    const int ntn = (a.nb + kGN - 1) / kGN;
+    const int ntiles = ((a.ma + kGM - 1) / kGM) * ntn;
+    const int mine = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int total = mine * nk;
+
+    if (warp < kGReaders) {
+        // ---- readers: add each chunk into float64, then the tile's kernel values
+        const int lq = warp & 3, ch = warp >> 2;
+        double acc[32];
 #pragma unroll
-    for (int k = 0; k < 32; k++) acc[k] = 0.0;
-    auto absorb = [&](int kc) {
-        tc::tc_fence_after();
-        float v[16];
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            tc::tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)((kc & 1) * kGN + ch * 32 + h * 16), v);
-#pragma unroll
-            for (int k = 0; k < 16; k++) acc[h * 16 + k] = __dadd_rn(acc[h * 16 + k], (double)v[k]);
-        }
-    };
-    bool ok = true;
-    for (int s = 0; s < kGStages - 1; s++) {
-        if (s < nk) load(s, s);
-        tc::cp_async_commit();
-    }
-    for (int kc = 0; kc < nk; kc++) {
-        const int s = kc % kGStages;
-        // the MMAs of chunk kc-1 have read their stage and written their accumulator
-        bool w = true;
-        if (kc >= 1) w = tc::mbar_wait(&bars[(kc - 1) % kGStages], ((kc - 1) / kGStages) & 1);
-        if (w && kc + kGStages - 1 < nk) load((kc + kGStages - 1) % kGStages, kc + kGStages - 1);
-        tc::cp_async_commit();
-        tc::cp_async_wait<kGStages - 1>();
-        tc::fence_async_smem();
-        ok = __syncthreads_and(w) != 0;
-        if (!ok) break;
-        if (tid == 0) {
+        for (int k = 0; k < 32; k++) acc[k] = 0.0;
+        int ab = 0, kc = 0, t = blockIdx.x;
+        unsigned ph = 0;
+        for (int g = 0; g < total; g++) {
+            if (!tc::mbar_wait_or(&accf[ab], ph, abort)) {
+                *abort = 1;
+                break;
+            }
             tc::tc_fence_after();
-            const uint32_t sa = base + s * kGStageBytes;
-            const uint32_t dst = tmem + (uint32_t)((kc & 1) * kGN);
-            if (SF == FORM_TF32) {
+            float v[16];
 #pragma unroll
-                for (int h = 0; h < 2; h++)
+            for (int h = 0; h < 2; h++) {
+                tc::tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + (uint32_t)(ab * kGN + ch * 32 + h * 16), v);
+#pragma unroll
+                for (int k = 0; k < 16; k++) acc[h * 16 + k] = __dadd_rn(acc[h * 16 + k], (double)v[k]);
+            }
+            tc::tc_fence_before();
+            tc::mbar_arrive(&acce[ab]);
+            if (++ab == kGAcc) {
+                ab = 0;
+                ph ^= 1u;
+            }
+            if (++kc < nk) continue;
+            // epilogue of tile t: this thread's row and 32 columns
+            const int m0 = (t / ntn) * kGM, n0 = (t % ntn) * kGN;
+            const int row = m0 + lq * 32 + lane;
+            if (row < a.ma) {
+                const int ra = a.ia ? a.ia[row] : row;
+                const double xa = a.xsq[ra];
+                const double sa_inv = a.xinv ? a.xinv[ra] : 1.0;
+#pragma unroll
+                for (int k = 0; k < 32; k++) {
+                    const int col = n0 + ch * 32 + k;
+                    if (col < a.nb) {
+                        const int rb = a.ib ? a.ib[col] : col;
+                        const double sb_inv = a.xinv_b ? a.xinv_b[rb] : 1.0;
+                        const double v2 = kernel_from_dot(a.kp, __dmul_rn(__dmul_rn(acc[k], sa_inv), sb_inv), xa, a.xsq_b[rb]);
+                        // transposed: the lanes of a warp (consecutive rows) write consecutive words
+                        if (a.trans) a.out[(long long)col * a.ldo + row] = v2;
+                        else a.out[(long long)row * a.ldo + col] = v2;
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 32; k++) acc[k] = 0.0;
+            kc = 0;
+            t += gridDim.x;
+        }
+    } else if (warp == kGIssuer) {
+        // ---- MMA issue
+        if (lane == 0) {
+            const uint32_t idesc = SF == FORM_TF32 ? tc::idesc_tf32_f32(kGM, kGN) : tc::idesc_f16_f32(kGM, kGN, SF == FORM_BF16X3);
+            int s = 0, ab = 0, issued = 0;
+            unsigned phs = 0, pha = 0;
+            for (int g = 0; g < total; g++) {
+                if (!tc::mbar_wait_or(&full[s], phs, abort) || !tc::mbar_wait_or(&acce[ab], pha ^ 1u, abort)) {
+                    *abort = 1;
+                    break;
+                }
+                tc::tc_fence_after();
+                const uint32_t sa = base + s * kGStageBytes;
+                const uint32_t dst = tmem + (uint32_t)(ab * kGN);
+                if (SF == FORM_TF32) {
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
+#pragma unroll
+                        for (int kk = 0; kk < 4; kk++)
+                            tc::mma_tf32(dst, tc::sw128_desc(sa + h * kGTileA + kk * 32),
+                                         tc::sw128_desc(sa + 2 * kGTileA + h * kGTileB + kk * 32), idesc, h > 0 || kk > 0);
+                } else {
+#pragma unroll
+                    // the small cross terms of the whole chunk first, then hi.hi: the
+                    // tensor core's fp32 accumulation rounds toward zero, and only the
+                    // four hi.hi additions then land on a large partial sum
+                    for (int kk = 0; kk < 4; kk++) {
+                        const uint64_t ahi = tc::sw128_desc(sa + kk * 32), alo = tc::sw128_desc(sa + kGTileA + kk * 32);
+                        const uint64_t bhi = tc::sw128_desc(sa + 2 * kGTileA + kk * 32);
+                        const uint64_t blo = tc::sw128_desc(sa + 2 * kGTileA + kGTileB + kk * 32);
+                        tc::mma_bf16(dst, ahi, blo, idesc, kk > 0);
+                        tc::mma_bf16(dst, alo, bhi, idesc, true);
+                    }
 #pragma unroll
                     for (int kk = 0; kk < 4; kk++)
-                        tc::mma_tf32(dst, tc::sw128_desc(sa + h * kGTileA + kk * 32),
-                                     tc::sw128_desc(sa + 2 * kGTileA + h * kGTileB + kk * 32), idesc, h > 0 || kk > 0);
-            } else {
-#pragma unroll
-                // the small cross terms of the whole chunk first, then hi.hi: the
-                // tensor core's fp32 accumulation rounds toward zero, and only the
-                // four hi.hi additions then land on a large partial sum
-                for (int kk = 0; kk < 4; kk++) {
-                    const uint64_t ahi = tc::sw128_desc(sa + kk * 32), alo = tc::sw128_desc(sa + kGTileA + kk * 32);
-                    const uint64_t bhi = tc::sw128_desc(sa + 2 * kGTileA + kk * 32);
-                    const uint64_t blo = tc::sw128_desc(sa + 2 * kGTileA + kGTileB + kk * 32);
-                    tc::mma_bf16(dst, ahi, blo, idesc, kk > 0);
-                    tc::mma_bf16(dst, alo, bhi, idesc, true);
+                        tc::mma_bf16(dst, tc::sw128_desc(sa + kk * 32), tc::sw128_desc(sa + 2 * kGTileA + kk * 32), idesc, true);
                 }
+                tc::mma_commit(&empty[s]);
+                tc::mma_commit(&accf[ab]);
+                issued++;
+                if (++s == kGStages) {
+                    s = 0;
+                    phs ^= 1u;
+                }
+                if (++ab == kGAcc) {
+                    ab = 0;
+                    pha ^= 1u;
+                }
+            }
+            if (issued < total && issued > 0) {
+                // stopped early: let the MMAs already issued finish first
+                const int G = issued - 1;
+                tc::mbar_wait(&empty[G % kGStages], (unsigned)((G / kGStages) & 1));
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- operand loads: piece i of a step is 16 bytes of an A row (i < 16 * kGM)
+        // or of a B row; a thread's pieces keep their rows for a whole tile
+        const int lt = tid - kGLoad0 * 32;
+        const uint16_t *src[kGPieces];
+        uint32_t off[kGPieces];
+        int s = 0, sd = 0, kc = 0, t = blockIdx.x;
+        unsigned phs = 0;
+        bool run = true;
+        // up to kGStages - 1 steps in flight; a landed step is handed to the
+        // MMA before this thread waits for a free stage, so that the MMAs of
+        // consecutive steps queue back to back
+        for (int g = 0; g < total + kGStages - 1; g++) {
+            if (g >= kGStages - 1 && run) {
+                // step g - (kGStages - 1) has landed (kGStages - 2 younger groups may be pending)
+                tc::cp_async_wait<kGStages - 2>();
+                tc::fence_async_smem();
+                tc::mbar_arrive(&full[sd]);
+                if (++sd == kGStages) sd = 0;
+            }
+            if (g < total && run) {
+                if (kc == 0) {
+                    const int m0 = (t / ntn) * kGM, n0 = (t % ntn) * kGN;
 #pragma unroll
-                for (int kk = 0; kk < 4; kk++)
-                    tc::mma_bf16(dst, tc::sw128_desc(sa + kk * 32), tc::sw128_desc(sa + 2 * kGTileA + kk * 32), idesc, true);
+                    for (int j = 0; j < kGPieces; j++) {
+                        const int i = lt + j * kGLoaders;
+                        src[j] = nullptr;
+                        off[j] = 0;
+                        const int q = i & 15;
+                        if (i < 16 * kGM) {
+                            const int r = i >> 4;
+                            if (m0 + r < a.ma) {
+                                src[j] = a.xs + (long long)(a.ia ? a.ia[m0 + r] : m0 + r) * a.rs + q * 8;
+                                off[j] = (q >= 8 ? kGTileA : 0) + tc::sw128_offset(r, q & 7);
+                            }
+                        } else if (i < 16 * (kGM + kGN)) {
+                            const int r = (i >> 4) - kGM;
+                            if (n0 + r < a.nb) {
+                                src[j] = a.xs_b + (long long)(a.ib ? a.ib[n0 + r] : n0 + r) * a.rs + q * 8;
+                                off[j] = 2 * kGTileA + (q >= 8 ? kGTileB : 0) + tc::sw128_offset(r, q & 7);
+                            }
+                        }
+                    }
+                }
+                if (!tc::mbar_wait_or(&empty[s], phs ^ 1u, abort)) {
+                    *abort = 1;
+                    run = false;
+                } else {
+                    const uint32_t sa = base + s * kGStageBytes;
+#pragma unroll
+                    for (int j = 0; j < kGPieces; j++)
+                        if (src[j]) tc::cp_async16(sa + off[j], src[j] + kc * 128, 16u);
+                }
+                if (++s == kGStages) {
+                    s = 0;
+                    phs ^= 1u;
+                }
+                if (++kc == nk) {
+                    kc = 0;
+                    t += gridDim.x;
+                }
             }
-            tc::mma_commit(&bars[s]);
+            tc::cp_async_commit();
         }
-        if (kc >= 1) {
-            absorb(kc - 1);
-            tc::tc_fence_before();
-        }
-        __syncthreads();
-    }
-    if (ok && nk > 0) {
-        ok = __syncthreads_and(tc::mbar_wait(&bars[(nk - 1) % kGStages], ((nk - 1) / kGStages) & 1)) != 0;
-        if (ok) absorb(nk - 1);
-    }
-    tc::cp_async_wait<0>();
-    if (!ok && tid == 0) atomicExch(a.err, 1);
-
-    // epilogue: this thread's row and 32 columns
-    const int row = m0 + lq * 32 + lane;
-    if (ok && nk > 0 && row < a.ma) {
-        const int ra = a.ia ? a.ia[row] : row;
-        const double xa = a.xsq[ra];
-        const double sa_inv = a.xinv ? a.xinv[ra] : 1.0;
-#pragma unroll 4
-        for (int k = 0; k < 32; k++) {
-            const int col = n0 + ch * 32 + k;
-            if (col < a.nb) {
-                const int rb = a.ib ? a.ib[col] : col;
-                const double sb_inv = a.xinv_b ? a.xinv_b[rb] : 1.0;
-                const double v = kernel_from_dot(a.kp, __dmul_rn(__dmul_rn(acc[k], sa_inv), sb_inv), xa, a.xsq_b[rb]);
-                // transposed: the lanes of a warp (consecutive rows) write consecutive words
-                if (a.trans) a.out[(long long)col * a.ldo + row] = v;
-                else a.out[(long long)row * a.ldo + col] = v;
-            }
-        }
+        tc::cp_async_wait<0>();
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, 2 * kGN);
+    if (*abort && tid == 0) atomicExch(a.err, 1);
+    if (warp == 0) tc::tmem_dealloc(tmem, kGAcc * kGN);
 }
 
 // CUDA-core kernel block: one thread per output, 16 x 16 threads per CTA
@@ -386,8 +469,18 @@ const void *gram_fn(int form)
     return (const void *)gram_split_kernel<FORM_FP16X3>;
 }
 
-void launch_gram(int form, dim3 grid, const GramArgs &a, cudaStream_t s)
+// one persistent CTA per SM (or per tile, when there are fewer tiles)
+void launch_gram(int form, const GramArgs &a, cudaStream_t s)
 {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const long long tiles = (long long)((a.ma + kGM - 1) / kGM) * ((a.nb + kGN - 1) / kGN);
+    const dim3 grid((unsigned)std::max<long long>(1, std::min<long long>(tiles, sms)));
     if (form == FORM_BF16X3) gram_split_kernel<FORM_BF16X3><<<grid, kGThreads, kGSmem, s>>>(a);
     else if (form == FORM_TF32) gram_split_kernel<FORM_TF32><<<grid, kGThreads, kGSmem, s>>>(a);
     else gram_split_kernel<FORM_FP16X3><<<grid, kGThreads, kGSmem, s>>>(a);
@@ -453,8 +546,7 @@ cudaError_t launch_kernel_block(const DeviceRows &rows, const KernelParams &kp, 
         a.out = d_out; a.ldo = ldo;
         a.trans = 0;
         a.err = d_err;
-        dim3 grid((nb + kGN - 1) / kGN, (ma + kGM - 1) / kGM);
-        launch_gram(form, grid, a, s);
+        launch_gram(form, a, s);
     } else {
         dim3 grid((nb + 15) / 16, (ma + 15) / 16), block(16, 16);
         if (form == FORM_EXACT)
@@ -490,8 +582,7 @@ cudaError_t launch_kernel_block2(const DeviceRows &A, const DeviceRows &B, const
     a.out = d_out; a.ldo = ldo;
     a.trans = trans;
     a.err = d_err;
-    dim3 grid((nb + kGN - 1) / kGN, (ma + kGM - 1) / kGM);
-    launch_gram(form, grid, a, s);
+    launch_gram(form, a, s);
     count_launch();
     return cudaGetLastError();
 }

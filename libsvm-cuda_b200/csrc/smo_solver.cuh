@@ -763,6 +763,10 @@ struct Shared {
     unsigned char tss[kTcMaxN];
     uint64_t tbar[kTcStages];
     uint32_t tmem;
+    // the fill pipeline's mbarriers: operand stage loaded / free, accumulator
+    // written / read; fabort is set by a role whose wait ran out
+    uint64_t ffull[kFillStagesMax], fempty[kFillStagesMax], faccf[kFillAcc], facce[kFillAcc];
+    int fabort;
 };
 
 // The group's prefetch candidates (kPrefetchCand per block).  They live in
@@ -793,6 +797,8 @@ struct Ctx {
     Partial *lrec;          // single-block groups keep their two records in shared memory
     uint32_t tcbase;        // FORM_BF16X3: shared address of the operand stages (1024-aligned)
     long long tc_g, tc_t;   // tensor-core steps and tiles issued so far (mbarrier phase parities)
+    long long fg;           // steps of the fill pipeline so far (its mbarrier phase parities)
+    int fstages;            // operand stages of the fill pipeline (3 or 4, by the stage area)
 };
 
 __device__ __forceinline__ void set_chunks(Ctx &c)
@@ -1179,49 +1185,234 @@ __device__ bool tc_product(Ctx &c, Shared &sh, int ns, int lo, int hi, bool glob
 }
 
 // tensor-core form of fill_rows: Q rows of ns (<= kPrefetchMax) sources into
-// cache slots, on my chunk of [0,A) (tail = 0) or of [A,l) (tail = 1)
+// cache slots, on my chunk of [0,A) (tail = 0) or of [A,l) (tail = 1).
+//
+// A warp-specialised pipeline over the steps (one 64-feature chunk of one
+// 128-target tile) with no block barrier per step:
+//   warps kFillLoad0..  load a step's target tile and source rows into a free
+//                       operand stage (cp.async), wait for their own copies,
+//                       fence them into the async proxy and arrive on ffull;
+//   warp 4, one lane    waits for ffull and for a free accumulator, issues the
+//                       step's MMAs and commits them to fempty (stage free) and
+//                       faccf (accumulator written);
+//   warps 0-3           (TMEM lanes = the tile's 128 targets) wait for faccf,
+//                       add the fp32 chunk into fp64 registers, arrive on facce,
+//                       and write the tile's Q values after its last chunk.
+// The MMAs, their order and the fp64 flush are those of tc_product, so the Q
+// values are the same bit for bit.  Every wait is bounded; a role whose wait
+// runs out sets fabort, which ends the other roles' waits.
 __device__ bool fill_rows_tc(Ctx &c, Shared &sh, int ns, const int *src_row, const int *src_y, const long long *slot,
                              int tail)
 {
     const InstanceDesc &D = *c.D;
     if (ns == 0) return true;
-    if (threadIdx.x < ns) sh.tsrow[threadIdx.x] = src_row[threadIdx.x];
-    double xs[kPrefetchMax], is[kPrefetchMax];
-    float *dst[kPrefetchMax];
-    int sy[kPrefetchMax];
-#pragma unroll
-    for (int k = 0; k < kPrefetchMax; k++) {
-        const int kk = k < ns ? k : 0;
-        xs[k] = D.x.xsq[src_row[kk]];
-        is[k] = D.x.xinv ? D.x.xinv[src_row[kk]] : 1.0;
-        dst[k] = D.cache.data + slot[kk] * D.cache.stride;
-        sy[k] = src_y[kk];
+    if (threadIdx.x < ns) {
+        // the sources' row, norm, inverse scale, label and destination row
+        const int k = threadIdx.x;
+        sh.tsrow[k] = src_row[k];
+        sh.fsx[k] = D.x.xsq[src_row[k]];
+        sh.tsi[k] = D.x.xinv ? D.x.xinv[src_row[k]] : 1.0;
+        sh.fsy[k] = src_y[k];
+        sh.fsd[k] = D.cache.data + slot[k] * D.cache.stride;
     }
     __syncthreads();
     const int lo = tail ? c.t0 : 0, hi = tail ? c.t1 : c.a1 - c.a0;
+    const int NK = D.x.nchunk;
+    const int ntiles = hi > lo ? (hi - lo + kTcM - 1) / kTcM : 0;
+    const int total = ntiles * NK;
+    if (total <= 0) return true;
+    const int S = c.fstages;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    return tc_product(c, sh, ns, lo, hi, tail != 0, [&](int tlo, const double *acc) {
-        if (warp < 4) {
-            const int t = tlo + warp * 32 + lane;
-            if (t < hi) {
-                int r, yp, col;
-                if (tail) {
-                    r = D.pos_row[t];
-                    yp = D.y[t];
-                    col = D.pos_local[t];
-                } else {
-                    r = c.sRow[t];
-                    yp = c.sY[t];
-                    col = c.sCol[t];
-                }
-                const double xe = D.x.xsq[r];
-                const double ie = D.x.xinv ? D.x.xinv[r] : 1.0;
+    volatile int *abort = &sh.fabort;
+    constexpr uint32_t kStage = (uint32_t)fill_stage_bytes();
+    constexpr uint32_t a_lo = kTcM * 128u;                       // target lo tile
+    constexpr uint32_t b_hi = 2u * kTcM * 128u;                  // source hi tile
+    constexpr uint32_t b_lo = b_hi + (uint32_t)kFillN * 128u;    // source lo tile
+    const long long rs = (long long)NK * 2 * kSplitChunk;
+    if (warp < 4) {
+        // ---- readers and epilogue: target t = tile base + warp * 32 + lane
+        double acc[kPrefetchMax];
 #pragma unroll
-                for (int k = 0; k < kPrefetchMax; k++)
-                    if (k < ns) dst[k][col] = q_value(D.kp, sy[k] * yp, __dmul_rn(__dmul_rn(acc[k], ie), is[k]), xs[k], xe);
+        for (int k = 0; k < kPrefetchMax; k++) acc[k] = 0.0;
+        int a = (int)(c.fg % kFillAcc);
+        unsigned ph = (unsigned)((c.fg / kFillAcc) & 1);
+        int kc = 0, tile = 0;
+        for (int g = 0; g < total; g++) {
+            if (!tc::mbar_wait_or(&sh.faccf[a], ph, abort)) {
+                *abort = 1;
+                break;
+            }
+            tc::tc_fence_after();
+            float v[kPrefetchMax];
+            tc::tmem_ld8(sh.tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * kFillN), v);
+#pragma unroll
+            for (int k = 0; k < kPrefetchMax; k++) acc[k] = __dadd_rn(acc[k], (double)v[k]);
+            tc::tc_fence_before();
+            tc::mbar_arrive(&sh.facce[a]);
+            if (++a == kFillAcc) {
+                a = 0;
+                ph ^= 1u;
+            }
+            if (++kc == NK) {
+                const int t = lo + tile * kTcM + warp * 32 + lane;
+                if (t < hi) {
+                    int r, yp, col;
+                    if (tail) {
+                        r = D.pos_row[t];
+                        yp = D.y[t];
+                        col = D.pos_local[t];
+                    } else {
+                        r = c.sRow[t];
+                        yp = c.sY[t];
+                        col = c.sCol[t];
+                    }
+                    const double xe = D.x.xsq[r];
+                    const double ie = D.x.xinv ? D.x.xinv[r] : 1.0;
+#pragma unroll
+                    for (int k = 0; k < kPrefetchMax; k++)
+                        if (k < ns)
+                            sh.fsd[k][col] = q_value(D.kp, sh.fsy[k] * yp, __dmul_rn(__dmul_rn(acc[k], ie), sh.tsi[k]),
+                                                     sh.fsx[k], xe);
+                }
+#pragma unroll
+                for (int k = 0; k < kPrefetchMax; k++) acc[k] = 0.0;
+                kc = 0;
+                tile++;
             }
         }
-    });
+    } else if (warp == 4) {
+        // ---- MMA issue
+        if (lane == 0) {
+            const uint32_t idesc = D.form == FORM_TF32 ? tc::idesc_tf32_f32(kTcM, kFillN)
+                                                       : tc::idesc_f16_f32(kTcM, kFillN, D.form == FORM_BF16X3);
+            int s = (int)(c.fg % S), a = (int)(c.fg % kFillAcc);
+            unsigned phs = (unsigned)((c.fg / S) & 1), pha = (unsigned)((c.fg / kFillAcc) & 1);
+            int issued = 0;
+            for (int g = 0; g < total; g++) {
+                if (!tc::mbar_wait_or(&sh.ffull[s], phs, abort) || !tc::mbar_wait_or(&sh.facce[a], pha ^ 1u, abort)) {
+                    *abort = 1;
+                    break;
+                }
+                tc::tc_fence_after();
+                const uint32_t sa = c.tcbase + (uint32_t)s * kStage;
+                const uint32_t dst = sh.tmem + (uint32_t)(a * kFillN);
+                if (D.form == FORM_TF32) {
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
+#pragma unroll
+                        for (int kk = 0; kk < 4; kk++)
+                            tc::mma_tf32(dst, tc::sw128_desc(sa + (h ? a_lo : 0u) + kk * 32),
+                                         tc::sw128_desc(sa + (h ? b_lo : b_hi) + kk * 32), idesc, h > 0 || kk > 0);
+                } else {
+                    // cross terms of the chunk first, then hi.hi (as in tc_product)
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) {
+                        tc::mma_bf16(dst, tc::sw128_desc(sa + kk * 32), tc::sw128_desc(sa + b_lo + kk * 32), idesc,
+                                     kk > 0);
+                        tc::mma_bf16(dst, tc::sw128_desc(sa + a_lo + kk * 32), tc::sw128_desc(sa + b_hi + kk * 32),
+                                     idesc, true);
+                    }
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++)
+                        tc::mma_bf16(dst, tc::sw128_desc(sa + kk * 32), tc::sw128_desc(sa + b_hi + kk * 32), idesc, true);
+                }
+                tc::mma_commit(&sh.fempty[s]);
+                tc::mma_commit(&sh.faccf[a]);
+                issued++;
+                if (++s == S) {
+                    s = 0;
+                    phs ^= 1u;
+                }
+                if (++a == kFillAcc) {
+                    a = 0;
+                    pha ^= 1u;
+                }
+            }
+            if (issued < total && issued > 0) {
+                // stopped early: let the MMAs already issued finish before the
+                // stages and the accumulators are given up
+                const long long G = c.fg + issued - 1;
+                tc::mbar_wait(&sh.fempty[G % S], (unsigned)((G / S) & 1));
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- operand loads: piece i of a step is a 16-byte piece of a target
+        // row (i < 16 * kTcM) or of a source row; the pieces of a thread keep
+        // their rows for a whole tile, only the chunk moves
+        constexpr int kLoaders = kThreads - kFillLoad0 * 32;
+        constexpr int kPieces = (16 * kTcM + 16 * kPrefetchMax + kLoaders - 1) / kLoaders;
+        const int lt = threadIdx.x - kFillLoad0 * 32;
+        const uint16_t *Xs = D.x.Xs;
+        const uint16_t *src[kPieces];
+        uint32_t off[kPieces];
+        int s = (int)(c.fg % S), sd = s;
+        unsigned phs = (unsigned)((c.fg / S) & 1);
+        int kc = 0, tile = 0;
+        bool run = true;
+        // up to S - 1 steps in flight; a landed step is handed to the MMA
+        // before this thread waits for a free stage, so that the MMAs of
+        // consecutive steps queue back to back
+        for (int g = 0; g < total + S - 1; g++) {
+            if (g >= S - 1 && run) {
+                // step g - (S - 1) has landed (S - 2 younger groups may be pending)
+                tc::cp_async_wait_n(S - 2);
+                tc::fence_async_smem();
+                tc::mbar_arrive(&sh.ffull[sd]);
+                if (++sd == S) sd = 0;
+            }
+            if (g < total && run) {
+                if (kc == 0) {
+                    const int tb = lo + tile * kTcM;
+#pragma unroll
+                    for (int j = 0; j < kPieces; j++) {
+                        const int i = lt + j * kLoaders;
+                        src[j] = nullptr;
+                        off[j] = 0;
+                        if (i < 16 * kTcM) {
+                            const int r = i >> 4, q = i & 15, t = tb + r;
+                            if (t < hi) {
+                                const int row = tail ? D.pos_row[t] : c.sRow[t];
+                                src[j] = Xs + (long long)row * rs + q * 8;
+                                off[j] = (q >= 8 ? a_lo : 0u) + tc::sw128_offset(r, q & 7);
+                            }
+                        } else if (i < 16 * kTcM + 16 * ns) {
+                            const int r = (i - 16 * kTcM) >> 4, q = i & 15;
+                            src[j] = Xs + (long long)sh.tsrow[r] * rs + q * 8;
+                            off[j] = (q >= 8 ? b_lo : b_hi) + tc::sw128_offset(r, q & 7);
+                        }
+                    }
+                }
+                if (!tc::mbar_wait_or(&sh.fempty[s], phs ^ 1u, abort)) {
+                    *abort = 1;
+                    run = false;
+                } else {
+                    const uint32_t sa = c.tcbase + (uint32_t)s * kStage;
+#pragma unroll
+                    for (int j = 0; j < kPieces; j++)
+                        if (src[j]) tc::cp_async16(sa + off[j], src[j] + kc * 128, 16u);
+                }
+                if (++s == S) {
+                    s = 0;
+                    phs ^= 1u;
+                }
+                if (++kc == NK) {
+                    kc = 0;
+                    tile++;
+                }
+            }
+            tc::cp_async_commit();
+        }
+        tc::cp_async_wait<0>();
+    }
+    c.fg += total;
+    tc::tc_fence_before();
+    __syncthreads();
+    const bool ok = *abort == 0;
+    if (!ok && threadIdx.x == 0) atomicExch(&D.sync->error, 1);
+    __syncthreads();
+    tc::tc_fence_after();
+    return ok;
 }
 
 // tensor-core form of accumulate_rows: sources are taken kTcMaxN (tc_n) at a
@@ -1825,6 +2016,8 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
         c.tcbase = 0;
         c.tc_g = 0;
         c.tc_t = 0;
+        c.fg = 0;
+        c.fstages = fill_stages(D.tc_n);
         if constexpr (is_tc_form(FORM)) {
             const uint32_t raw = tc::smem_addr(dyn);
             c.tcbase = (raw + 1023u) & ~1023u;
@@ -2523,6 +2716,15 @@ smo_persistent(const InstanceDesc *__restrict__ insts, const int *__restrict__ b
         // mbarriers of the tensor-core pipeline and the TMEM accumulator (one block per SM)
         if (threadIdx.x == 0) {
             for (int k = 0; k < kTcStages; k++) tc::mbar_init(&sh.tbar[k], 1);
+            for (int k = 0; k < kFillStagesMax; k++) {
+                tc::mbar_init(&sh.ffull[k], kThreads - kFillLoad0 * 32);
+                tc::mbar_init(&sh.fempty[k], 1);
+            }
+            for (int k = 0; k < kFillAcc; k++) {
+                tc::mbar_init(&sh.faccf[k], 1);
+                tc::mbar_init(&sh.facce[k], kTcM);
+            }
+            sh.fabort = 0;
             tc::mbar_init_fence();
         }
         if (threadIdx.x < 32) {

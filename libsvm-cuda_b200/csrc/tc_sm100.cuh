@@ -71,6 +71,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity)
     return false;
 }
 
+// the same, but also gives up as soon as *abort is non-zero (another role of
+// the block ran out of time and stopped feeding this barrier)
+__device__ __forceinline__ bool mbar_wait_or(uint64_t *bar, unsigned parity, const volatile int *abort)
+{
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (unsigned it = 0; it < kSpinLimit; ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255u) == 255u && (*abort != 0 || global_ns() - t0 > kWaitNs)) return false;
+    }
+    return false;
+}
+
+// one arrival (release at CTA scope)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // ---- proxy / tcgen05 ordering -----------------------------------------------
 // generic-proxy writes to shared memory (st.shared, cp.async) -> visible to the
 // tensor core's async proxy
@@ -111,6 +130,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 32 lanes x 8 consecutive 32-bit columns
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v)
+{
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // ---- descriptors ------------------------------------------------------------
