@@ -38,6 +38,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cstdint>
 
 #include "engine.hpp"
 #include "kernel_math.cuh"
@@ -62,6 +63,12 @@ constexpr int kGStageBytes = 2 * kGTileA + 2 * kGTileB; // A hi, A lo, B hi, B l
 constexpr int kGSmem = kGStages * kGStageBytes + 1024;  // + alignment slack
 constexpr int kGPieces = ((kGM + kGN) * 16 + kGLoaders - 1) / kGLoaders;   // 16-byte pieces per loader and step
 static_assert(kGSmem <= 227 * 1024, "stages exceed the shared memory of a CTA");
+// Column norms and scales of a tile, written by reader threads 0-63 when the
+// tile starts and read by all readers at its end.  Reader warps stay within
+// kGAcc steps of each other, so a slot is rewritten at the earliest
+// 1 + ceil((kGAcc + 1) / nchunk) tiles later: 8 slots cover nchunk = 1.
+constexpr int kGColRing = 8;
+static_assert(kGColRing >= 2 + kGAcc, "column ring too short for one-chunk rows");
 
 struct GramArgs {
     const uint16_t *xs;         // split rows [n][nchunk][128] of the tile rows (A)
@@ -97,6 +104,8 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
     __shared__ uint64_t full[kGStages], empty[kGStages], accf[kGAcc], acce[kGAcc];
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
+    __shared__ double col_xsq[kGColRing][kGN], col_inv[kGColRing][kGN];
+    __shared__ uint64_t colready[kGColRing];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t raw = tc::smem_addr(g_smem_raw);
@@ -112,6 +121,7 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
             tc::mbar_init(&accf[s], 1);
             tc::mbar_init(&acce[s], kGReaders * 32);
         }
+        for (int s = 0; s < kGColRing; s++) tc::mbar_init(&colready[s], kGN);
         abort_flag = 0;
         tc::mbar_init_fence();
     }
@@ -131,14 +141,39 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
     const int total = mine * nk;
 
     if (warp < kGReaders) {
-        // ---- readers: add each chunk into float64, then the tile's kernel values
-        const int lq = warp & 3, ch = warp >> 2;
+        // ---- readers: add each chunk into float64, then the tile's kernel values.
+        // A tile's row norm and scale (registers) and its 64 columns' norms and
+        // scales (shared memory, one buffer per tile parity) are loaded when the
+        // tile starts, so the epilogue waits on no global load.
+        const int lq = warp & 3, ch = warp >> 2, rt = warp * 32 + lane;
         double acc[32];
 #pragma unroll
         for (int k = 0; k < 32; k++) acc[k] = 0.0;
-        int ab = 0, kc = 0, t = blockIdx.x;
-        unsigned ph = 0;
+        int ab = 0, kc = 0, t = blockIdx.x, slot = 0;
+        unsigned ph = 0, phc = 0;
+        double xa = 0.0, sa_inv = 1.0;
         for (int g = 0; g < total; g++) {
+            if (kc == 0) {
+                const int m0 = (t / ntn) * kGM, n0 = (t % ntn) * kGN;
+                const int row = m0 + lq * 32 + lane;
+                if (row < a.ma) {
+                    const int ra = a.ia ? a.ia[row] : row;
+                    xa = a.xsq[ra];
+                    sa_inv = a.xinv ? a.xinv[ra] : 1.0;
+                }
+                if (rt < kGN) {
+                    const int col = n0 + rt;
+                    double cx = 0.0, cs = 1.0;
+                    if (col < a.nb) {
+                        const int rb = a.ib ? a.ib[col] : col;
+                        cx = a.xsq_b[rb];
+                        cs = a.xinv_b ? a.xinv_b[rb] : 1.0;
+                    }
+                    col_xsq[slot][rt] = cx;
+                    col_inv[slot][rt] = cs;
+                    tc::mbar_arrive(&colready[slot]);
+                }
+            }
             if (!tc::mbar_wait_or(&accf[ab], ph, abort)) {
                 *abort = 1;
                 break;
@@ -158,23 +193,33 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
                 ph ^= 1u;
             }
             if (++kc < nk) continue;
-            // epilogue of tile t: this thread's row and 32 columns
+            // epilogue of tile t: this thread's row and 32 columns, once the
+            // tile's column data are in place
+            if (!tc::mbar_wait_or(&colready[slot], phc, abort)) {
+                *abort = 1;
+                break;
+            }
             const int m0 = (t / ntn) * kGM, n0 = (t % ntn) * kGN;
-            const int row = m0 + lq * 32 + lane;
+            const int row = m0 + lq * 32 + lane, c0 = n0 + ch * 32;
             if (row < a.ma) {
-                const int ra = a.ia ? a.ia[row] : row;
-                const double xa = a.xsq[ra];
-                const double sa_inv = a.xinv ? a.xinv[ra] : 1.0;
 #pragma unroll
-                for (int k = 0; k < 32; k++) {
-                    const int col = n0 + ch * 32 + k;
-                    if (col < a.nb) {
-                        const int rb = a.ib ? a.ib[col] : col;
-                        const double sb_inv = a.xinv_b ? a.xinv_b[rb] : 1.0;
-                        const double v2 = kernel_from_dot(a.kp, __dmul_rn(__dmul_rn(acc[k], sa_inv), sb_inv), xa, a.xsq_b[rb]);
-                        // transposed: the lanes of a warp (consecutive rows) write consecutive words
-                        if (a.trans) a.out[(long long)col * a.ldo + row] = v2;
-                        else a.out[(long long)row * a.ldo + col] = v2;
+                for (int k = 0; k < 32; k++)
+                    acc[k] = kernel_from_dot(a.kp, __dmul_rn(__dmul_rn(acc[k], sa_inv), col_inv[slot][ch * 32 + k]), xa,
+                                             col_xsq[slot][ch * 32 + k]);
+                if (a.trans) {
+                    // the lanes of a warp (consecutive rows) write consecutive words
+#pragma unroll
+                    for (int k = 0; k < 32; k++)
+                        if (c0 + k < a.nb) a.out[(long long)(c0 + k) * a.ldo + row] = acc[k];
+                } else {
+                    double *o = a.out + (long long)row * a.ldo + c0;
+                    if (c0 + 32 <= a.nb && ((uintptr_t)o & 15u) == 0) {
+#pragma unroll
+                        for (int k = 0; k < 32; k += 2) *reinterpret_cast<double2 *>(o + k) = make_double2(acc[k], acc[k + 1]);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 32; k++)
+                            if (c0 + k < a.nb) o[k] = acc[k];
                     }
                 }
             }
@@ -182,6 +227,10 @@ __global__ void __launch_bounds__(kGThreads, 1) gram_split_kernel(GramArgs a)
             for (int k = 0; k < 32; k++) acc[k] = 0.0;
             kc = 0;
             t += gridDim.x;
+            if (++slot == kGColRing) {
+                slot = 0;
+                phc ^= 1u;
+            }
         }
     } else if (warp == kGIssuer) {
         // ---- MMA issue

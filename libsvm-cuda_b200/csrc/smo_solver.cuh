@@ -1230,14 +1230,37 @@ __device__ bool fill_rows_tc(Ctx &c, Shared &sh, int ns, const int *src_row, con
     constexpr uint32_t b_lo = b_hi + (uint32_t)kFillN * 128u;    // source lo tile
     const long long rs = (long long)NK * 2 * kSplitChunk;
     if (warp < 4) {
-        // ---- readers and epilogue: target t = tile base + warp * 32 + lane
+        // ---- readers and epilogue: target t = tile base + warp * 32 + lane.
+        // The target's row norm, scale, label and cache column are loaded when
+        // its tile starts, so the epilogue waits on no global load.
         double acc[kPrefetchMax];
 #pragma unroll
         for (int k = 0; k < kPrefetchMax; k++) acc[k] = 0.0;
         int a = (int)(c.fg % kFillAcc);
         unsigned ph = (unsigned)((c.fg / kFillAcc) & 1);
         int kc = 0, tile = 0;
+        int yp = 0, col = 0;
+        bool tok = false;
+        double xe = 0.0, ie = 1.0;
         for (int g = 0; g < total; g++) {
+            if (kc == 0) {
+                const int t = lo + tile * kTcM + warp * 32 + lane;
+                tok = t < hi;
+                if (tok) {
+                    int r;
+                    if (tail) {
+                        r = D.pos_row[t];
+                        yp = D.y[t];
+                        col = D.pos_local[t];
+                    } else {
+                        r = c.sRow[t];
+                        yp = c.sY[t];
+                        col = c.sCol[t];
+                    }
+                    xe = D.x.xsq[r];
+                    ie = D.x.xinv ? D.x.xinv[r] : 1.0;
+                }
+            }
             if (!tc::mbar_wait_or(&sh.faccf[a], ph, abort)) {
                 *abort = 1;
                 break;
@@ -1254,25 +1277,12 @@ __device__ bool fill_rows_tc(Ctx &c, Shared &sh, int ns, const int *src_row, con
                 ph ^= 1u;
             }
             if (++kc == NK) {
-                const int t = lo + tile * kTcM + warp * 32 + lane;
-                if (t < hi) {
-                    int r, yp, col;
-                    if (tail) {
-                        r = D.pos_row[t];
-                        yp = D.y[t];
-                        col = D.pos_local[t];
-                    } else {
-                        r = c.sRow[t];
-                        yp = c.sY[t];
-                        col = c.sCol[t];
-                    }
-                    const double xe = D.x.xsq[r];
-                    const double ie = D.x.xinv ? D.x.xinv[r] : 1.0;
+                if (tok) {
 #pragma unroll
                     for (int k = 0; k < kPrefetchMax; k++)
                         if (k < ns)
-                            sh.fsd[k][col] = q_value(D.kp, sh.fsy[k] * yp, __dmul_rn(__dmul_rn(acc[k], ie), sh.tsi[k]),
-                                                     sh.fsx[k], xe);
+                            __stcg(sh.fsd[k] + col, q_value(D.kp, sh.fsy[k] * yp,
+                                                            __dmul_rn(__dmul_rn(acc[k], ie), sh.tsi[k]), sh.fsx[k], xe));
                 }
 #pragma unroll
                 for (int k = 0; k < kPrefetchMax; k++) acc[k] = 0.0;
