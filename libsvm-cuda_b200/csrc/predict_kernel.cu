@@ -320,6 +320,7 @@ int upload_nodes(const svm_node *const *x, int n, int d, int base, bool dense, R
     if (out.ld == 0) out.ld = 4;
     if (dense) {
         std::vector<double> h((size_t)std::max(n, 1) * out.ld, 0.0);
+#pragma omp parallel for schedule(static)
         for (int r = 0; r < n; r++)
             for (const svm_node *p = x[r]; p->index != -1; ++p) {
                 const int c = p->index - base;
@@ -328,18 +329,24 @@ int upload_nodes(const svm_node *const *x, int n, int d, int base, bool dense, R
         PK(grow(out.X, out.capX, h.size() * sizeof(double)));
         PK(xfer(out.X, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
     } else {
-        std::vector<long long> rp(n + 1, 0);
-        std::vector<int> col;
-        std::vector<double> val;
+        std::vector<long long> rp((size_t)n + 1, 0);
+#pragma omp parallel for schedule(static)
         for (int r = 0; r < n; r++) {
-            rp[r] = (long long)col.size();
-            for (const svm_node *p = x[r]; p->index != -1; ++p) {
-                col.push_back(p->index - base);
-                val.push_back(p->value);
+            long long c = 0;
+            for (const svm_node *p = x[r]; p->index != -1; ++p) c++;
+            rp[(size_t)r + 1] = c;
+        }
+        for (int r = 0; r < n; r++) rp[(size_t)r + 1] += rp[r];
+        std::vector<int> col((size_t)std::max<long long>(rp[n], 1), 0);
+        std::vector<double> val(col.size(), 0.0);
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < n; r++) {
+            long long k = rp[r];
+            for (const svm_node *p = x[r]; p->index != -1; ++p, ++k) {
+                col[k] = p->index - base;
+                val[k] = p->value;
             }
         }
-        rp[n] = (long long)col.size();
-        if (col.empty()) { col.push_back(0); val.push_back(0); }
         PK(grow(out.rowptr, out.capRp, rp.size() * sizeof(long long)));
         PK(grow(out.col, out.capCol, col.size() * sizeof(int)));
         PK(grow(out.val, out.capVal, val.size() * sizeof(double)));
@@ -404,17 +411,26 @@ Session *get_session(const svm_model *m)
 // rows as host CSR (0-based columns) of width d
 int rows_to_device(const svm_node *const *x, int n, int d, int form, DeviceRows &out)
 {
+    // CSR of the rows (columns = libsvm indices), counted and filled in
+    // parallel over rows
     std::vector<long long> rp((size_t)n + 1, 0);
-    std::vector<int> col;
-    std::vector<float> val;
+#pragma omp parallel for schedule(static)
     for (int r = 0; r < n; r++) {
-        for (const svm_node *p = x[r]; p->index != -1; ++p) {
-            col.push_back(p->index);
-            val.push_back((float)p->value);
-        }
-        rp[r + 1] = (long long)col.size();
+        long long c = 0;
+        for (const svm_node *p = x[r]; p->index != -1; ++p) c++;
+        rp[(size_t)r + 1] = c;
     }
-    if (col.empty()) { col.push_back(0); val.push_back(0.0f); }
+    for (int r = 0; r < n; r++) rp[(size_t)r + 1] += rp[r];
+    std::vector<int> col((size_t)std::max<long long>(rp[n], 1), 0);
+    std::vector<float> val(col.size(), 0.0f);
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < n; r++) {
+        long long k = rp[r];
+        for (const svm_node *p = x[r]; p->index != -1; ++p, ++k) {
+            col[k] = p->index;
+            val[k] = (float)p->value;
+        }
+    }
     if (upload_csr(rp.data(), col.data(), val.data(), n, d, out, -1, 0) != 0) return -1;
     return out.prepare_form(form, 0);
 }
@@ -491,6 +507,7 @@ int predict_batch(const svm_model *m, const svm_node *const *rows, int n, double
         // test rows: features beyond the SVs' width cannot meet an SV feature in a
         // dot product but still count in the RBF distance, so widen to cover them
         int maxi = s->d - 1;
+#pragma omp parallel for schedule(static) reduction(max : maxi)
         for (int r = 0; r < n; r++)
             for (const svm_node *p = rows[r]; p->index != -1; ++p) maxi = std::max(maxi, p->index);
         const bool wider = maxi + 1 > s->d;
