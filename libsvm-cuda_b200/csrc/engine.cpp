@@ -526,9 +526,9 @@ const DeviceRows &rows_of(const SubProblem &sp, const DeviceRows &rows) { return
 }  // namespace
 
 int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, int first,
-              int capacity, Wave &w)
+              int capacity, Wave &w, int limit)
 {
-    const int ninst = (int)subs.size();
+    const int ninst = limit >= 0 && limit < (int)subs.size() ? limit : (int)subs.size();
     const int tune_pf = w.tune_prefetch, tune_rpb = w.tune_rows_per_block;
     w = Wave();
     w.tune_prefetch = tune_pf;
@@ -1147,13 +1147,13 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
     // share a launch.
     std::vector<SubProblem> sorted_subs;
     std::vector<int> order;
+    std::vector<int> group_end;     // per planned position: the end of its parameter group
     const std::vector<SubProblem> *plan = &subs;
     if (ninst > capacity) {
         order.resize(ninst);
         for (int k = 0; k < ninst; k++) order[k] = k;
         // group of an instance: the rank of its parameters in numeric order
-        // (kernel, gamma, ..., C), so that neighbouring groups -- which share
-        // a launch at their boundary -- are alike too
+        // (kernel, gamma, ..., C)
         std::vector<int> group(ninst, 0);
         {
             std::vector<std::array<double, 6>> key(ninst);
@@ -1174,6 +1174,13 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         sorted_subs.reserve(ninst);
         for (int k : order) sorted_subs.push_back(subs[k]);
         plan = &sorted_subs;
+        // a launch holds the instances of one group only: the first launches
+        // of the next group hold its largest instances, which (other
+        // parameters, other iteration counts) would set the length of a
+        // launch that mixes them with the previous group's smallest
+        group_end.assign(ninst, ninst);
+        for (int k = ninst - 1; k > 0; k--)
+            group_end[k - 1] = group[order[k - 1]] == group[order[k]] ? group_end[k] : k;
     }
     std::vector<SolveResult> sorted_res;
     std::vector<SolveResult> &out = order.empty() ? res : sorted_res;
@@ -1191,7 +1198,7 @@ int solve_batch(const DeviceRows &rows, const std::vector<SubProblem> &subs, con
         Wave w;
         w.tune_prefetch = tune.prefetch;
         w.tune_rows_per_block = tune.rows_per_block;
-        if (wave_plan(rows, *plan, prm, first, capacity, w) != 0) return -1;
+        if (wave_plan(rows, *plan, prm, first, capacity, w, group_end.empty() ? -1 : group_end[first]) != 0) return -1;
         clk.mark("plan");
         char *arena = arena_reserve(w.dev_bytes);
         if (!arena) {

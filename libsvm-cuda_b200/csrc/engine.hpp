@@ -119,10 +119,11 @@ struct Wave {
 };
 
 // Plan the wave that starts at instance `first` within `capacity` co-resident
-// blocks (as many instances as fit).  Needs w.dev_bytes of device memory and
-// w.up_bytes + w.down_bytes of (preferably page-locked) host staging.
+// blocks (as many instances before `limit` as fit; limit < 0: up to the end).
+// Needs w.dev_bytes of device memory and w.up_bytes + w.down_bytes of
+// (preferably page-locked) host staging.
 int wave_plan(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, int first,
-              int capacity, Wave &w);
+              int capacity, Wave &w, int limit = -1);
 // Upload, launch and queue the result download on stream s (asynchronous).
 int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, const SolveParams &prm, Wave &w,
                char *dev, char *host, cudaStream_t s);

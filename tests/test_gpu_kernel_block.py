@@ -100,3 +100,27 @@ def test_tensor_form_on_csr_rows(engine):
     assert np.all(np.abs(got32 - want) <= (2.0 ** -10 + 2 * 5000 * 2.0 ** -24) * S + 1e-30)
     ex = rows.kernel_block(ia, ib, make_params(kernel_type=0, form=FORM_EXACT))
     assert np.all(np.abs(ex - want) <= 1e-12 * (1 + np.abs(want)))
+
+
+@pytest.mark.parametrize("form", [FORM_FP16X3, FORM_BF16X3, FORM_TF32])
+def test_many_tiles_per_cta_one_chunk(engine, form):
+    """d <= 64: one 64-feature chunk per 128 x 64 tile, so the persistent
+    CTAs walk ~15 tiles each and the tile ring of column data wraps twice;
+    ragged block edges.  Same bounds as the linear-block test."""
+    n, d = 6000, 40
+    p, X = _dense_rows(n, d, seed=11)
+    rows = ResidentRows(engine, p)
+    ia, ib = _blocks(n, 3001, 6003, seed=12)
+    A, B = X[ia], X[ib]
+    want = A @ B.T
+    S = np.abs(A) @ np.abs(B).T
+    u = 2.0 ** -24
+    got = rows.kernel_block(ia, ib, make_params(kernel_type=0, form=form))
+    if form == FORM_FP16X3:
+        M = d * np.abs(A).max(1)[:, None] * np.abs(B).max(1)[None, :]
+        bound = (2.0 ** -19 + 2 * d * u) * M
+    elif form == FORM_BF16X3:
+        bound = (2.0 ** -14 + 2 * d * u) * S
+    else:
+        bound = (2.0 ** -10 + 2 * d * u) * S
+    assert np.all(np.abs(got - want) <= bound + 1e-30)
