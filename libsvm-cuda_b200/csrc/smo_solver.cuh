@@ -651,30 +651,66 @@ __device__ __forceinline__ void cache_read_set(const CacheState &cs, const Cache
 // lookup (`prefetch`) takes a slot only if its set keeps at least two
 // evictable ways, so that the rows the solver must place later always find
 // one; otherwise it returns slot -1.
-__device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, int cur_epoch,
-                               unsigned long long clk, int whole, unsigned long long protect, int prefetch,
-                               const SetStage *pre = nullptr)
+//
+// The 32 lanes of one warp decide together: lane w reads and overlays way w
+// (the set's metadata, then the previous and this phase's decisions), and
+// the hit, the victim and the count of evictable ways come from ballots and
+// a shuffle reduction.  A hit is the highest way holding the tag; the victim
+// is the highest empty way, else the evictable way with the least stamp
+// (lowest way on equal stamps).  Every lane returns the same Lookup; lane 0
+// records the decision.  Called by all lanes of the warp with the same
+// arguments.
+__device__ Lookup cache_lookup_w(CacheState &cs, const CacheView &cv, int local, int cur_epoch,
+                                 unsigned long long clk, int whole, unsigned long long protect, int prefetch,
+                                 const SetStage *pre = nullptr)
 {
-    int tag[kMaxWays], ep[kMaxWays];
-    unsigned long long st[kMaxWays];
+    const int lane = threadIdx.x & 31;
     const int set = local % cv.nsets;
-    cache_read_set(cs, cv, set, tag, ep, st, pre);
-    int way = -1, ep_hit = 0;
-    unsigned long long st_hit = 0;
-#pragma unroll
-    for (int w = 0; w < kMaxWays; w++)
-        if (w < cv.nways && tag[w] == local) {
-            way = w;
-            ep_hit = ep[w];
-            st_hit = st[w];
+    const bool mine = lane < cv.nways;
+    int tag = kNoTag, ep = 0;
+    unsigned long long st = 0;
+    if (mine) {
+        if (pre && pre->set == set) {
+            tag = pre->tag[lane];
+            ep = pre->ep[lane];
+            st = pre->st[lane];
+        } else {
+            const long long s = (long long)set * cv.nways + lane;
+            tag = __ldcg(&cv.tag[s]);
+            ep = __ldcg(&cv.epoch[s]);
+            st = __ldcg(&cv.stamp[s]);
         }
+    }
+    // the previous phase's decisions, then this phase's, in order
+    const int nprev = cs.nprev, ncur = cs.ncur;
+    for (int k = 0; k < nprev; k++) {
+        const CacheRec &r = cs.prev[k];
+        if (r.set == set && r.way == lane) {
+            tag = r.tag;
+            ep = r.epoch;
+            st = r.stamp;
+        }
+    }
+    for (int k = 0; k < ncur; k++) {
+        const CacheRec &r = cs.cur[k];
+        if (r.set == set && r.way == lane) {
+            tag = r.tag;
+            ep = r.epoch;
+            st = r.stamp;
+        }
+    }
     Lookup L;
     L.was_prefetched = 0;
     CacheRec rec;
     rec.set = set;
     rec.stamp = prefetch ? (clk | kPrefetchMark) : clk;
     rec.tag = local;
-    if (way >= 0) {
+    int way;
+    const unsigned hit = __ballot_sync(0xffffffffu, mine && tag == local);
+    if (hit) {
+        way = 31 - __clz(hit);
+        const int ep_hit = __shfl_sync(0xffffffffu, ep, way);
+        const unsigned long long st_hit = __shfl_sync(0xffffffffu, st, way);
         const int va = ep_hit == kEpochFull || ep_hit == cur_epoch;
         L.valid_active = va;
         L.was_prefetched = va && (st_hit & kPrefetchMark) ? 1 : 0;
@@ -682,23 +718,22 @@ __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, i
         rec.way = way;
         rec.epoch = whole ? kEpochFull : (va ? ep_hit : cur_epoch);
     } else {
-        // victim: an empty way, else the least recently stamped evictable one
-        // (the first such way on equal stamps)
-        int victim = -1, evictable = 0, vtag = kNoTag;
-        unsigned long long vst = 0;
-#pragma unroll
-        for (int w = 0; w < kMaxWays; w++) {
-            if (w >= cv.nways) continue;
-            const unsigned long long sw = st[w] & ~kPrefetchMark;
-            if (tag[w] != kNoTag && sw >= protect) continue;
-            evictable++;
-            if (victim < 0 || tag[w] == kNoTag || (vtag != kNoTag && sw < vst)) {
-                victim = w;
-                vtag = tag[w];
-                vst = sw;
+        const unsigned long long sw = st & ~kPrefetchMark;
+        const bool evict = mine && !(tag != kNoTag && sw >= protect);
+        const unsigned em = __ballot_sync(0xffffffffu, evict);
+        const unsigned empty = __ballot_sync(0xffffffffu, evict && tag == kNoTag);
+        unsigned long long bv = evict ? sw : ~0ull;
+        int bw = evict ? lane : 32;
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int ow = __shfl_xor_sync(0xffffffffu, bw, o);
+            if (ov < bv || (ov == bv && ow < bw)) {
+                bv = ov;
+                bw = ow;
             }
         }
-        if (victim < 0 || (prefetch && evictable < 3)) {
+        const int victim = empty ? 31 - __clz(empty) : (em ? bw : -1);
+        if (victim < 0 || (prefetch && __popc(em) < 3)) {
             L.slot = -1;
             L.valid_active = 0;
             return L;
@@ -709,7 +744,12 @@ __device__ Lookup cache_lookup(CacheState &cs, const CacheView &cv, int local, i
         way = victim;
     }
     L.slot = (long long)set * cv.nways + way;
-    cs.cur[cs.ncur++] = rec;
+    __syncwarp();                     // every lane has read cs.cur
+    if (lane == 0) {
+        cs.cur[ncur] = rec;
+        cs.ncur = ncur + 1;
+    }
+    __syncwarp();
     return L;
 }
 
@@ -2176,28 +2216,34 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                     sh.bd[3] = v[1]; sh.bi[4] = ix[1];
                 }
                 __syncthreads();
-                if (threadIdx.x == 0) {
-                    // cache decisions for the row(s) of phase A; missing rows go to the fill list
+                if (threadIdx.x < 32) {
+                    // cache decisions for the row(s) of phase A (warp 0 together; lane 0
+                    // writes them); missing rows go to the fill list
                     const int whole = c.A == l;
-                    sh.nfill = 0;
+                    int nf = 0;
                     for (int k = 0; k < 2; k++) {
-                        sh.bl[k] = -1;
-                        sh.bi[8 + k] = 1;
+                        long long slot = -1;
+                        int va = 1;
                         if (sh.bi[4 * k] >= 0 && (k == 0 || nu)) {
-                            Lookup L = cache_lookup(sh.cs, D.cache, sh.bi[4 * k + 1], c.epoch, clkA, whole, clkA, 0);
-                            sh.bl[k] = L.slot;
-                            sh.bi[8 + k] = L.valid_active;
+                            const Lookup L = cache_lookup_w(sh.cs, D.cache, sh.bi[4 * k + 1], c.epoch, clkA, whole, clkA, 0);
+                            slot = L.slot;
+                            va = L.valid_active;
                             cnt_look++;
                             cnt_hit += L.valid_active;
                             cnt_pf_used += L.was_prefetched;
-                            if (!L.valid_active) {
-                                sh.frow[sh.nfill] = sh.bi[4 * k + 2];
-                                sh.fy[sh.nfill] = sh.bi[4 * k + 3];
-                                sh.fslot[sh.nfill] = L.slot;
-                                sh.nfill++;
+                            if (!va && threadIdx.x == 0) {
+                                sh.frow[nf] = sh.bi[4 * k + 2];
+                                sh.fy[nf] = sh.bi[4 * k + 3];
+                                sh.fslot[nf] = slot;
                             }
+                            if (!va) nf++;
+                        }
+                        if (threadIdx.x == 0) {
+                            sh.bl[k] = slot;
+                            sh.bi[8 + k] = va;
                         }
                     }
+                    if (threadIdx.x == 0) sh.nfill = nf;
                 }
                 __syncthreads();
                 // speculative prefetch: a missing row is evaluated together with
@@ -2252,19 +2298,26 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
                         }
                     }
                     __syncthreads();
-                    if (threadIdx.x == 0) {
+                    if (threadIdx.x < 32) {
                         const int whole = c.A == l;
-                        for (int t = 0; t < sh.npick && sh.nfill < D.prefetch; t++) {
+                        int nf = sh.nfill;
+                        const int npick = sh.npick;
+                        for (int t = 0; t < npick && nf < D.prefetch; t++) {
                             const int e = sh.pick[t];
-                            Lookup L = cache_lookup(sh.cs, D.cache, c.pt->loc[e], c.epoch, clkA, whole, clkA, 1, &sh.sset[t]);
+                            const Lookup L = cache_lookup_w(sh.cs, D.cache, c.pt->loc[e], c.epoch, clkA, whole, clkA, 1,
+                                                            &sh.sset[t]);
                             if (L.slot >= 0 && !L.valid_active) {
-                                sh.frow[sh.nfill] = c.pt->row[e];
-                                sh.fy[sh.nfill] = c.pt->y[e];
-                                sh.fslot[sh.nfill] = L.slot;
-                                sh.nfill++;
+                                if (threadIdx.x == 0) {
+                                    sh.frow[nf] = c.pt->row[e];
+                                    sh.fy[nf] = c.pt->y[e];
+                                    sh.fslot[nf] = L.slot;
+                                }
+                                nf++;
                                 cnt_pf++;
                             }
                         }
+                        __syncwarp();
+                        if (threadIdx.x == 0) sh.nfill = nf;
                     }
                     __syncthreads();
                 }
@@ -2423,10 +2476,12 @@ __device__ void solve_instance(const InstanceDesc &D, int rank, Shared &sh, unsi
             // Q_j row
             // phase-B stamp: above every phase-A stamp of this iteration, below the next
             const unsigned long long clkB = 4ull * (unsigned long long)iter - 1ull;
-            if (threadIdx.x == 0) {
-                Lookup L = cache_lookup(sh.cs, D.cache, loc_j, c.epoch, clkB, c.A == l, clkA, 0);
-                sh.bl[2] = L.slot;
-                sh.bi[16] = L.valid_active;
+            if (threadIdx.x < 32) {
+                const Lookup L = cache_lookup_w(sh.cs, D.cache, loc_j, c.epoch, clkB, c.A == l, clkA, 0);
+                if (threadIdx.x == 0) {
+                    sh.bl[2] = L.slot;
+                    sh.bi[16] = L.valid_active;
+                }
                 cnt_look++;
                 cnt_hit += L.valid_active;
                 cnt_pf_used += L.was_prefetched;
