@@ -65,9 +65,9 @@ SolveParams to_solve_params(const svmb_params &p)
     return prm;
 }
 
-// one problem in the reference's formulation of params.svm_type
-// (svm.cpp:1500-1699), over the rows with ids rows[0..l)
-int make_subproblem(const svmb_params &p, int l, const int *rows, const double *y, int nrows, SubProblem &sp)
+// the input checks of one instance (sets the error message; no side effects
+// otherwise, so instances can be built in parallel once all have passed)
+int check_subproblem(const svmb_params &p, int l, const int *rows, const double *y, int nrows)
 {
     if (l < 0) { set_error("inst_ptr must be non-decreasing"); return -1; }
     for (int i = 0; i < l; i++)
@@ -78,6 +78,14 @@ int make_subproblem(const svmb_params &p, int l, const int *rows, const double *
         for (int i = 0; i < l; i++) (y[i] > 0 ? npos : nneg)++;
         if (p.nu * l / 2 > std::min(npos, nneg)) { set_error("specified nu is infeasible"); return -1; }
     }
+    return 0;
+}
+
+// one problem in the reference's formulation of params.svm_type
+// (svm.cpp:1500-1699), over the rows with ids rows[0..l)
+int make_subproblem(const svmb_params &p, int l, const int *rows, const double *y, int nrows, SubProblem &sp)
+{
+    if (check_subproblem(p, l, rows, y, nrows) != 0) return -1;
     return formulate(p.svm_type, rows, y, l, p.C_pos, p.C_neg, p.C_pos, p.nu, p.p, sp);
 }
 
@@ -128,16 +136,28 @@ int solve_many(const DeviceRows &rows, int ninst, const int *inst_ptr, const int
     }
     // every instance carries its own parameters (kernel, C, eps, cache, ...);
     // only the arithmetic form is common to a launch
+    for (int k = 0; k < ninst; k++)
+        if (check_subproblem(params[k], inst_ptr[k + 1] - inst_ptr[k], inst_rows + inst_ptr[k], inst_y + inst_ptr[k],
+                             rows.n) != 0)
+            return -1;
+    // the instances are independent: built, and their results decoded, on all
+    // host threads (formulate fails only for an svm_type that check_params
+    // already rejected)
     std::vector<SolveParams> own(ninst);
     std::vector<SubProblem> subs(ninst);
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad) if (ninst > 1)
     for (int k = 0; k < ninst; k++) {
         const int a = inst_ptr[k], b = inst_ptr[k + 1];
-        if (make_subproblem(params[k], b - a, inst_rows + a, inst_y + a, rows.n, subs[k]) != 0) return -1;
+        bad |= formulate(params[k].svm_type, inst_rows + a, inst_y + a, b - a, params[k].C_pos, params[k].C_neg,
+                         params[k].C_pos, params[k].nu, params[k].p, subs[k]) != 0;
         own[k] = to_solve_params(params[k]);
         subs[k].own = &own[k];
     }
+    if (bad) { set_error("unknown svm_type"); return -1; }
     std::vector<SolveResult> res;
     if (solve_batch(rows, subs, own[0], res, 0) != 0) return -1;
+#pragma omp parallel for schedule(dynamic, 1) if (ninst > 1)
     for (int k = 0; k < ninst; k++)
         finish_instance(params[k], subs[k], res[k], inst_y + inst_ptr[k], inst_ptr[k + 1] - inst_ptr[k],
                         alpha_out + inst_ptr[k], stats ? &stats[k] : nullptr);
