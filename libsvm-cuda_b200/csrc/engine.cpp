@@ -328,6 +328,49 @@ int upload_csr(const long long *rowptr, const int *col, const float *val, int n,
     return 0;
 }
 
+// Dense rows [n][ld] built on the host, uploaded as they are: the device
+// block holds [dense rows][norms x 2] and no CSR arrays.
+static int upload_dense(const float *X, int n, int d, long long nnz, DeviceRows &out, cudaStream_t s, int alloc)
+{
+    const bool async_alloc = alloc == kAllocAsync;
+    out.n = n;
+    out.d = d > 0 ? d : 1;
+    out.ld = (out.d + 3) & ~3;
+    out.dense = true;
+    out.nnz = nnz;
+    auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
+    const size_t xbytes = std::max<size_t>((size_t)n * out.ld, 4) * sizeof(float);
+    const size_t b_sq = al(xbytes);
+    const size_t b_end = b_sq + 2 * al((size_t)std::max(n, 1) * sizeof(double));
+    char *blk = nullptr;
+    if (alloc == kAllocPooled) blk = rowpool_take(b_end);
+    out.block_pooled = blk != nullptr;
+    if (!blk) {
+        if (async_alloc) CK(cudaMallocAsync((void **)&blk, b_end, s));
+        else CK(cudaMalloc((void **)&blk, b_end));
+    }
+    out.block = blk;
+    out.block_async = async_alloc;
+    out.block_bytes = b_end;
+    out.rowptr = nullptr;
+    out.col = nullptr;
+    out.val = nullptr;
+    out.X = (float *)blk;
+    out.xsq[0] = (double *)(blk + b_sq);
+    out.xsq[1] = (double *)(blk + b_sq + al((size_t)std::max(n, 1) * sizeof(double)));
+    if (n) CK(xfer_async(out.X, X, (size_t)n * out.ld * sizeof(float), cudaMemcpyHostToDevice, s));
+    out.h2d_bytes = (size_t)n * out.ld * sizeof(float);
+    out.bytes = (size_t)n * out.ld * sizeof(float);
+    for (int f = 0; f < 2; f++) {
+        if (n) {
+            CK(launch_xsq(out.view(f), n, out.xsq[f], f, s));
+            count_launch();
+        }
+    }
+    if (!async_alloc) CK(cudaStreamSynchronize(s));
+    return 0;
+}
+
 int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cudaStream_t s, int alloc)
 {
     // CSR with 0-based columns; libsvm indices start at 1 (index 0 is kept as a
@@ -352,8 +395,52 @@ int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cud
         return -1;
     }
     const int base = (nnz && min_index == 0) ? 0 : 1;
-    // CSR arrays built directly in page-locked staging memory
     std::lock_guard<std::mutex> g(g_pin_mu);
+    {
+        // upload_csr's layout rule; dense rows that are no larger than the CSR
+        // arrays are built here and uploaded as they are (half the bytes of the
+        // CSR arrays for fully dense data, and no scatter on the device)
+        const int d = nnz ? max_index - base + 1 : 1;
+        const int ld = (d + 3) & ~3;
+        const double dense_bytes = (double)n * ld * 4.0;
+        const double csr_bytes = (double)(n + 1) * 8.0 + (double)nnz * 8.0;
+        bool dense = force == 1 || (force < 0 && dense_bytes <= 1.2 * csr_bytes);
+        if (dense && dense_bytes > 60e9) dense = false;
+        if (dense && dense_bytes <= csr_bytes) {
+            const size_t elems = std::max<size_t>((size_t)n * ld, 4);
+            float *X = (float *)pinned_staging(elems * sizeof(float));
+            std::vector<float> fallback_x;
+            if (!X) {
+                fallback_x.resize(elems);
+                X = fallback_x.data();
+            }
+#pragma omp parallel for schedule(static)
+            for (int r = 0; r < n; r++) {
+                float *row = X + (size_t)r * ld;
+                // a row of ld strictly increasing indices covers every column;
+                // any other row is cleared first
+                bool full = cnt[r + 1] - cnt[r] == ld;
+                if (full) {
+                    int prev = -1;
+                    for (const svm_node *p = x[r]; p->index != -1; ++p) {
+                        const int c = p->index - base;
+                        if (c <= prev) { full = false; break; }
+                        prev = c;
+                        row[c] = (float)p->value;
+                    }
+                }
+                if (!full) {
+                    memset(row, 0, sizeof(float) * ld);
+                    for (const svm_node *p = x[r]; p->index != -1; ++p) row[p->index - base] = (float)p->value;
+                }
+            }
+            clk.mark("convert");
+            const int rc = upload_dense(X, n, d, nnz, out, s, alloc);
+            clk.mark("upload");
+            return rc;
+        }
+    }
+    // CSR arrays built directly in page-locked staging memory
     const size_t bytes = ((size_t)n + 1) * 8 + (size_t)nnz * 8 + 64;
     char *pin = (char *)pinned_staging(bytes);
     std::vector<char> fallback;

@@ -380,9 +380,15 @@ void plan_training(const svm_problem *prob, const svm_parameter *param, const in
     t.subs.resize(npair);
     t.sub_y.resize(npair);
     if (param->probability) t.est.resize(npair);
-    int p = 0;
-    for (int i = 0; i < nr_class; i++)
-        for (int j = i + 1; j < nr_class; j++, p++) {
+    std::vector<int> pair_i(npair), pair_j(npair);
+    for (int i = 0, p = 0; i < nr_class; i++)
+        for (int j = i + 1; j < nr_class; j++, p++) pair_i[p] = i, pair_j[p] = j;
+    // the pairs are independent, so they are built on all host threads --
+    // except with probability estimates, whose shuffles draw rand() in pair order
+#pragma omp parallel for schedule(dynamic, 1) if (npair > 1 && !param->probability)
+    for (int p = 0; p < npair; p++) {
+        {
+            const int i = pair_i[p], j = pair_j[p];
             // class i's rows as +1, then class j's as -1
             const int ci = t.count[i], cj = t.count[j], n = ci + cj;
             std::vector<int> rows(n);
@@ -430,6 +436,7 @@ void plan_training(const svm_problem *prob, const svm_parameter *param, const in
             formulate(param->svm_type, rows.data(), yv.data(), n, t.weighted_C[i], t.weighted_C[j], param->C,
                       param->nu, param->p, t.subs[p]);
         }
+    }
 }
 
 void collect(Training &t, std::vector<SubProblem> &all)
@@ -438,9 +445,13 @@ void collect(Training &t, std::vector<SubProblem> &all)
         for (Training::Fold &f : e.folds)
             if (f.model) collect(*f.model, all);
     t.first = all.size();
-    for (SubProblem &sp : t.subs) {
-        sp.own = &t.solve;
-        all.push_back(sp);
+    const int nsub = (int)t.subs.size();
+    all.resize(t.first + nsub);
+    // copies of independent subproblems (hundreds of thousands of positions)
+#pragma omp parallel for schedule(dynamic, 1) if (nsub > 1)
+    for (int p = 0; p < nsub; p++) {
+        t.subs[p].own = &t.solve;
+        all[t.first + p] = t.subs[p];
     }
 }
 
