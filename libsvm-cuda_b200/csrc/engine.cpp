@@ -371,11 +371,91 @@ static int upload_dense(const float *X, int n, int d, long long nnz, DeviceRows 
     return 0;
 }
 
+// Row r of x written as a dense row of width d (padded to ld with zeros),
+// columns index - base.  Returns its entry count, or -1 (nothing defined)
+// when an index lies outside [base, base + d).
+static long long dense_row(const svm_node *row_nodes, int base, int d, int ld, float *row)
+{
+    long long c = 0;
+    int prev = -1;
+    bool inorder = true;
+    for (const svm_node *p = row_nodes; p->index != -1; ++p, ++c) {
+        const int k = p->index - base;
+        if (k < 0 || k >= d) return -1;
+        if (k <= prev) inorder = false;
+        prev = k;
+        row[k] = (float)p->value;
+    }
+    if (inorder && c == d) {
+        // every column written once: only the padding is cleared
+        for (int k = d; k < ld; k++) row[k] = 0.0f;
+    } else {
+        memset(row, 0, sizeof(float) * ld);
+        for (const svm_node *p = row_nodes; p->index != -1; ++p) row[p->index - base] = (float)p->value;
+    }
+    return c;
+}
+
+// upload_csr's layout rule: dense rows when they are not much larger than the CSR arrays
+static bool dense_layout(int force, int n, int ld, long long nnz, double *dense_bytes, double *csr_bytes)
+{
+    *dense_bytes = (double)n * ld * 4.0;
+    *csr_bytes = (double)(n + 1) * 8.0 + (double)nnz * 8.0;
+    bool dense = force == 1 || (force < 0 && *dense_bytes <= 1.2 * *csr_bytes);
+    if (dense && *dense_bytes > 60e9) dense = false;
+    return dense;
+}
+
 int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cudaStream_t s, int alloc)
 {
     // CSR with 0-based columns; libsvm indices start at 1 (index 0 is kept as a
-    // column when present).  Rows are converted in parallel on the host.
+    // column when present).  Rows are converted in parallel on the host.  When
+    // the dense layout is chosen and is no larger than the CSR arrays, the rows
+    // are built dense here and uploaded as they are (half the bytes of the CSR
+    // arrays for fully dense data, and no scatter on the device).
     StageClock clk("upload_rows");
+    std::lock_guard<std::mutex> g(g_pin_mu);
+    auto pinned_rows = [](size_t elems, std::vector<float> &fallback) {
+        float *X = (float *)pinned_staging(elems * sizeof(float));
+        if (!X) {
+            fallback.resize(elems);
+            X = fallback.data();
+        }
+        return X;
+    };
+    if (force != 0 && n > 0) {
+        // Dense data in one pass: when the first row holds every column from
+        // its first index (0 or 1) on, the rows are written as dense rows of
+        // that width while they are counted.  The result is the two-pass
+        // path's exactly (same base, width and values); a row with an index
+        // outside that range, or the layout rule choosing CSR, sends the call
+        // on to the two passes.
+        const svm_node *r0 = x[0];
+        int c0 = 0;
+        bool inc = r0[0].index == 0 || r0[0].index == 1;
+        for (; r0[c0].index != -1; c0++)
+            if (c0 > 0 && r0[c0].index != r0[c0 - 1].index + 1) inc = false;
+        if (inc && c0 > 0) {
+            const int base = r0[0].index, d = c0, ld = (d + 3) & ~3;
+            double db, cb;
+            std::vector<float> fallback_x;
+            float *X = pinned_rows(std::max<size_t>((size_t)n * ld, 4), fallback_x);
+            long long nnz = 0;
+            int bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nnz) reduction(| : bad)
+            for (int r = 0; r < n; r++) {
+                const long long c = dense_row(x[r], base, d, ld, X + (size_t)r * ld);
+                if (c < 0) bad = 1;
+                else nnz += c;
+            }
+            if (!bad && dense_layout(force, n, ld, nnz, &db, &cb) && db <= cb) {
+                clk.mark("convert");
+                const int rc = upload_dense(X, n, d, nnz, out, s, alloc);
+                clk.mark("upload");
+                return rc;
+            }
+        }
+    }
     std::vector<long long> cnt((size_t)n + 1, 0);
     int min_index = INT_MAX, max_index = 0;
 #pragma omp parallel for schedule(static) reduction(min : min_index) reduction(max : max_index)
@@ -395,45 +475,15 @@ int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cud
         return -1;
     }
     const int base = (nnz && min_index == 0) ? 0 : 1;
-    std::lock_guard<std::mutex> g(g_pin_mu);
     {
-        // upload_csr's layout rule; dense rows that are no larger than the CSR
-        // arrays are built here and uploaded as they are (half the bytes of the
-        // CSR arrays for fully dense data, and no scatter on the device)
         const int d = nnz ? max_index - base + 1 : 1;
         const int ld = (d + 3) & ~3;
-        const double dense_bytes = (double)n * ld * 4.0;
-        const double csr_bytes = (double)(n + 1) * 8.0 + (double)nnz * 8.0;
-        bool dense = force == 1 || (force < 0 && dense_bytes <= 1.2 * csr_bytes);
-        if (dense && dense_bytes > 60e9) dense = false;
-        if (dense && dense_bytes <= csr_bytes) {
-            const size_t elems = std::max<size_t>((size_t)n * ld, 4);
-            float *X = (float *)pinned_staging(elems * sizeof(float));
+        double db, cb;
+        if (dense_layout(force, n, ld, nnz, &db, &cb) && db <= cb) {
             std::vector<float> fallback_x;
-            if (!X) {
-                fallback_x.resize(elems);
-                X = fallback_x.data();
-            }
+            float *X = pinned_rows(std::max<size_t>((size_t)n * ld, 4), fallback_x);
 #pragma omp parallel for schedule(static)
-            for (int r = 0; r < n; r++) {
-                float *row = X + (size_t)r * ld;
-                // a row of ld strictly increasing indices covers every column;
-                // any other row is cleared first
-                bool full = cnt[r + 1] - cnt[r] == ld;
-                if (full) {
-                    int prev = -1;
-                    for (const svm_node *p = x[r]; p->index != -1; ++p) {
-                        const int c = p->index - base;
-                        if (c <= prev) { full = false; break; }
-                        prev = c;
-                        row[c] = (float)p->value;
-                    }
-                }
-                if (!full) {
-                    memset(row, 0, sizeof(float) * ld);
-                    for (const svm_node *p = x[r]; p->index != -1; ++p) row[p->index - base] = (float)p->value;
-                }
-            }
+            for (int r = 0; r < n; r++) dense_row(x[r], base, d, ld, X + (size_t)r * ld);
             clk.mark("convert");
             const int rc = upload_dense(X, n, d, nnz, out, s, alloc);
             clk.mark("upload");
@@ -986,10 +1036,16 @@ int wave_start(const DeviceRows &rows, const std::vector<SubProblem> &subs, cons
         D.cache.nsets = Lk.sets;
         D.cache.nways = Lk.ways;
         D.cache.stride = l;
+    }
+    // the instances' initial state into the staging block, on all host threads
+#pragma omp parallel for schedule(dynamic, 1) if (count > 1)
+    for (int k = 0; k < count; k++) {
+        const SubProblem &sp = subs[first + k];
+        const size_t l = sp.rows.size();
         memcpy(h_alpha + w.loff[k], sp.alpha0.data(), sizeof(double) * l);
         memcpy(h_p + w.loff[k], sp.p.data(), sizeof(double) * l);
         memcpy(h_row + w.loff[k], sp.rows.data(), sizeof(int) * l);
-        memcpy(h_y + w.loff[k], sp.y.data(), (size_t)l);
+        memcpy(h_y + w.loff[k], sp.y.data(), l);
     }
     if (g_drop_block.exchange(0)) {
         w.drop_last_block = true;
@@ -1046,6 +1102,7 @@ int wave_finish(Wave &w, std::vector<SolveResult> &res)
     const SolveOut *h_out = (const SolveOut *)(w.host + w.up_bytes);
     const double *h_alocal = (const double *)(w.host + w.up_bytes + (w.o_alocal - w.o_out));
     int rc = 0;
+#pragma omp parallel for schedule(dynamic, 1) if (w.count > 1)
     for (int k = 0; k < w.count; k++) {
         SolveResult &R = res[w.first + k];
         const size_t l = w.loff[k + 1] - w.loff[k];
@@ -1053,11 +1110,12 @@ int wave_finish(Wave &w, std::vector<SolveResult> &res)
         R.out = h_out[k];
         R.seconds = ms * 1e-3;
         R.fill_path = w.fill_path[k];
-        if (R.out.status < 0) {
+    }
+    for (int k = 0; k < w.count; k++)
+        if (h_out[k].status < 0) {
             set_error("solver group barrier timed out");
             rc = -1;
         }
-    }
     return rc;
 }
 

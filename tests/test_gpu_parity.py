@@ -200,3 +200,46 @@ def test_results_independent_of_block_count(engine, name, blocks):
     assert np.array_equal(one["sv_indices"], many["sv_indices"])
     assert np.array_equal(one["sv_coef"], many["sv_coef"])
     assert np.array_equal(one["rho"], many["rho"])
+
+
+def _csr_from_rows(rows, y):
+    from svmb200 import datagen
+    indptr = np.zeros(len(rows) + 1, dtype=np.int64)
+    np.cumsum([len(r) for r in rows], out=indptr[1:])
+    idx = np.concatenate([np.array([k for k, _ in r], dtype=np.int32) for r in rows])
+    val = np.concatenate([np.array([v for _, v in r], dtype=np.float32).astype(np.float64) for r in rows])
+    return datagen.CSR(indptr, idx, val, np.asarray(y, dtype=np.float64), int(idx.max()))
+
+
+@pytest.mark.parametrize("shape", ["full", "holes", "wider_row"])
+def test_dense_upload_paths_match_oracle(engine, oracle, shape):
+    """svm_node rows become dense device rows in one pass when the first row
+    holds every column, in two passes otherwise; rows with missing columns
+    are cleared first.  Every path must train what the oracle trains."""
+    from svmb200 import cabi
+    rng = np.random.default_rng(11)
+    n, d = 300, 13                       # width not a multiple of 4: padded rows
+    X = rng.normal(size=(n, d)).astype(np.float32)
+    y = np.where(X[:, 0] + 0.5 * X[:, 1] + 0.3 * rng.normal(size=n) > 0, 1.0, -1.0)
+    rows = [[(k + 1, float(X[i, k])) for k in range(d)] for i in range(n)]
+    if shape in ("holes", "wider_row"):
+        for i in range(1, n, 7):         # drop some columns of later rows
+            rows[i] = [e for e in rows[i] if e[0] % 3 != (i % 3)]
+    if shape == "wider_row":
+        rows[n // 2] = rows[n // 2] + [(d + 3, 0.75)]   # wider than the first row
+    tr = _csr_from_rows(rows, y)
+    te = _csr_from_rows(rows[:50], y[:50])
+    prm = cabi.make_param(svm_type=0, kernel_type=2, gamma=1.0 / d, C_=1.0)
+    model = engine.train(tr, prm)
+    ours = model.arrays()
+    stats = engine.last_stats()
+    m, _, gold, infos = oracle.train(tr, prm)
+    assert abs(stats[0]["iters"] - infos[0]["iters"]) <= max(1, 0.02 * infos[0]["iters"])
+    assert abs(ours["rho"][0] - gold["rho"][0]) <= 1e-4
+    assert abs(stats[0]["obj"] - infos[0]["obj"]) <= 1e-6 * abs(infos[0]["obj"])
+    lab, dec = engine.predict(model, te)
+    olab, odec = oracle.predict(m, te)
+    assert np.array_equal(lab, olab)
+    assert np.max(np.abs(dec - odec)) <= 1e-5
+    oracle.free(m)
+    model.free()
