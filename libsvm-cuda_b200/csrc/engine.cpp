@@ -435,7 +435,9 @@ int upload_rows(const svm_node *const *x, int n, DeviceRows &out, int force, cud
         bool inc = r0[0].index == 0 || r0[0].index == 1;
         for (; r0[c0].index != -1; c0++)
             if (c0 > 0 && r0[c0].index != r0[c0 - 1].index + 1) inc = false;
-        if (inc && c0 > 0) {
+        // (only while the attempt's dense rows stay modest: sparse data whose
+        // first row happens to be complete would otherwise stage n x d floats)
+        if (inc && c0 > 0 && (double)n * (double)((c0 + 3) & ~3) * 4.0 <= 4e9) {
             const int base = r0[0].index, d = c0, ld = (d + 3) & ~3;
             double db, cb;
             std::vector<float> fallback_x;
