@@ -21,6 +21,7 @@ write) between timed steps.
 """
 import argparse
 import ctypes as C
+import datetime
 import json
 import math
 import multiprocessing as mp
@@ -81,11 +82,14 @@ def pair_instances(p):
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons.  The sampler is
+    started well before the timed region (its start-up, NVML initialisation
+    included, must not overlap the timed steps); stop() keeps the samples
+    whose timestamps fall inside the timed window."""
 
     def __init__(self, index, path):
         self.path, self.proc = path, None
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+        q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
         try:
@@ -95,7 +99,7 @@ class Clocks:
         except Exception:
             self.proc = None
 
-    def stop(self):
+    def stop(self, window=None):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -104,22 +108,25 @@ class Clocks:
         except Exception:
             self.proc.kill()
         self.f.close()
-        sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        samples = []
         for line in open(self.path):
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                samples.append((ts, float(parts[2]), float(parts[3]), parts[6:10]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
+        inside = [x for x in samples if window and window[0] - 0.06 <= x[0] <= window[1] + 0.06]
+        use = inside if inside else samples
+        sm = [x[1] for x in use]
+        mx = [x[2] for x in use]
+        reasons = {nm for x in use for nm, v in zip(names, x[3]) if v.lower() == "active"}
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window": "timed steps" if inside else "whole sampling (no sample inside the timed steps)"}
 
 
 # ----------------------------------------------------------------------------
@@ -667,6 +674,10 @@ def main():
         torch.cuda.synchronize()
 
     # ---------------- value: resident rows ----------------
+    # the clock sampler starts here, long before the timed steps, so that its
+    # start-up does not overlap them
+    clocks_dir = args.clocks_dir or tempfile.gettempdir()
+    clocks = Clocks(local, os.path.join(clocks_dir, f"svmb_clocks_rank{rank}.csv"))
     # the autotuner settles its configuration for this workload first (untimed;
     # every configuration gives the same results)
     for _ in range(12):
@@ -676,10 +687,10 @@ def main():
     tuned = eng.autotune_last()
     for _ in range(args.warmup):
         res.solve_many(rows, ys, params)
-    clocks_dir = args.clocks_dir or tempfile.gettempdir()
-    clocks = Clocks(local, os.path.join(clocks_dir, f"svmb_clocks_rank{rank}.csv"))
     step_ms, kern_s, alg_bytes, stats_all = [], [], [], []
     launches0 = eng.launches()
+    barrier()
+    t_window0 = time.time()
     for _ in range(args.steps):
         flush.fill_(1.0)
         barrier()
@@ -699,7 +710,8 @@ def main():
         alg_bytes.append(sum(46.0 * s["sum_active"] + s["fill_targets"] * (row_bytes + 4.0) for s in stats))
         stats_all.append(stats)
     launches = eng.launches() - launches0
-    clk = clocks.stop()
+    t_window1 = time.time()
+    clk = clocks.stop(window=(t_window0, t_window1))
     t = torch.tensor([max(step_ms)], device="cuda", dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
