@@ -165,6 +165,19 @@ def _ref_solve_pair(k):
     return k, dt, nsv
 
 
+def max_over_ranks(value, world, device):
+    """The largest `value` over the ranks of the process group (every rank gets
+    it); the value itself when there is one rank.  Replicas time themselves and
+    the job's time is its slowest replica's."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
@@ -655,7 +668,6 @@ def main():
 
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     eng = Engine()
     if not eng.available():
@@ -712,14 +724,9 @@ def main():
     launches = eng.launches() - launches0
     t_window1 = time.time()
     clk = clocks.stop(window=(t_window0, t_window1))
-    t = torch.tensor([max(step_ms)], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    mean_ms = sum(step_ms) / len(step_ms)
-    if world > 1:
-        tm = torch.tensor([mean_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        mean_ms = float(tm.item())
+    # the slowest rank's times: every rank takes the same collectives in the same order
+    max_over_ranks(max(step_ms), world, "cuda")
+    mean_ms = max_over_ranks(sum(step_ms) / len(step_ms), world, "cuda")
     solves_per_step = len(rows) * world
     value = solves_per_step / (mean_ms * 1e-3)
 
@@ -763,11 +770,7 @@ def main():
         d2h.append(db1.value - db0.value)
         eng.lib.svm_free_and_destroy_model(C.byref(m))
     eng.lib.svm_set_print_string_function(eng._cb)
-    e2e_mean = sum(e2e_ms) / len(e2e_ms)
-    if world > 1:
-        tm = torch.tensor([e2e_mean], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-        e2e_mean = float(tm.item())
+    e2e_mean = max_over_ranks(sum(e2e_ms) / len(e2e_ms), world, "cuda")
 
     # ---------------- batched vs largest subproblem alone ----------------
     big = int(np.argmax([len(r) for r in rows]))
