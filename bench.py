@@ -547,6 +547,31 @@ def cv_grid_extra(eng):
             "best_point": {"C": Cs[int(np.argmax(acc))], "gamma": gs[int(np.argmax(acc))], "accuracy": max(acc)}}
 
 
+def _serving_ref_init():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    lib = oracle_py.reference_lib()
+    if lib is None:
+        raise RuntimeError("oracle/_ref/libsvm_ref.so is not built")
+    quiet = cabi.PRINT_FUNC(lambda s: None)
+    lib.svm_set_print_string_function(quiet)
+    lib.svm_free_and_destroy_model.argtypes = [C.POINTER(C.POINTER(cabi.svm_model))]
+    _W.update(lib=lib, quiet=quiet, specs=datagen.serving_specs(n_jobs=48, rate=200.0))
+
+
+def _serving_ref_job(k):
+    """Job k of the serving stream through the reference's svm_train (CPU)."""
+    j = datagen.serving_job(_W["specs"][k])
+    nodes = cabi.NodeRows(j.problem)
+    prm = cabi.make_param(svm_type=j.svm_type, kernel_type=j.kernel_type, gamma=j.gamma, degree=j.degree, C_=j.C,
+                          nu=j.nu, cache_size=100.0, eps=1e-3, shrinking=1, cuda_flag=0)
+    t0 = time.perf_counter()
+    m = _W["lib"].svm_train(C.byref(nodes.prob), C.byref(prm))
+    dt = time.perf_counter() - t0
+    _W["lib"].svm_free_and_destroy_model(C.byref(m))
+    return k, dt
+
+
 def serving_extra(eng, make_params):
     """Request loop: 48 mixed training requests arriving as a Poisson stream at
     200/s (n log-uniform in [500, 50000], d in {16,64,256,512}, 60% dense / 40%
@@ -570,21 +595,41 @@ def serving_extra(eng, make_params):
     res = [srv.wait(t) for t in tickets]
     st = srv.stats()
     srv.close()
-    lat, fin = [], 0.0
+    lat, dur, fin = [], [], 0.0
     for j in jobs:
         t1 = time.perf_counter()
         eng.solve_binary(j.problem, prm(j))
         d = time.perf_counter() - t1
+        dur.append(d)
         fin = max(j.arrival, fin) + d
         lat.append(fin - j.arrival)
     same = all(np.array_equal(a, eng.solve_binary(j.problem, prm(j))[0]) for j, (a, _, _) in zip(jobs[:8], res[:8]))
+    # the reference's CPU solver, one process per job on the host's cores, on a
+    # bounded sample: the 24 smallest jobs (the largest take over 15 minutes
+    # each on one core)
+    cpu = None
+    if _reference_lib() is not None:
+        specs = datagen.serving_specs(n_jobs=48, rate=200.0)
+        small = sorted(range(len(specs)), key=lambda k: specs[k]["n"])[:24]
+        procs = min(os.cpu_count() or 1, len(small))
+        with mp.get_context("spawn").Pool(processes=procs, initializer=_serving_ref_init) as pool:
+            t1 = time.perf_counter()
+            per_job = pool.map(_serving_ref_job, small, chunksize=1)
+            wall = time.perf_counter() - t1
+        gpu_same = sum(dur[k] for k in small)
+        cpu = {"sample": f"the 24 smallest of the 48 jobs (n {specs[small[0]]['n']}-{specs[small[-1]]['n']}), "
+                         f"reference svm_train, one process per job",
+               "processes": procs, "cores": procs, "kind": "reference", "solves_per_s": len(small) / wall,
+               "wall_s": wall, "cpu_seconds": sum(dt for _, dt in per_job),
+               "gpu_one_at_a_time_same_jobs_solves_per_s": len(small) / gpu_same}
     return {"workload": "48 requests, Poisson 200/s, serving mix (seeded)",
             "server": {"p50_s": st["p50_s"], "p99_s": st["p99_s"], "solves_per_s": st["solves_per_s"],
                        "launches": st["waves"], "max_concurrent_launches": st["max_concurrent_waves"],
                        "peak_device_bytes": st["peak_mem_bytes"]},
             "one_at_a_time": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                               "solves_per_s": len(jobs) / (fin - jobs[0].arrival)},
-            "first8_identical_alone": bool(same)}
+            "first8_identical_alone": bool(same),
+            "cpu_reference_sample": cpu}
 
 
 def profile_case(name):

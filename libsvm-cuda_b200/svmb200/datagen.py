@@ -214,25 +214,39 @@ class Job:
     degree: int
 
 
-def serving_mix(n_jobs: int = 64, rate: float = 200.0, n_lo: int = 500, n_hi: int = 50000,
-                seed: int = 5, dims=(16, 64, 256, 512)) -> List[Job]:
-    """Poisson arrivals of mixed jobs: 60% dense Gaussian mixtures / 40% sparse CSR
-    (nnz mean 40), 70% C-SVC / 30% nu-SVC (nu=0.3), RBF or degree-3 poly, C in {1,10}."""
+def serving_specs(n_jobs: int = 64, rate: float = 200.0, n_lo: int = 500, n_hi: int = 50000,
+                  seed: int = 5, dims=(16, 64, 256, 512)) -> List[dict]:
+    """The job stream of serving_mix without the rows: arrival time, size,
+    width, data seed and kind, formulation, kernel and C of every job, drawn in
+    the same order, so that serving_job(spec) rebuilds job k alone."""
     rng = np.random.default_rng(seed)
     t = 0.0
-    jobs = []
+    specs = []
     for j in range(n_jobs):
         t += rng.exponential(1.0 / rate)
         n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
         d = int(rng.choice(dims))
         js = int(rng.integers(0, 2**31 - 1))
-        if rng.random() < 0.6:
-            p, _ = dense_gauss(n=n, n_test=0, d=d, seed=js, flip=0.05)
-        else:
-            p, _ = sparse_text(n=n, n_test=0, d=max(d, 64), nnz_mean=min(40.0, max(d, 64) / 2), seed=js)
+        dense = bool(rng.random() < 0.6)
         svm_type = 1 if rng.random() < 0.3 else 0
         kernel = 2 if rng.random() < 0.5 else 1
         C = float(rng.choice([1.0, 10.0]))
-        gamma = 1.0 / p.d
-        jobs.append(Job(t, p, svm_type, kernel, C, 0.3, gamma, 3))
-    return jobs
+        specs.append(dict(arrival=t, n=n, d=d, seed=js, dense=dense, svm_type=svm_type, kernel=kernel, C=C))
+    return specs
+
+
+def serving_job(spec: dict) -> Job:
+    """One job of the serving stream, with its rows."""
+    n, d, js = spec["n"], spec["d"], spec["seed"]
+    if spec["dense"]:
+        p, _ = dense_gauss(n=n, n_test=0, d=d, seed=js, flip=0.05)
+    else:
+        p, _ = sparse_text(n=n, n_test=0, d=max(d, 64), nnz_mean=min(40.0, max(d, 64) / 2), seed=js)
+    return Job(spec["arrival"], p, spec["svm_type"], spec["kernel"], spec["C"], 0.3, 1.0 / p.d, 3)
+
+
+def serving_mix(n_jobs: int = 64, rate: float = 200.0, n_lo: int = 500, n_hi: int = 50000,
+                seed: int = 5, dims=(16, 64, 256, 512)) -> List[Job]:
+    """Poisson arrivals of mixed jobs: 60% dense Gaussian mixtures / 40% sparse CSR
+    (nnz mean 40), 70% C-SVC / 30% nu-SVC (nu=0.3), RBF or degree-3 poly, C in {1,10}."""
+    return [serving_job(s) for s in serving_specs(n_jobs, rate, n_lo, n_hi, seed, dims)]
