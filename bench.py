@@ -279,7 +279,9 @@ def precision_form_extra(eng, ResidentRows, make_params):
     bf16 split, tf32; fp32 TMEM accumulation, fp64 G/alpha/step/rho) against
     the plain fp32 CUDA-core form (one row per cache miss, incremental G_bar)
     and the exact form (bit-identical to the reference's float-Q solver).
-    Device seconds of the solve launch."""
+    Device seconds of the solve launch.  The reference's CPU solver runs on a
+    bounded sample (the first 2,000 rows) beside the engine's exact and FP16X3
+    forms on the same rows."""
     tr, te = datagen.dense_pixels(n=100000, n_test=20000)
     rows = ResidentRows(eng, tr, layout=1)
     idx = [np.arange(tr.n, dtype=np.int32)]
@@ -306,6 +308,24 @@ def precision_form_extra(eng, ResidentRows, make_params):
                      "section_share": {k: prof[q] / tot for q, k in enumerate(
                          ["a_reduce", "a_fill", "a_scan", "b_reduce", "b_fill", "b_update", "shrink"])}}
     rows.free()
+    # the reference's CPU solver on a bounded sample (the first 2,000 rows;
+    # the whole set would take hours on one core), and the engine on the same rows
+    sample = None
+    lib = _reference_lib()
+    if lib is not None:
+        sub = tr.take(np.arange(2000))
+        rprm = cabi.make_param(svm_type=0, kernel_type=2, gamma=1.0 / 784, C_=10.0, cache_size=4096.0, eps=1e-3,
+                               shrinking=1, cuda_flag=0)
+        r = reference_train(lib, sub, rprm)
+        lib.svm_free_and_destroy_model(C.byref(r["model"]))
+        lib.svm_set_print_string_function(cabi.PRINT_FUNC(lambda s: None))
+        srows = ResidentRows(eng, sub, layout=1)
+        sample = {"rows": 2000, "reference_seconds": r["seconds"], "reference_cores": 1}
+        for name in ("exact", "fp16x3_tensor"):
+            _, st = srows.solve_many([np.arange(sub.n, dtype=np.int32)], [np.ascontiguousarray(sub.y, dtype=np.float64)],
+                                     [forms[name]])
+            sample[name] = {"gpu_seconds": st[0]["seconds"], "vs_reference": _compare(st[0], r)}
+        srows.free()
     ex = out["exact"]
     for name in out:
         out[name]["obj_rel_diff_vs_exact"] = abs(out[name]["obj"] - ex["obj"]) / abs(ex["obj"])
@@ -315,6 +335,7 @@ def precision_form_extra(eng, ResidentRows, make_params):
                         "gamma=1/784, eps=1e-3, 4096 MB cache",
             "forms": out,
             "decision_values": predict,
+            "cpu_reference_sample": sample,
             "tensor_speedup_vs_fp32_plain": out["fp32_plain"]["seconds"] / out["fp16x3_tensor"]["seconds"],
             "speedup_vs_fp32_plain": {k: out["fp32_plain"]["seconds"] / v["seconds"] for k, v in out.items()},
             "tensor_speedup_vs_exact": out["exact"]["seconds"] / out["fp16x3_tensor"]["seconds"],
