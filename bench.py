@@ -43,9 +43,9 @@ WORKLOAD = "ovo45_rbf_d256: 10 classes 12000*0.8^k (53646 rows), d=256, RBF g=1/
 D = 256
 GAMMA = 1.0 / 256
 # DRAM bytes read + written by one batched launch of this workload, from an ncu
-# capture (dram__bytes_read.sum 9.16 GB + dram__bytes_write.sum 2.39 GB; one
+# capture (dram__bytes_read.sum 9.01 GB + dram__bytes_write.sum 2.69 GB; one
 # pass, so the full-size launch was captured); a profiler figure, not timed here
-TRAFFIC_PER_LAUNCH = 11.55e9
+TRAFFIC_PER_LAUNCH = 11.70e9
 CVAL = 1.0
 
 
