@@ -391,23 +391,31 @@ def dense_c1_extra(eng):
     ref_cli = os.path.join(ROOT, "oracle", "_ref", "svm-train")
     our_cli = os.path.join(ROOT, "libsvm-cuda_b200", "svm-train")
     if os.path.exists(ref_cli) and os.path.exists(our_cli):
-        with tempfile.TemporaryDirectory() as tmp:
-            data = os.path.join(tmp, "c1.txt")
-            datagen.write_libsvm(data, tr)
-            flags = ["-s", "0", "-t", "2", "-c", "1", "-g", "0.015625", "-e", "0.001", "-m", "100", "-q"]
-            subprocess.run([our_cli] + flags + [data, os.path.join(tmp, "warm.model")], check=True)
-            times = {}
-            for name, cli in (("ours", our_cli), ("reference", ref_cli)):
-                t0 = time.perf_counter()
-                subprocess.run([cli] + flags + [data, os.path.join(tmp, name + ".model")], check=True)
-                times[name] = time.perf_counter() - t0
-            same = open(os.path.join(tmp, "ours.model"), "rb").read() == open(os.path.join(tmp, "reference.model"),
-                                                                                 "rb").read()
-        out["svm_train_command"] = {"ours_s": times["ours"], "reference_s": times["reference"],
-                                    "speedup": times["reference"] / times["ours"], "model_files_identical": same,
-                                    "note": "wall time of each process: text parse, training, model file; ours "
-                                            "includes CUDA start-up"}
+        try:
+            out["svm_train_command"] = _cli_comparison(tr, our_cli, ref_cli)
+        except Exception as e:          # the rest of this workload's line stays
+            out["svm_train_command"] = {"error": str(e)}
     return out
+
+
+def _cli_comparison(tr, our_cli, ref_cli):
+    """Wall time of each svm-train process on the same text file and flags,
+    and whether the two model files are byte-identical."""
+    with tempfile.TemporaryDirectory() as tmp:
+        data = os.path.join(tmp, "c1.txt")
+        datagen.write_libsvm(data, tr)
+        flags = ["-s", "0", "-t", "2", "-c", "1", "-g", "0.015625", "-e", "0.001", "-m", "100", "-q"]
+        subprocess.run([our_cli] + flags + [data, os.path.join(tmp, "warm.model")], check=True)
+        times = {}
+        for name, cli in (("ours", our_cli), ("reference", ref_cli)):
+            t0 = time.perf_counter()
+            subprocess.run([cli] + flags + [data, os.path.join(tmp, name + ".model")], check=True)
+            times[name] = time.perf_counter() - t0
+        with open(os.path.join(tmp, "ours.model"), "rb") as f1, open(os.path.join(tmp, "reference.model"), "rb") as f2:
+            same = f1.read() == f2.read()
+    return {"ours_s": times["ours"], "reference_s": times["reference"], "speedup": times["reference"] / times["ours"],
+            "model_files_identical": same,
+            "note": "wall time of each process: text parse, training, model file; ours includes CUDA start-up"}
 
 
 def sparse_c2_extra(eng, ResidentRows, make_params):
